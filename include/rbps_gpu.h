@@ -1,0 +1,311 @@
+/*
+ * rbps_gpu.h - C ABI of the B200 (sm_100a) implementation of the RBPS
+ * per-step hot path: SAP broadphase, narrowphase + contact manifolds and the
+ * XPBD substep (integrate, contact/joint position solve, velocity update,
+ * restitution/friction velocity solve, joint damping).
+ *
+ * Every entry point returns an int status (RBPS_OK == 0, negative on error);
+ * rbps_last_error() gives the message of the last failing call on the
+ * calling thread.  No torch or CUDA types appear in the signatures: the
+ * stream is passed as an opaque pointer (a cudaStream_t or NULL).
+ *
+ * The surface mirrors the reference facade rbps::World
+ * (include/rbps/API/World.hpp:87-213) and its parameter structs
+ * (BodyAPI.hpp:22-31, ColliderAPI.hpp:17-27, JointAPI.hpp:24-57), generalised
+ * to a batch of independent worlds that step together on one GPU.  IDs follow
+ * the reference's "ID == slot == index" rule for collections without
+ * removals (storage/Soa.hpp:465,577): the n-th body / collider / joint added
+ * to a world gets ID n.
+ *
+ * Ownership: the caller owns every host buffer; the library owns all device
+ * memory.  One host thread drives a batch at a time (the reference World is
+ * likewise not thread-safe).
+ */
+#ifndef RBPS_GPU_H
+#define RBPS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define RBPS_API __attribute__((visibility("default")))
+#else
+#define RBPS_API
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    RBPS_OK = 0,
+    RBPS_ERR_INVALID = -1,       /* bad argument / call order              */
+    RBPS_ERR_CAPACITY = -2,      /* a device buffer (pairs, contacts, ...) overflowed */
+    RBPS_ERR_CUDA = -3,          /* CUDA runtime failure                   */
+    RBPS_ERR_NOT_CONVERGED = -4, /* an iterative kernel hit its iteration cap */
+    RBPS_ERR_STATE = -5,         /* non-finite body state detected          */
+    RBPS_ERR_INTERNAL = -6       /* a device consistency check failed       */
+};
+
+/* ------------------------------------------------------------------ enums */
+/* Arithmetic of the device state and solver. */
+enum {
+    RBPS_PRECISION_FP64 = 0,       /* everything double, reference operation order */
+    RBPS_PRECISION_FP32 = 1,       /* everything float                              */
+    RBPS_PRECISION_FP32_POS64 = 2  /* float solver, double body positions           */
+};
+
+/* Order in which contact and joint rows are relaxed inside a substep. */
+enum {
+    RBPS_SOLVE_REFERENCE_ORDER = 0, /* sequential Gauss-Seidel in ContactList order (Contact.cpp:295-309) */
+    RBPS_SOLVE_COLORED = 1          /* graph-coloured Gauss-Seidel, one thread per pair per colour       */
+};
+
+/* rbps::BodyType (Body.hpp: enum BodyType { STATIC, DYNAMIC }). */
+enum { RBPS_BODY_STATIC = 0, RBPS_BODY_DYNAMIC = 1 };
+
+/* Shape kinds; the values are the rbc::Shape variant indices
+ * (rbc/shapes/ShapeTypes.hpp:67-69). */
+enum {
+    RBPS_SHAPE_SPHERE = 0,
+    RBPS_SHAPE_BOX = 1,
+    RBPS_SHAPE_CAPSULE = 3,
+    RBPS_SHAPE_PLANE = 6,
+    RBPS_SHAPE_CONVEX_HULL = 9
+};
+
+/* rbps::JointType / JointActuationType (constraints/Joint.hpp). */
+enum { RBPS_JOINT_PRISMATIC = 0, RBPS_JOINT_REVOLUTE = 1, RBPS_JOINT_FIXED = 2 };
+enum { RBPS_ACTUATION_FREE = 0, RBPS_ACTUATION_POSITION = 1, RBPS_ACTUATION_SPEED = 2 };
+
+/* ---------------------------------------------------------- descriptors */
+typedef struct rbps_batch_desc {
+    uint32_t n_worlds;          /* independent worlds in the batch                 */
+    double timestep;            /* World::timestep (World.hpp:97)                  */
+    int32_t substeps;           /* World::substeps (World.hpp:98)                  */
+    int32_t precision;          /* RBPS_PRECISION_*                                */
+    int32_t solve_mode;         /* RBPS_SOLVE_*                                    */
+    double fat_margin;          /* BroadPhaseConfig::fat_margin (BroadPhase.hpp:116)        */
+    double reinsert_threshold;  /* BroadPhaseConfig::reinsert_threshold (BroadPhase.hpp:124) */
+    int32_t use_velocity_expansion; /* CollisionPipelineConfig (CollisionPipeline.hpp:146-154) */
+    int32_t device;             /* CUDA device ordinal                             */
+    void *stream;               /* cudaStream_t, NULL = the library's own stream   */
+    uint32_t max_pairs_per_world;   /* broadphase pair capacity per world, 0 = automatic */
+    uint32_t block_threads;     /* threads per world-CTA, 0 = automatic (autotuned)  */
+} rbps_batch_desc;
+
+/* Mirrors rbps::BodyParams (BodyAPI.hpp:22-31).  inertia = {xx,yy,zz,xy,xz,yz}
+ * (m3d::smat3 field order), orientation = {w,x,y,z}.  As in create_body
+ * (BodyAPI.hpp:61) the body's force defaults to (0, -9.8f*mass, 0). */
+typedef struct rbps_body_desc {
+    int32_t type;
+    double mass;
+    double inertia[6];
+    double position[3];
+    double orientation[4];
+    double linear_velocity[3];
+    double angular_velocity[3];
+} rbps_body_desc;
+
+/* Mirrors rbps::ColliderParams (ColliderAPI.hpp:17-27).
+ *   sphere : params = {radius}
+ *   box    : params = {hx, hy, hz}
+ *   capsule: params = {half_height, radius}   (segment along local Y)
+ *   plane  : params = {nx, ny, nz, d}         (normal . x = d)
+ *   hull   : hull = id returned by rbps_hull_create */
+typedef struct rbps_collider_desc {
+    int32_t shape;
+    double params[4];
+    uint32_t hull;
+    uint32_t body_id;
+    int32_t is_static;
+    double local_pos[3];
+    double local_rot[4];
+    double restitution;
+    double static_friction;
+    double dynamic_friction;
+} rbps_collider_desc;
+
+/* Mirrors Prismatic/Revolute/FixedJointParams (JointAPI.hpp:24-57).
+ * axis = moving_axis (prismatic) or aligned_axis (revolute). */
+typedef struct rbps_joint_desc {
+    int32_t type;
+    uint32_t body_1;
+    uint32_t body_2;
+    double axis[3];
+    double limit_axis[3];
+    double r_1[3];
+    double r_2[3];
+    int32_t actuation;
+    double compliance;
+    double damping;
+    int32_t limited;
+    double lower_limit;
+    double upper_limit;
+    double target_position;
+    double target_speed;
+} rbps_joint_desc;
+
+/* Host views of body state (length n bodies each; NULL fields are skipped). */
+typedef struct rbps_state_view {
+    double *position;          /* 3n */
+    double *orientation;       /* 4n, w,x,y,z */
+    double *linear_velocity;   /* 3n */
+    double *angular_velocity;  /* 3n */
+} rbps_state_view;
+
+/* One row of the reference ContactList (CollisionPipeline.hpp:46-82) as
+ * produced by the last narrowphase pass of the last step. */
+typedef struct rbps_contact {
+    uint32_t body_a, body_b, collider_a, collider_b;
+    double normal[3];
+    double r_a_local[3];
+    double r_b_local[3];
+    double point_on_a[3];
+    double point_on_b[3];
+    double penetration_depth;
+    double normal_lambda;
+    double tangent_lambda;
+    double relative_velocity;
+    double restitution, static_friction, dynamic_friction;
+    int32_t collision;
+    int32_t pad_;
+} rbps_contact;
+
+typedef struct rbps_stats {
+    uint64_t steps;            /* steps run since commit                        */
+    uint64_t pairs;            /* SAP pairs of the last step, all worlds         */
+    uint64_t candidates;       /* narrowphase candidates (pairs + plane tests)   */
+    uint64_t contacts;         /* contact points of the last substep             */
+    uint32_t max_colors;       /* largest colour count of any world, last step   */
+    uint32_t serial_overflow;  /* pairs that needed the serial fallback colour   */
+    int32_t device_error;      /* last device error word (RBPS_ERR_* or 0)       */
+    uint32_t pad_;
+    uint64_t kernel_launches;  /* kernels launched by the last rbps_batch_step  */
+} rbps_stats;
+
+typedef struct rbps_batch rbps_batch;
+
+/* ---------------------------------------------------------------- batch */
+RBPS_API void rbps_batch_desc_default(rbps_batch_desc *desc);
+RBPS_API void rbps_body_desc_default(rbps_body_desc *desc);      /* BodyParams{} */
+RBPS_API void rbps_collider_desc_default(rbps_collider_desc *desc); /* ColliderParams{} */
+RBPS_API void rbps_joint_desc_default(rbps_joint_desc *desc, int32_t type);
+
+/* Replaces World::World(timestep, substeps) (World.hpp:103) for n worlds. */
+RBPS_API int rbps_batch_create(const rbps_batch_desc *desc, rbps_batch **out);
+RBPS_API int rbps_batch_destroy(rbps_batch *batch);
+
+/* Convex hull from CCW triangles, like convex_hull_data_create
+ * (ConvexHull.hpp:126-420); the data is copied.  verts = 3*n_verts doubles. */
+RBPS_API int rbps_hull_create(rbps_batch *batch, const double *verts, uint32_t n_verts,
+                              const uint32_t *tris, uint32_t n_tris, uint32_t *hull_id);
+/* Quickhull helper (the reference ships no hull builder, ConvexHull.hpp:29-33):
+ * CCW outward triangles of the convex hull of n points.  Writes at most
+ * tri_cap triangles; *n_tris receives the count. */
+RBPS_API int rbps_quickhull(const double *points, uint32_t n_points,
+                            uint32_t *tris, uint32_t tri_cap, uint32_t *n_tris);
+
+/* Replaces World::create_body (World.hpp:113 -> BodyAPI.hpp:53-80). */
+RBPS_API int rbps_world_add_body(rbps_batch *batch, uint32_t world,
+                                 const rbps_body_desc *desc, uint32_t *id_out);
+/* Bulk form: n bodies, ids first_id .. first_id+n-1. */
+RBPS_API int rbps_world_add_bodies(rbps_batch *batch, uint32_t world, uint32_t n,
+                                   const rbps_body_desc *descs, uint32_t *first_id);
+/* Writes bodies.force / bodies.torque (Body.hpp BODY_FIELDS) of one body. */
+RBPS_API int rbps_world_set_body_force(rbps_batch *batch, uint32_t world, uint32_t body,
+                                       const double force[3], const double torque[3]);
+/* Replaces World::create_collider (World.hpp:124-132 -> ColliderAPI.hpp:61-91). */
+RBPS_API int rbps_world_add_collider(rbps_batch *batch, uint32_t world,
+                                     const rbps_collider_desc *desc, uint32_t *id_out);
+RBPS_API int rbps_world_add_colliders(rbps_batch *batch, uint32_t world, uint32_t n,
+                                      const rbps_collider_desc *descs, uint32_t *first_id);
+/* Replaces World::create_{prismatic,revolute,fixed}_joint (World.hpp:141-156). */
+RBPS_API int rbps_world_add_joint(rbps_batch *batch, uint32_t world,
+                                  const rbps_joint_desc *desc, uint32_t *id_out);
+
+/* Uploads every world, builds offsets, the initial SAP state (the
+ * broad_phase_insert of each collider, BroadPhase.cpp:169-197), plane
+ * candidate lists and joint colouring.  No adds are allowed afterwards. */
+RBPS_API int rbps_batch_commit(rbps_batch *batch);
+
+/* Replaces World::step (World.hpp:192-212), n_steps times, on every world.
+ * Asynchronous on the batch stream; device errors surface at the next
+ * rbps_batch_synchronize / get_* call. */
+RBPS_API int rbps_batch_step(rbps_batch *batch, int32_t n_steps);
+RBPS_API int rbps_batch_synchronize(rbps_batch *batch);
+
+/* Per-world body state, host doubles (converted from the device precision). */
+RBPS_API int rbps_batch_get_state(rbps_batch *batch, uint32_t world, const rbps_state_view *view);
+RBPS_API int rbps_batch_set_state(rbps_batch *batch, uint32_t world, const rbps_state_view *view);
+/* All worlds at once: bodies in world order (world 0 bodies, world 1 bodies, ...). */
+RBPS_API int rbps_batch_get_state_all(rbps_batch *batch, const rbps_state_view *view);
+/* Per-body force (3 doubles each) for all worlds, copied host -> device. */
+RBPS_API int rbps_batch_set_forces_all(rbps_batch *batch, const double *force);
+RBPS_API int rbps_batch_body_count(rbps_batch *batch, uint32_t world, uint32_t *n_bodies);
+RBPS_API int rbps_batch_total_bodies(rbps_batch *batch, uint64_t *n_bodies, uint64_t *n_dynamic);
+
+/* Parity dumps (enable before stepping; they cost extra device copies). */
+RBPS_API int rbps_batch_set_dump(rbps_batch *batch, int32_t enable);
+/* BroadPhaseState::pairs of the last step (BroadPhase.hpp:141), as
+ * (id_a, id_b) uint32 pairs in emission order. */
+RBPS_API int rbps_batch_get_pairs(rbps_batch *batch, uint32_t world, uint32_t *pairs,
+                                  uint32_t cap, uint32_t *n_out);
+/* ContactList of the last substep of the last step, in list order. */
+RBPS_API int rbps_batch_get_contacts(rbps_batch *batch, uint32_t world, rbps_contact *out,
+                                     uint32_t cap, uint32_t *n_out);
+/* Colour of every narrowphase candidate of the last step (colored mode);
+ * candidates in list order (SAP pairs, then plane tests); bodies of each. */
+RBPS_API int rbps_batch_get_colors(rbps_batch *batch, uint32_t world, uint32_t *colors,
+                                   uint32_t *body_a, uint32_t *body_b, uint32_t cap,
+                                   uint32_t *n_out);
+RBPS_API int rbps_batch_get_stats(rbps_batch *batch, rbps_stats *stats);
+/* Persistent SAP state of one world, as the reference BroadPhaseState holds
+ * it (BroadPhase.hpp:88-143): fat AABB of each SAP object (6 doubles; object
+ * order = collider order, planes skipped) and the endpoint list in its
+ * current order as (object*2 + is_max) with the float values.  Any pointer
+ * may be NULL; *n_objects receives the object count. */
+RBPS_API int rbps_batch_get_sap_state(rbps_batch *batch, uint32_t world, double *fat, uint32_t *ep_ids,
+                                      float *ep_values, uint32_t *n_objects);
+
+/* ------------------------------------------------- standalone broadphase
+ * GPU drop-in for the rbc SAP API (rbc/BroadPhase.hpp:151-260): objects are
+ * inserted / moved on the host exactly as in the reference, and
+ * rbps_bp_update runs the sort and sweep on the device.  Pairs come back in
+ * the reference emission order. */
+typedef struct rbps_bp rbps_bp;
+RBPS_API int rbps_bp_create(double fat_margin, double reinsert_threshold, rbps_bp **out);
+RBPS_API int rbps_bp_destroy(rbps_bp *bp);
+/* aabb = {min.x,min.y,min.z,max.x,max.y,max.z} */
+RBPS_API int rbps_bp_insert(rbps_bp *bp, uint32_t user_id, const double aabb[6], uint32_t *handle);
+RBPS_API int rbps_bp_remove(rbps_bp *bp, uint32_t handle);
+RBPS_API int rbps_bp_move(rbps_bp *bp, uint32_t handle, const double aabb[6]);
+RBPS_API int rbps_bp_move_swept(rbps_bp *bp, uint32_t handle, const double aabb[6],
+                                const double linear_velocity[3], double dt);
+RBPS_API int rbps_bp_update(rbps_bp *bp);
+RBPS_API int rbps_bp_get_pairs(rbps_bp *bp, uint32_t *pairs, uint32_t cap, uint32_t *n_out);
+RBPS_API int rbps_bp_get_fat_aabb(rbps_bp *bp, uint32_t handle, double aabb[6]);
+/* Runs the sort + sweep on one CTA of block_threads threads instead of a
+ * cooperative grid (cheaper for small object counts). */
+RBPS_API int rbps_bp_configure(rbps_bp *bp, int32_t single_cta, int32_t block_threads);
+
+/* ------------------------------------------------------------ self tests
+ * Self-checking runs of the device primitives every step phase is built on:
+ * a stable radix sort of keys (values = original positions) by their low
+ * `bits` bits, and an exclusive scan, on one CTA (grid = 0) or a cooperative
+ * grid (grid = 1) of block_threads threads per CTA. */
+RBPS_API int rbps_selftest_sort(const uint32_t *keys, uint32_t n, int32_t bits, int32_t grid,
+                                int32_t block_threads, uint32_t *keys_out, uint32_t *vals_out);
+RBPS_API int rbps_selftest_scan(const uint32_t *in, uint32_t n, int32_t grid, int32_t block_threads,
+                                uint32_t *out, uint32_t *total);
+
+/* ------------------------------------------------------------- errors */
+RBPS_API int rbps_last_error(char *buf, size_t size);
+RBPS_API const char *rbps_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBPS_GPU_H */

@@ -1,0 +1,205 @@
+"""ctypes binding of the oracle: the unmodified reference engine built from
+its own sources into oracle/_ref/librbps_ref.so (see oracle/Makefile).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker.  The product never imports it.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from rbps_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "librbps_ref.so")
+_lib = None
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_U = C.POINTER(C.c_uint32)
+
+
+def available():
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError(f"oracle library missing: {LIB_PATH} (run `make -C oracle`)")
+        L = C.CDLL(LIB_PATH)
+        L.ref_world_create.restype = _P
+        L.ref_world_create.argtypes = [C.c_double, C.c_int, C.c_double, C.c_double]
+        L.ref_world_destroy.argtypes = [_P]
+        L.ref_hull_create.restype = C.c_uint32
+        L.ref_hull_create.argtypes = [_P, _D, C.c_uint32, _U, C.c_uint32]
+        L.ref_add_body.restype = C.c_uint32
+        L.ref_add_body.argtypes = [_P, _P]
+        L.ref_set_body_force.argtypes = [_P, C.c_uint32, _D, _D]
+        L.ref_add_collider.restype = C.c_uint32
+        L.ref_add_collider.argtypes = [_P, _P]
+        L.ref_add_joint.restype = C.c_uint32
+        L.ref_add_joint.argtypes = [_P, _P]
+        L.ref_step.argtypes = [_P, C.c_int]
+        L.ref_body_count.restype = C.c_uint32
+        L.ref_body_count.argtypes = [_P]
+        L.ref_get_state.argtypes = [_P, _D, _D, _D, _D]
+        L.ref_set_state.argtypes = [_P, _D, _D, _D, _D]
+        L.ref_get_pairs.restype = C.c_uint32
+        L.ref_get_pairs.argtypes = [_P, _U, C.c_uint32]
+        L.ref_get_contacts.restype = C.c_uint32
+        L.ref_get_contacts.argtypes = [_P, _P, C.c_uint32]
+        L.ref_get_sap_state.restype = C.c_uint32
+        L.ref_get_sap_state.argtypes = [_P, _D, _U, C.POINTER(C.c_float)]
+        L.ref_collision_groups.restype = C.c_uint32
+        L.ref_collision_groups.argtypes = [_P, _U, C.c_uint32]
+        L.ref_step_worlds.restype = C.c_double
+        L.ref_step_worlds.argtypes = [C.POINTER(_P), C.c_uint32, C.c_int, C.c_int]
+        L.ref_bp_create.restype = _P
+        L.ref_bp_create.argtypes = [C.c_double, C.c_double]
+        L.ref_bp_destroy.argtypes = [_P]
+        L.ref_bp_insert.restype = C.c_uint32
+        L.ref_bp_insert.argtypes = [_P, C.c_uint32, _D]
+        L.ref_bp_remove.argtypes = [_P, C.c_uint32]
+        L.ref_bp_move.argtypes = [_P, C.c_uint32, _D]
+        L.ref_bp_move_swept.argtypes = [_P, C.c_uint32, _D, _D, C.c_double]
+        L.ref_bp_update.argtypes = [_P]
+        L.ref_bp_get_pairs.restype = C.c_uint32
+        L.ref_bp_get_pairs.argtypes = [_P, _U, C.c_uint32]
+        L.ref_bp_get_fat_aabb.argtypes = [_P, C.c_uint32, _D]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+class RefWorld:
+    """One reference rbps::World built from a scenes.WorldSpec."""
+
+    def __init__(self, spec, timestep, substeps, fat_margin=0.1, reinsert_threshold=0.05):
+        L = lib()
+        self.h = L.ref_world_create(timestep, substeps, fat_margin, reinsert_threshold)
+        for verts, tris in spec.hulls:
+            v = np.ascontiguousarray(verts, np.float64)
+            t = np.ascontiguousarray(tris, np.uint32)
+            L.ref_hull_create(self.h, _dp(v), len(v), t.ctypes.data_as(_U), len(t))
+        bodies = np.ascontiguousarray(spec.bodies)
+        for i in range(len(bodies)):
+            L.ref_add_body(self.h, C.c_void_p(bodies.ctypes.data + i * bodies.itemsize))
+        forces = np.ascontiguousarray(spec.forces, np.float64)
+        for i in range(len(bodies)):
+            L.ref_set_body_force(self.h, i, _dp(forces[i]), None)
+        cols = np.ascontiguousarray(spec.colliders)
+        for i in range(len(cols)):
+            L.ref_add_collider(self.h, C.c_void_p(cols.ctypes.data + i * cols.itemsize))
+        joints = np.ascontiguousarray(spec.joints)
+        for i in range(len(joints)):
+            L.ref_add_joint(self.h, C.c_void_p(joints.ctypes.data + i * joints.itemsize))
+        self.n = L.ref_body_count(self.h)
+
+    def close(self):
+        if self.h:
+            lib().ref_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        lib().ref_step(self.h, n)
+
+    def state(self):
+        n = self.n
+        pos, quat = np.zeros((n, 3)), np.zeros((n, 4))
+        vel, omega = np.zeros((n, 3)), np.zeros((n, 3))
+        lib().ref_get_state(self.h, _dp(pos), _dp(quat), _dp(vel), _dp(omega))
+        return {"position": pos, "orientation": quat, "linear_velocity": vel, "angular_velocity": omega}
+
+    def set_state(self, st):
+        a = {k: np.ascontiguousarray(v, np.float64) for k, v in st.items()}
+        lib().ref_set_state(self.h, _dp(a["position"]), _dp(a["orientation"]),
+                            _dp(a["linear_velocity"]), _dp(a["angular_velocity"]))
+
+    def pairs(self):
+        L = lib()
+        n = L.ref_get_pairs(self.h, None, 0)
+        out = np.zeros((max(n, 1), 2), np.uint32)
+        L.ref_get_pairs(self.h, out.ctypes.data_as(_U), n)
+        return out[:n]
+
+    def contacts(self):
+        L = lib()
+        n = L.ref_get_contacts(self.h, None, 0)
+        out = np.zeros(max(n, 1), abi.CONTACT_DT)
+        L.ref_get_contacts(self.h, C.c_void_p(out.ctypes.data), n)
+        return out[:n]
+
+    def sap_state(self):
+        L = lib()
+        n = L.ref_get_sap_state(self.h, None, None, None)
+        fat = np.zeros((max(n, 1), 6))
+        ids = np.zeros(max(2 * n, 1), np.uint32)
+        vals = np.zeros(max(2 * n, 1), np.float32)
+        L.ref_get_sap_state(self.h, _dp(fat), ids.ctypes.data_as(_U), vals.ctypes.data_as(C.POINTER(C.c_float)))
+        return fat[:n], ids[:2 * n], vals[:2 * n]
+
+    def collision_groups(self):
+        c = self.contacts()
+        colors = np.zeros(max(len(c), 1), np.uint32)
+        ng = lib().ref_collision_groups(self.h, colors.ctypes.data_as(_U), len(c))
+        return colors[:len(c)], ng
+
+
+def step_worlds(worlds, steps, threads):
+    """Steps every RefWorld `steps` times on `threads` host threads; returns
+    wall seconds."""
+    arr = (_P * len(worlds))(*[w.h for w in worlds])
+    return lib().ref_step_worlds(arr, len(worlds), steps, threads)
+
+
+class RefBroadPhase:
+    """The reference rbc SAP broadphase (BroadPhase.cpp), unmodified."""
+
+    def __init__(self, fat_margin=0.1, reinsert_threshold=0.05):
+        self.h = lib().ref_bp_create(fat_margin, reinsert_threshold)
+
+    def __del__(self):
+        try:
+            lib().ref_bp_destroy(self.h)
+        except Exception:
+            pass
+
+    def insert(self, user_id, aabb):
+        return lib().ref_bp_insert(self.h, user_id, _dp(np.asarray(aabb, np.float64)))
+
+    def remove(self, handle):
+        lib().ref_bp_remove(self.h, handle)
+
+    def move(self, handle, aabb):
+        lib().ref_bp_move(self.h, handle, _dp(np.asarray(aabb, np.float64)))
+
+    def move_swept(self, handle, aabb, vel, dt):
+        lib().ref_bp_move_swept(self.h, handle, _dp(np.asarray(aabb, np.float64)),
+                                _dp(np.asarray(vel, np.float64)), dt)
+
+    def update(self):
+        lib().ref_bp_update(self.h)
+
+    def pairs(self):
+        L = lib()
+        n = L.ref_bp_get_pairs(self.h, None, 0)
+        out = np.zeros((max(n, 1), 2), np.uint32)
+        L.ref_bp_get_pairs(self.h, out.ctypes.data_as(_U), n)
+        return out[:n]
+
+    def fat_aabb(self, handle):
+        out = np.zeros(6)
+        lib().ref_bp_get_fat_aabb(self.h, handle, _dp(out))
+        return out

@@ -1,0 +1,347 @@
+// ref_harness.cpp - TEST INFRASTRUCTURE ONLY (the oracle).
+//
+// A thin extern "C" shim around the UNMODIFIED reference engine
+// (rbps::World, include/rbps/API/World.hpp:87-213, and the rbc SAP
+// broadphase, include/rbc/BroadPhase.hpp:151-260), compiled from the
+// reference's own sources by oracle/Makefile into oracle/_ref/librbps_ref.so.
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
+// it; the product library never links or calls it.
+//
+// It takes the same descriptor structs as the product C ABI (rbps_gpu.h) so a
+// parity test builds the identical scene in both engines.
+
+#include "rbps/API/World.hpp"
+#include "rbc/BroadPhase.hpp"
+#include "rbps_gpu.h"
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+namespace
+{
+    struct HullStore
+    {
+        std::vector<m3d::vec3> verts;
+        std::vector<uint32_t> tris;
+        rbc::ConvexHullData *data = nullptr;
+        ~HullStore() { rbc::convex_hull_data_destroy(data); }
+    };
+
+    struct RefWorld
+    {
+        rbps::World w;
+        std::vector<std::unique_ptr<HullStore>> hulls;
+        RefWorld(double dt, int substeps) : w(dt, substeps) {}
+    };
+
+    m3d::vec3 v3(const double *p) { return m3d::vec3(p[0], p[1], p[2]); }
+    m3d::quat q4(const double *p) { return m3d::quat(p[0], p[1], p[2], p[3]); }
+    void put3(double *o, const m3d::vec3 &v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
+    void put4(double *o, const m3d::quat &q) { o[0] = q.w; o[1] = q.x; o[2] = q.y; o[3] = q.z; }
+    void aabb_in(const double *a, rbc::AABB &out)
+    {
+        out.min = m3d::vec3(a[0], a[1], a[2]);
+        out.max = m3d::vec3(a[3], a[4], a[5]);
+    }
+} // namespace
+
+extern "C"
+{
+    void *ref_world_create(double timestep, int substeps, double fat_margin, double reinsert_threshold)
+    {
+        auto *rw = new RefWorld(timestep, substeps);
+        rbc::BroadPhaseConfig cfg;
+        cfg.fat_margin = fat_margin;
+        cfg.reinsert_threshold = reinsert_threshold;
+        rbc::broad_phase_init(rw->w.broad_phase_state, cfg);
+        return rw;
+    }
+
+    void ref_world_destroy(void *h) { delete static_cast<RefWorld *>(h); }
+
+    uint32_t ref_hull_create(void *h, const double *verts, uint32_t n_verts,
+                             const uint32_t *tris, uint32_t n_tris)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        auto hs = std::make_unique<HullStore>();
+        hs->verts.resize(n_verts);
+        for (uint32_t i = 0; i < n_verts; ++i)
+            hs->verts[i] = v3(verts + 3 * i);
+        hs->tris.assign(tris, tris + 3 * n_tris);
+        hs->data = rbc::convex_hull_data_create(hs->verts.data(), n_verts,
+                                                hs->tris.data(), n_tris);
+        rw->hulls.push_back(std::move(hs));
+        return static_cast<uint32_t>(rw->hulls.size() - 1);
+    }
+
+    uint32_t ref_add_body(void *h, const rbps_body_desc *d)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        rbps::BodyParams p;
+        p.type = d->type == RBPS_BODY_STATIC ? rbps::STATIC : rbps::DYNAMIC;
+        p.mass = d->mass;
+        p.inertia_tensor = m3d::smat3(d->inertia[0], d->inertia[1], d->inertia[2],
+                                      d->inertia[3], d->inertia[4], d->inertia[5]);
+        p.position = v3(d->position);
+        p.orientation = q4(d->orientation);
+        p.linear_velocity = v3(d->linear_velocity);
+        p.angular_velocity = v3(d->angular_velocity);
+        return rw->w.create_body(p);
+    }
+
+    void ref_set_body_force(void *h, uint32_t body, const double *force, const double *torque)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        const uint32_t i = rw->w.bodies.index_of(body);
+        if (force)
+            rw->w.bodies.force[i] = v3(force);
+        if (torque)
+            rw->w.bodies.torque[i] = v3(torque);
+    }
+
+    uint32_t ref_add_collider(void *h, const rbps_collider_desc *d)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        rbps::ColliderParams p;
+        switch (d->shape)
+        {
+        case RBPS_SHAPE_SPHERE: p.shape = rbc::Sphere(d->params[0]); break;
+        case RBPS_SHAPE_BOX: p.shape = rbc::Box(v3(d->params)); break;
+        case RBPS_SHAPE_CAPSULE: p.shape = rbc::Capsule(d->params[0], d->params[1]); break;
+        case RBPS_SHAPE_PLANE: p.shape = rbc::Plane(v3(d->params), d->params[3]); break;
+        case RBPS_SHAPE_CONVEX_HULL: p.shape = rbc::ConvexHull(rw->hulls.at(d->hull)->data); break;
+        default: return UINT32_MAX;
+        }
+        p.body_id = d->body_id;
+        p.is_static = d->is_static != 0;
+        p.local_pos = v3(d->local_pos);
+        p.local_rot = q4(d->local_rot);
+        p.restitution = d->restitution;
+        p.static_friction = d->static_friction;
+        p.dynamic_friction = d->dynamic_friction;
+        return rw->w.create_collider(p);
+    }
+
+    uint32_t ref_add_joint(void *h, const rbps_joint_desc *d)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        uint32_t id = UINT32_MAX;
+        const auto act = static_cast<rbps::JointActuationType>(d->actuation);
+        if (d->type == RBPS_JOINT_REVOLUTE)
+        {
+            rbps::RevoluteJointParams p;
+            p.body_1 = d->body_1; p.body_2 = d->body_2;
+            p.aligned_axis = v3(d->axis); p.limit_axis = v3(d->limit_axis);
+            p.r_1 = v3(d->r_1); p.r_2 = v3(d->r_2);
+            p.actuation_type = act; p.compliance = d->compliance; p.damping = d->damping;
+            p.limited = d->limited != 0; p.lower_limit = d->lower_limit; p.upper_limit = d->upper_limit;
+            id = rw->w.create_revolute_joint(p);
+        }
+        else if (d->type == RBPS_JOINT_PRISMATIC)
+        {
+            rbps::PrismaticJointParams p;
+            p.body_1 = d->body_1; p.body_2 = d->body_2;
+            p.moving_axis = v3(d->axis);
+            p.r_1 = v3(d->r_1); p.r_2 = v3(d->r_2);
+            p.actuation_type = act; p.compliance = d->compliance; p.damping = d->damping;
+            p.limited = d->limited != 0; p.lower_limit = d->lower_limit; p.upper_limit = d->upper_limit;
+            id = rw->w.create_prismatic_joint(p);
+        }
+        else if (d->type == RBPS_JOINT_FIXED)
+        {
+            rbps::FixedJointParams p;
+            p.body_1 = d->body_1; p.body_2 = d->body_2;
+            p.r_1 = v3(d->r_1); p.r_2 = v3(d->r_2);
+            id = rw->w.create_fixed_joint(p);
+        }
+        if (id != UINT32_MAX)
+        {
+            const uint32_t j = rw->w.joints.index_of(id);
+            rw->w.joints.target_position[j] = d->target_position;
+            rw->w.joints.target_speed[j] = d->target_speed;
+        }
+        return id;
+    }
+
+    void ref_step(void *h, int n)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        for (int i = 0; i < n; ++i)
+            rw->w.step();
+    }
+
+    uint32_t ref_body_count(void *h) { return static_cast<RefWorld *>(h)->w.bodies.count(); }
+
+    void ref_get_state(void *h, double *pos, double *quat, double *vel, double *omega)
+    {
+        auto &b = static_cast<RefWorld *>(h)->w.bodies;
+        for (uint32_t i = 0; i < b.count(); ++i)
+        {
+            if (pos) put3(pos + 3 * i, b.position[i]);
+            if (quat) put4(quat + 4 * i, b.orientation[i]);
+            if (vel) put3(vel + 3 * i, b.linear_velocity[i]);
+            if (omega) put3(omega + 3 * i, b.angular_velocity[i]);
+        }
+    }
+
+    void ref_set_state(void *h, const double *pos, const double *quat, const double *vel, const double *omega)
+    {
+        auto &b = static_cast<RefWorld *>(h)->w.bodies;
+        for (uint32_t i = 0; i < b.count(); ++i)
+        {
+            if (pos) b.position[i] = v3(pos + 3 * i);
+            if (quat) b.orientation[i] = q4(quat + 4 * i);
+            if (vel) b.linear_velocity[i] = v3(vel + 3 * i);
+            if (omega) b.angular_velocity[i] = v3(omega + 3 * i);
+        }
+    }
+
+    uint32_t ref_get_pairs(void *h, uint32_t *out, uint32_t cap)
+    {
+        const auto &pairs = static_cast<RefWorld *>(h)->w.broad_phase_state.pairs;
+        const uint32_t n = static_cast<uint32_t>(pairs.size());
+        for (uint32_t i = 0; i < n && i < cap; ++i)
+        {
+            out[2 * i] = pairs[i].id_a;
+            out[2 * i + 1] = pairs[i].id_b;
+        }
+        return n;
+    }
+
+    uint32_t ref_get_contacts(void *h, rbps_contact *out, uint32_t cap)
+    {
+        const auto &c = static_cast<RefWorld *>(h)->w.contacts;
+        const uint32_t n = c.n_contacts;
+        for (uint32_t i = 0; i < n && i < cap; ++i)
+        {
+            rbps_contact &o = out[i];
+            std::memset(&o, 0, sizeof(o));
+            o.body_a = c.body_a[i]; o.body_b = c.body_b[i];
+            o.collider_a = c.collider_a[i]; o.collider_b = c.collider_b[i];
+            put3(o.normal, c.normal[i]);
+            put3(o.r_a_local, c.r_a_local[i]);
+            put3(o.r_b_local, c.r_b_local[i]);
+            put3(o.point_on_a, c.point_on_a[i]);
+            put3(o.point_on_b, c.point_on_b[i]);
+            o.penetration_depth = c.penetration_depth[i];
+            o.normal_lambda = c.normal_lambda[i];
+            o.tangent_lambda = c.tangent_lambda[i];
+            o.relative_velocity = c.relative_velocity[i];
+            o.restitution = c.restitution[i];
+            o.static_friction = c.static_friction[i];
+            o.dynamic_friction = c.dynamic_friction[i];
+            o.collision = c.collision[i] ? 1 : 0;
+        }
+        return n;
+    }
+
+    // BroadPhaseState of the world: fat AABB per object slot and the endpoint
+    // list as (slot*2 + is_max) with values; returns the object count.
+    uint32_t ref_get_sap_state(void *h, double *fat, uint32_t *ep_ids, float *ep_values)
+    {
+        const auto &bp = static_cast<RefWorld *>(h)->w.broad_phase_state;
+        for (size_t o = 0; o < bp.objects.size(); ++o)
+            if (fat)
+            {
+                put3(fat + 6 * o, bp.objects[o].fat_aabb.min);
+                put3(fat + 6 * o + 3, bp.objects[o].fat_aabb.max);
+            }
+        for (size_t i = 0; i < bp.endpoints.size(); ++i)
+        {
+            if (ep_ids)
+                ep_ids[i] = 2u * bp.endpoints[i].slot + bp.endpoints[i].is_max;
+            if (ep_values)
+                ep_values[i] = bp.endpoints[i].value;
+        }
+        return static_cast<uint32_t>(bp.objects.size());
+    }
+
+    // Colouring of the current ContactList by the reference's own
+    // get_collision_groups (CollisionPipeline.cpp:223-293): writes the colour
+    // of each contact and returns the number of groups.
+    uint32_t ref_collision_groups(void *h, uint32_t *color_of_contact, uint32_t cap)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        auto groups = rbps::get_collision_groups(rw->w.contacts, rw->w.bodies);
+        for (uint32_t g = 0; g < groups.size(); ++g)
+            for (uint32_t c : groups[g])
+                if (c < cap)
+                    color_of_contact[c] = g;
+        return static_cast<uint32_t>(groups.size());
+    }
+
+    // CPU baseline: steps n independent worlds `steps` times on `threads`
+    // host threads (one World per thread at a time; worlds share no state)
+    // and returns the wall-clock seconds.
+    double ref_step_worlds(void **worlds, uint32_t n, int steps, int threads)
+    {
+        if (threads < 1)
+            threads = 1;
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; ++t)
+            pool.emplace_back([=]() {
+                for (uint32_t i = t; i < n; i += threads)
+                    ref_step(worlds[i], steps);
+            });
+        for (auto &th : pool)
+            th.join();
+        const auto t1 = std::chrono::steady_clock::now();
+        return std::chrono::duration<double>(t1 - t0).count();
+    }
+
+    // ---- the rbc SAP broadphase, unmodified (BroadPhase.cpp:160-245) ----
+    void *ref_bp_create(double fat_margin, double reinsert_threshold)
+    {
+        auto *bp = new rbc::BroadPhaseState();
+        rbc::BroadPhaseConfig cfg;
+        cfg.fat_margin = fat_margin;
+        cfg.reinsert_threshold = reinsert_threshold;
+        rbc::broad_phase_init(*bp, cfg);
+        return bp;
+    }
+    void ref_bp_destroy(void *h) { delete static_cast<rbc::BroadPhaseState *>(h); }
+    uint32_t ref_bp_insert(void *h, uint32_t user_id, const double *aabb)
+    {
+        rbc::AABB a;
+        aabb_in(aabb, a);
+        return rbc::broad_phase_insert(*static_cast<rbc::BroadPhaseState *>(h), user_id, a);
+    }
+    void ref_bp_remove(void *h, uint32_t handle)
+    {
+        rbc::broad_phase_remove(*static_cast<rbc::BroadPhaseState *>(h), handle);
+    }
+    void ref_bp_move(void *h, uint32_t handle, const double *aabb)
+    {
+        rbc::AABB a;
+        aabb_in(aabb, a);
+        rbc::broad_phase_move(*static_cast<rbc::BroadPhaseState *>(h), handle, a);
+    }
+    void ref_bp_move_swept(void *h, uint32_t handle, const double *aabb, const double *vel, double dt)
+    {
+        rbc::AABB a;
+        aabb_in(aabb, a);
+        rbc::broad_phase_move_swept(*static_cast<rbc::BroadPhaseState *>(h), handle, a, v3(vel), dt);
+    }
+    void ref_bp_update(void *h) { rbc::broad_phase_update(*static_cast<rbc::BroadPhaseState *>(h)); }
+    uint32_t ref_bp_get_pairs(void *h, uint32_t *out, uint32_t cap)
+    {
+        const auto &pairs = static_cast<rbc::BroadPhaseState *>(h)->pairs;
+        const uint32_t n = static_cast<uint32_t>(pairs.size());
+        for (uint32_t i = 0; i < n && i < cap; ++i)
+        {
+            out[2 * i] = pairs[i].id_a;
+            out[2 * i + 1] = pairs[i].id_b;
+        }
+        return n;
+    }
+    void ref_bp_get_fat_aabb(void *h, uint32_t handle, double *aabb)
+    {
+        const auto &o = static_cast<rbc::BroadPhaseState *>(h)->objects.at(handle);
+        put3(aabb, o.fat_aabb.min);
+        put3(aabb + 3, o.fat_aabb.max);
+    }
+}

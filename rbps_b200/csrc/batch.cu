@@ -1,0 +1,1451 @@
+// batch.cu - host driver and C ABI (include/rbps_gpu.h) of the batched
+// engine: scene building, upload, per-step launches and state readback.
+//
+// The setup surface mirrors rbps::World (include/rbps/API/World.hpp:87-213):
+// create_body (BodyAPI.hpp:53-80), create_collider with the initial
+// broad_phase_insert (ColliderAPI.hpp:61-91, BroadPhase.cpp:169-197),
+// create_{prismatic,revolute,fixed}_joint (JointAPI.hpp:191-267).  Host-side
+// arithmetic that must round like the reference (inverse inertia, initial fat
+// AABBs, endpoint keys) uses the shared math headers in double.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine_types.cuh"
+#include "rbps_gpu.h"
+
+using namespace rbps_gpu;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CU(...)                                                                                  \
+    do                                                                                           \
+    {                                                                                            \
+        cudaError_t e_ = (__VA_ARGS__);                                                          \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(RBPS_ERR_CUDA, "%s failed: %s (%s:%d)", #__VA_ARGS__,                    \
+                        cudaGetErrorString(e_), __FILE__, __LINE__);                             \
+    } while (0)
+
+extern "C" int rbps_last_error(char *buf, size_t size)
+{
+    if (buf && size)
+    {
+        std::strncpy(buf, g_last_error.c_str(), size - 1);
+        buf[size - 1] = 0;
+    }
+    return (int)g_last_error.size();
+}
+
+extern "C" const char *rbps_version(void) { return "rbps_b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------- host helpers
+namespace
+{
+    // smat3::inverse (mat3.hpp:248-272)
+    void smat3_inverse(const double *m, double *out)
+    {
+        const double xx = m[0], yy = m[1], zz = m[2], xy = m[3], xz = m[4], yz = m[5];
+        const double det = xx * yy * zz + 2 * xy * xz * yz - xx * yz * yz - yy * xz * xz - zz * xy * xy;
+        if (std::fabs(det) < kEpsilon)
+        {
+            for (int i = 0; i < 6; ++i)
+                out[i] = 0.0;
+            return;
+        }
+        const double inv = 1.0 / det;
+        out[0] = (yy * zz - yz * yz) * inv;
+        out[1] = (xx * zz - xz * xz) * inv;
+        out[2] = (xx * yy - xy * xy) * inv;
+        out[3] = (xz * yz - xy * zz) * inv;
+        out[4] = (xy * yz - xz * yy) * inv;
+        out[5] = (xy * xz - xx * yz) * inv;
+    }
+
+    uint32_t order_key_host(float f)
+    {
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        if ((u & 0x7fffffffu) == 0u)
+            u = 0u;
+        return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    }
+
+    struct HostWorld
+    {
+        std::vector<rbps_body_desc> bodies;
+        std::vector<double> force;  // 3 per body
+        std::vector<double> torque; // 3 per body
+        std::vector<rbps_collider_desc> colliders;
+        std::vector<rbps_joint_desc> joints;
+    };
+
+    struct HostHull
+    {
+        std::vector<double> verts;
+        double aabb[6];
+    };
+
+    struct DevBuf
+    {
+        void *p = nullptr;
+        size_t bytes = 0;
+    };
+
+    size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+} // namespace
+
+struct rbps_batch
+{
+    rbps_batch_desc desc;
+    std::vector<HostWorld> worlds;
+    std::vector<HostHull> hulls;
+    bool committed = false;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 0;
+    int block = 256;
+
+    // device allocations
+    std::vector<void *> allocs;
+    // typed device pointers (as raw bytes; views are built per precision)
+    void *pos = nullptr, *rot = nullptr, *lin = nullptr, *ang = nullptr, *prev_pos = nullptr, *prev_rot = nullptr;
+    void *force = nullptr, *torque = nullptr, *inertia = nullptr, *inv_inertia = nullptr;
+    uint8_t *btype = nullptr;
+    ShapeDev *shape = nullptr;
+    uint32_t *c_body = nullptr;
+    V4<double> *c_lpos = nullptr;
+    Q4<double> *c_lrot = nullptr;
+    uint8_t *c_static = nullptr;
+    void *c_mat = nullptr;
+    double *hull_verts = nullptr;
+    uint32_t *hull_voff = nullptr;
+    double *hull_aabb = nullptr;
+    uint32_t *bp_coll = nullptr;
+    FatBox *fat = nullptr;
+    uint32_t *ep_key = nullptr, *ep_id = nullptr, *ep_pos = nullptr;
+    uint2 *plane_cand = nullptr;
+    void *joints_d = nullptr, *rows_d = nullptr;
+    uint32_t *jorder = nullptr, *jcolor_off = nullptr;
+    WorldDev *worlds_d = nullptr;
+    WorldStats *stats_d = nullptr;
+    int *error_d = nullptr;
+    uint32_t *work_counter = nullptr;
+    uint32_t *small_list = nullptr;
+    char *scratch_small = nullptr, *scratch_big = nullptr;
+
+    // host mirrors
+    std::vector<WorldDev> wdev;
+    std::vector<uint32_t> small_ids, big_ids;
+    ScratchLayout lay_small{}, lay_big{};
+    int grid_small = 0, grid_big = 0;
+    uint64_t total_bodies = 0, total_dynamic = 0;
+    uint32_t n_bodies_all = 0, n_coll_all = 0, n_bp_all = 0, n_joint_all = 0, n_row_all = 0;
+    uint64_t steps_done = 0;
+    uint64_t launches_last = 0;
+
+    // dumps
+    bool dump = false;
+    uint32_t *dump_pairs = nullptr;
+    Cand *dump_cand = nullptr;
+    void *dump_cc = nullptr;
+    uint32_t *dump_color = nullptr;
+    uint32_t dump_pair_cap = 0, dump_cand_cap = 0;
+
+    size_t t_size() const { return desc.precision == RBPS_PRECISION_FP64 ? 8 : 4; }
+    size_t p_size() const { return desc.precision == RBPS_PRECISION_FP32 ? 4 : 8; }
+
+    int alloc(void **p, size_t bytes)
+    {
+        if (bytes == 0)
+            bytes = 16;
+        CU(cudaMalloc(p, bytes));
+        CU(cudaMemset(*p, 0, bytes));
+        allocs.push_back(*p);
+        return RBPS_OK;
+    }
+    template <class X>
+    int upload(X **p, const std::vector<X> &v)
+    {
+        int rc = alloc((void **)p, v.size() * sizeof(X));
+        if (rc)
+            return rc;
+        if (!v.empty())
+            CU(cudaMemcpy(*p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice));
+        return RBPS_OK;
+    }
+    ~rbps_batch()
+    {
+        if (stream)
+            cudaStreamSynchronize(stream);
+        for (void *p : allocs)
+            cudaFree(p);
+        if (own_stream && stream)
+            cudaStreamDestroy(stream);
+    }
+};
+
+// ------------------------------------------------------------ defaults
+extern "C" void rbps_batch_desc_default(rbps_batch_desc *d)
+{
+    std::memset(d, 0, sizeof(*d));
+    d->n_worlds = 1;
+    d->timestep = 1.0 / 60.0;
+    d->substeps = 20;
+    d->precision = RBPS_PRECISION_FP64;
+    d->solve_mode = RBPS_SOLVE_REFERENCE_ORDER;
+    d->fat_margin = 0.1;
+    d->reinsert_threshold = 0.05;
+    d->use_velocity_expansion = 1;
+}
+
+extern "C" void rbps_body_desc_default(rbps_body_desc *d)
+{
+    std::memset(d, 0, sizeof(*d));
+    d->type = RBPS_BODY_DYNAMIC;
+    d->mass = 1.0;
+    d->inertia[0] = d->inertia[1] = d->inertia[2] = 1.0;
+    d->orientation[0] = 1.0;
+}
+
+extern "C" void rbps_collider_desc_default(rbps_collider_desc *d)
+{
+    std::memset(d, 0, sizeof(*d));
+    d->shape = RBPS_SHAPE_SPHERE;
+    d->params[0] = 0.5;
+    d->local_rot[0] = 1.0;
+    d->restitution = 0.5;
+    d->static_friction = 0.5;
+    d->dynamic_friction = 0.5;
+}
+
+extern "C" void rbps_joint_desc_default(rbps_joint_desc *d, int32_t type)
+{
+    std::memset(d, 0, sizeof(*d));
+    d->type = type;
+    d->axis[0] = 1.0;
+    if (type == RBPS_JOINT_REVOLUTE)
+        d->limit_axis[1] = 1.0;
+}
+
+// ------------------------------------------------------------ creation
+extern "C" int rbps_batch_create(const rbps_batch_desc *desc, rbps_batch **out)
+{
+    if (!desc || !out)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_create: null argument");
+    if (desc->n_worlds == 0 || desc->substeps <= 0 || !(desc->timestep > 0.0))
+        return fail(RBPS_ERR_INVALID, "rbps_batch_create: need n_worlds > 0, substeps > 0, timestep > 0");
+    if (desc->precision < 0 || desc->precision > 2 || desc->solve_mode < 0 || desc->solve_mode > 1)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_create: bad precision or solve mode");
+    if (desc->block_threads && (desc->block_threads % 32 || desc->block_threads > 256))
+        return fail(RBPS_ERR_INVALID, "rbps_batch_create: block_threads must be a multiple of 32 and <= 256");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(RBPS_ERR_CUDA, "rbps_batch_create: no CUDA device available");
+    if (desc->device < 0 || desc->device >= ndev)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_create: device %d out of range", desc->device);
+    CU(cudaSetDevice(desc->device));
+    auto b = std::make_unique<rbps_batch>();
+    b->desc = *desc;
+    b->worlds.resize(desc->n_worlds);
+    CU(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, desc->device));
+    if (desc->stream)
+        b->stream = (cudaStream_t)desc->stream;
+    else
+    {
+        CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        b->own_stream = true;
+    }
+    b->block = desc->block_threads ? (int)desc->block_threads : (desc->solve_mode == RBPS_SOLVE_COLORED ? 128 : 128);
+    *out = b.release();
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_destroy(rbps_batch *b)
+{
+    delete b;
+    return RBPS_OK;
+}
+
+static int check_world(rbps_batch *b, uint32_t world, bool adding)
+{
+    if (!b)
+        return fail(RBPS_ERR_INVALID, "null batch");
+    if (world >= b->worlds.size())
+        return fail(RBPS_ERR_INVALID, "world %u out of range (%zu worlds)", world, b->worlds.size());
+    if (adding && b->committed)
+        return fail(RBPS_ERR_INVALID, "batch already committed: no adds after rbps_batch_commit");
+    return RBPS_OK;
+}
+
+extern "C" int rbps_hull_create(rbps_batch *b, const double *verts, uint32_t n_verts, const uint32_t *tris,
+                                uint32_t n_tris, uint32_t *hull_id)
+{
+    if (!b || !verts || n_verts == 0)
+        return fail(RBPS_ERR_INVALID, "rbps_hull_create: need vertices");
+    if (b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_hull_create: batch already committed");
+    (void)tris;
+    (void)n_tris;
+    HostHull h;
+    h.verts.assign(verts, verts + 3 * n_verts);
+    // local AABB as convex_hull_data_create computes it (ConvexHull.hpp:401-414)
+    double mn[3] = {(double)1e30f, (double)1e30f, (double)1e30f};
+    double mx[3] = {(double)-1e30f, (double)-1e30f, (double)-1e30f};
+    for (uint32_t v = 0; v < n_verts; ++v)
+        for (int k = 0; k < 3; ++k)
+        {
+            mn[k] = rmin(mn[k], verts[3 * v + k]);
+            mx[k] = rmax(mx[k], verts[3 * v + k]);
+        }
+    for (int k = 0; k < 3; ++k)
+    {
+        h.aabb[k] = mn[k];
+        h.aabb[3 + k] = mx[k];
+    }
+    b->hulls.push_back(std::move(h));
+    if (hull_id)
+        *hull_id = (uint32_t)(b->hulls.size() - 1);
+    return RBPS_OK;
+}
+
+extern "C" int rbps_world_add_bodies(rbps_batch *b, uint32_t world, uint32_t n, const rbps_body_desc *d,
+                                     uint32_t *first_id)
+{
+    int rc = check_world(b, world, true);
+    if (rc)
+        return rc;
+    if (n && !d)
+        return fail(RBPS_ERR_INVALID, "rbps_world_add_bodies: null descriptors");
+    HostWorld &w = b->worlds[world];
+    if (first_id)
+        *first_id = (uint32_t)w.bodies.size();
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        if (d[i].type != RBPS_BODY_STATIC && !(d[i].mass > 0.0))
+            return fail(RBPS_ERR_INVALID, "dynamic body needs mass > 0");
+        w.bodies.push_back(d[i]);
+        // create_body bakes gravity into the force (BodyAPI.hpp:61)
+        w.force.push_back(0.0);
+        w.force.push_back((double)(-9.8f) * d[i].mass);
+        w.force.push_back(0.0);
+        w.torque.insert(w.torque.end(), {0.0, 0.0, 0.0});
+    }
+    return RBPS_OK;
+}
+
+extern "C" int rbps_world_add_body(rbps_batch *b, uint32_t world, const rbps_body_desc *d, uint32_t *id)
+{
+    return rbps_world_add_bodies(b, world, 1, d, id);
+}
+
+extern "C" int rbps_world_set_body_force(rbps_batch *b, uint32_t world, uint32_t body, const double f[3],
+                                         const double t[3])
+{
+    int rc = check_world(b, world, true);
+    if (rc)
+        return rc;
+    HostWorld &w = b->worlds[world];
+    if (body >= w.bodies.size())
+        return fail(RBPS_ERR_INVALID, "body %u out of range", body);
+    for (int k = 0; k < 3; ++k)
+    {
+        if (f)
+            w.force[3 * body + k] = f[k];
+        if (t)
+            w.torque[3 * body + k] = t[k];
+    }
+    return RBPS_OK;
+}
+
+extern "C" int rbps_world_add_colliders(rbps_batch *b, uint32_t world, uint32_t n, const rbps_collider_desc *d,
+                                        uint32_t *first_id)
+{
+    int rc = check_world(b, world, true);
+    if (rc)
+        return rc;
+    HostWorld &w = b->worlds[world];
+    if (first_id)
+        *first_id = (uint32_t)w.colliders.size();
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const rbps_collider_desc &c = d[i];
+        if (c.body_id >= w.bodies.size())
+            return fail(RBPS_ERR_INVALID, "collider body %u does not exist", c.body_id);
+        if (c.shape != RBPS_SHAPE_SPHERE && c.shape != RBPS_SHAPE_BOX && c.shape != RBPS_SHAPE_CAPSULE &&
+            c.shape != RBPS_SHAPE_PLANE && c.shape != RBPS_SHAPE_CONVEX_HULL)
+            return fail(RBPS_ERR_INVALID, "unsupported shape kind %d", c.shape);
+        if (c.shape == RBPS_SHAPE_CONVEX_HULL && c.hull >= b->hulls.size())
+            return fail(RBPS_ERR_INVALID, "hull %u does not exist", c.hull);
+        w.colliders.push_back(c);
+    }
+    return RBPS_OK;
+}
+
+extern "C" int rbps_world_add_collider(rbps_batch *b, uint32_t world, const rbps_collider_desc *d, uint32_t *id)
+{
+    return rbps_world_add_colliders(b, world, 1, d, id);
+}
+
+extern "C" int rbps_world_add_joint(rbps_batch *b, uint32_t world, const rbps_joint_desc *d, uint32_t *id)
+{
+    int rc = check_world(b, world, true);
+    if (rc)
+        return rc;
+    HostWorld &w = b->worlds[world];
+    if (!d || d->body_1 >= w.bodies.size() || d->body_2 >= w.bodies.size())
+        return fail(RBPS_ERR_INVALID, "joint bodies out of range");
+    if (d->type < RBPS_JOINT_PRISMATIC || d->type > RBPS_JOINT_FIXED)
+        return fail(RBPS_ERR_INVALID, "bad joint type %d", d->type);
+    if (id)
+        *id = (uint32_t)w.joints.size();
+    w.joints.push_back(*d);
+    return RBPS_OK;
+}
+
+// ------------------------------------------------------------ commit
+namespace
+{
+    template <class T, class P>
+    Engine<T, P> make_engine(rbps_batch *b)
+    {
+        Engine<T, P> e;
+        std::memset(&e, 0, sizeof(e));
+        e.B.pos = (V4<P> *)b->pos;
+        e.B.rot = (Q4<T> *)b->rot;
+        e.B.lin = (V4<T> *)b->lin;
+        e.B.ang = (V4<T> *)b->ang;
+        e.B.prev_pos = (V4<P> *)b->prev_pos;
+        e.B.prev_rot = (Q4<T> *)b->prev_rot;
+        e.B.force = (V4<T> *)b->force;
+        e.B.torque = (V4<T> *)b->torque;
+        e.B.inertia = (S8<T> *)b->inertia;
+        e.B.inv_inertia = (S8<T> *)b->inv_inertia;
+        e.B.type = b->btype;
+        e.shape = b->shape;
+        e.c_body = b->c_body;
+        e.c_lpos = b->c_lpos;
+        e.c_lrot = b->c_lrot;
+        e.c_static = b->c_static;
+        e.c_mat = (const V4<T> *)b->c_mat;
+        e.hulls.verts = b->hull_verts;
+        e.hulls.v_off = b->hull_voff;
+        e.hulls.local_aabb = b->hull_aabb;
+        e.bp_coll = b->bp_coll;
+        e.fat = b->fat;
+        e.ep_key = b->ep_key;
+        e.ep_id = b->ep_id;
+        e.ep_pos = b->ep_pos;
+        e.plane_cand = b->plane_cand;
+        e.joints = (Joint<T> *)b->joints_d;
+        e.rows = (Row<T> *)b->rows_d;
+        e.jorder = b->jorder;
+        e.jcolor_off = b->jcolor_off;
+        e.worlds = b->worlds_d;
+        e.stats = b->stats_d;
+        e.error = b->error_d;
+        const double h = b->desc.timestep / b->desc.substeps;
+        e.dt_frame = b->desc.timestep;
+        e.h = T(h);
+        e.inv_h = T(1.0 / h);
+        e.substeps = b->desc.substeps;
+        e.fat_margin = b->desc.fat_margin;
+        e.reinsert_threshold = b->desc.reinsert_threshold;
+        e.solve_mode = b->desc.solve_mode;
+        e.use_vel_exp = b->desc.use_velocity_expansion;
+        e.work_counter = b->work_counter;
+        e.small_worlds = b->small_list;
+        e.n_small = (uint32_t)b->small_ids.size();
+        e.dump_pairs = b->dump ? b->dump_pairs : nullptr;
+        e.dump_cand = b->dump ? b->dump_cand : nullptr;
+        e.dump_cc = b->dump ? (CandContacts<T, P> *)b->dump_cc : nullptr;
+        e.dump_color = b->dump ? b->dump_color : nullptr;
+        e.dump_pair_cap = b->dump_pair_cap;
+        e.dump_cand_cap = b->dump_cand_cap;
+        return e;
+    }
+
+    ScratchLayout make_layout(uint32_t nbp, uint32_t nb, uint32_t pair_cap, uint32_t npc, uint32_t block,
+                              size_t cc_size)
+    {
+        ScratchLayout L{};
+        const size_t nep = 2 * (size_t)nbp + 1;
+        const size_t pc = (size_t)pair_cap + 1;
+        const size_t nc = pc + npc;
+        const size_t nt_max = std::max((nep + block - 1) / block, (pc + block - 1) / block) + 1;
+        const size_t counts = 256 * nt_max;
+        const size_t tsums = std::max((counts + block - 1) / block, nt_max) + 4;
+        size_t off = 0;
+        auto take = [&](size_t &field, size_t bytes) {
+            off = align_up(off, 128);
+            field = off;
+            off += bytes;
+        };
+        take(L.ep_k2, nep * 4);
+        take(L.ep_v2, nep * 4);
+        take(L.counts, counts * 4);
+        take(L.tile_sums, tsums * 4);
+        take(L.cnt, nep * 4);
+        take(L.pr_a, pc * 4);
+        take(L.pr_b, pc * 4);
+        take(L.pk, pc * 4);
+        take(L.pv, pc * 4);
+        take(L.pk2, pc * 4);
+        take(L.pv2, pc * 4);
+        take(L.cflag, pc * 4);
+        take(L.cand, nc * sizeof(Cand));
+        take(L.cc, nc * cc_size);
+        take(L.color, nc * 4);
+        take(L.bmask, (size_t)nb * 8 + 8);
+        take(L.bprio, (size_t)nb * 8 + 8);
+        take(L.corder, nc * 4);
+        take(L.misc, kMiscWords * 4);
+        L.stride = align_up(off, 256);
+        return L;
+    }
+
+    size_t cc_size_of(int precision)
+    {
+        if (precision == RBPS_PRECISION_FP64)
+            return sizeof(CandContacts<double, double>);
+        if (precision == RBPS_PRECISION_FP32)
+            return sizeof(CandContacts<float, float>);
+        return sizeof(CandContacts<float, double>);
+    }
+
+    template <class T>
+    void put_v4(std::vector<char> &buf, size_t idx, double x, double y, double z, double w)
+    {
+        T *p = (T *)(buf.data() + idx * 4 * sizeof(T));
+        p[0] = T(x); p[1] = T(y); p[2] = T(z); p[3] = T(w);
+    }
+
+    constexpr uint32_t kSmallWorldBodies = 4096;
+} // namespace
+
+template <class T, class P>
+static int commit_typed(rbps_batch *b)
+{
+    const uint32_t W = (uint32_t)b->worlds.size();
+    // ---- offsets
+    b->wdev.assign(W, WorldDev{});
+    uint32_t nb = 0, nc = 0, nbp = 0, npc = 0, nj = 0, nr = 0, njc = 0;
+    std::vector<std::vector<uint32_t>> bp_lists(W);
+    std::vector<std::vector<uint2>> pc_lists(W);
+    std::vector<std::vector<uint32_t>> jorders(W), joffs(W);
+    for (uint32_t w = 0; w < W; ++w)
+    {
+        const HostWorld &hw = b->worlds[w];
+        WorldDev &d = b->wdev[w];
+        d.body_off = nb;
+        d.n_bodies = (uint32_t)hw.bodies.size();
+        d.coll_off = nc;
+        d.n_coll = (uint32_t)hw.colliders.size();
+        for (uint32_t c = 0; c < d.n_coll; ++c)
+            if (hw.colliders[c].shape != RBPS_SHAPE_PLANE)
+                bp_lists[w].push_back(c);
+        d.bp_off = nbp;
+        d.n_bp = (uint32_t)bp_lists[w].size();
+        // plane loop of run_narrow_phase (CollisionPipeline.cpp:159-196)
+        for (uint32_t pi = 0; pi < d.n_coll; ++pi)
+        {
+            const rbps_collider_desc &pc = hw.colliders[pi];
+            if (pc.shape != RBPS_SHAPE_PLANE)
+                continue;
+            for (uint32_t di = 0; di < d.n_coll; ++di)
+            {
+                const rbps_collider_desc &dc = hw.colliders[di];
+                if (di == pi || dc.shape == RBPS_SHAPE_PLANE)
+                    continue;
+                if (pc.is_static && dc.is_static)
+                    continue;
+                if (pc.body_id == dc.body_id)
+                    continue;
+                pc_lists[w].push_back(make_uint2(di, pi));
+            }
+        }
+        d.pc_off = npc;
+        d.n_pc = (uint32_t)pc_lists[w].size();
+        d.joint_off = nj;
+        d.n_joints = (uint32_t)hw.joints.size();
+        d.row_off = nr;
+        uint32_t rows = 0;
+        for (const auto &j : hw.joints)
+            rows += j.type == RBPS_JOINT_REVOLUTE ? 4 : (j.type == RBPS_JOINT_PRISMATIC ? 3 : 2);
+        d.n_rows = rows;
+        // greedy joint colouring by shared dynamic bodies
+        {
+            std::vector<uint32_t> color(d.n_joints, 0);
+            uint32_t ncol = 0;
+            std::vector<std::vector<uint32_t>> body_cols(d.n_bodies);
+            for (uint32_t j = 0; j < d.n_joints; ++j)
+            {
+                const auto &jd = hw.joints[j];
+                std::vector<uint32_t> used;
+                for (uint32_t bb : {jd.body_1, jd.body_2})
+                    if (hw.bodies[bb].type != RBPS_BODY_STATIC)
+                        used.insert(used.end(), body_cols[bb].begin(), body_cols[bb].end());
+                uint32_t c = 0;
+                while (std::find(used.begin(), used.end(), c) != used.end())
+                    ++c;
+                color[j] = c;
+                ncol = std::max(ncol, c + 1);
+                for (uint32_t bb : {jd.body_1, jd.body_2})
+                    if (hw.bodies[bb].type != RBPS_BODY_STATIC)
+                        body_cols[bb].push_back(c);
+            }
+            std::vector<uint32_t> off(ncol + 1, 0);
+            for (uint32_t j = 0; j < d.n_joints; ++j)
+                off[color[j] + 1]++;
+            for (uint32_t c = 0; c < ncol; ++c)
+                off[c + 1] += off[c];
+            std::vector<uint32_t> fill(off.begin(), off.end() - 1), order(d.n_joints);
+            for (uint32_t j = 0; j < d.n_joints; ++j)
+                order[fill[color[j]]++] = j;
+            jorders[w] = order;
+            joffs[w] = off;
+            d.jc_off = njc;
+            d.n_jcolors = ncol;
+            njc += ncol + 1;
+        }
+        d.pair_cap = b->desc.max_pairs_per_world ? b->desc.max_pairs_per_world
+                                                 : std::max<uint32_t>(1024u, 8u * d.n_bp);
+        d.dump_slot = ~0u;
+        nb += d.n_bodies;
+        nc += d.n_coll;
+        nbp += d.n_bp;
+        npc += d.n_pc;
+        nj += d.n_joints;
+        nr += rows;
+    }
+    b->n_bodies_all = nb;
+    b->n_coll_all = nc;
+    b->n_bp_all = nbp;
+    b->n_joint_all = nj;
+    b->n_row_all = nr;
+
+    // ---- bodies
+    std::vector<char> pos(nb * 4 * sizeof(P)), ppos(nb * 4 * sizeof(P));
+    std::vector<char> rot(nb * 4 * sizeof(T)), lin(nb * 4 * sizeof(T)), ang(nb * 4 * sizeof(T));
+    std::vector<char> frc(nb * 4 * sizeof(T)), trq(nb * 4 * sizeof(T));
+    std::vector<char> inr(nb * 8 * sizeof(T)), iinr(nb * 8 * sizeof(T));
+    std::vector<uint8_t> btype(nb);
+    b->total_bodies = nb;
+    b->total_dynamic = 0;
+    for (uint32_t w = 0; w < W; ++w)
+    {
+        const HostWorld &hw = b->worlds[w];
+        for (uint32_t i = 0; i < hw.bodies.size(); ++i)
+        {
+            const rbps_body_desc &d = hw.bodies[i];
+            const size_t g = b->wdev[w].body_off + i;
+            const bool st = d.type == RBPS_BODY_STATIC;
+            const double inv_mass = st ? 0.0 : 1.0 / d.mass;
+            double iinv[6] = {0, 0, 0, 0, 0, 0};
+            if (!st)
+                smat3_inverse(d.inertia, iinv);
+            put_v4<P>(pos, g, d.position[0], d.position[1], d.position[2], 0);
+            put_v4<P>(ppos, g, d.position[0], d.position[1], d.position[2], 0);
+            put_v4<T>(rot, g, d.orientation[0], d.orientation[1], d.orientation[2], d.orientation[3]);
+            put_v4<T>(lin, g, d.linear_velocity[0], d.linear_velocity[1], d.linear_velocity[2], inv_mass);
+            put_v4<T>(ang, g, d.angular_velocity[0], d.angular_velocity[1], d.angular_velocity[2], 0);
+            put_v4<T>(frc, g, hw.force[3 * i], hw.force[3 * i + 1], hw.force[3 * i + 2], 0);
+            put_v4<T>(trq, g, hw.torque[3 * i], hw.torque[3 * i + 1], hw.torque[3 * i + 2], 0);
+            T *I = (T *)(inr.data() + g * 8 * sizeof(T));
+            T *Ii = (T *)(iinr.data() + g * 8 * sizeof(T));
+            for (int k = 0; k < 6; ++k)
+            {
+                I[k] = T(d.inertia[k]);
+                Ii[k] = T(iinv[k]);
+            }
+            I[6] = I[7] = Ii[6] = Ii[7] = T(0);
+            btype[g] = st ? kStatic : kDynamic;
+            if (!st)
+                b->total_dynamic++;
+        }
+    }
+    int rc = 0;
+    auto up = [&](void **dst, const std::vector<char> &v) {
+        if (rc)
+            return;
+        rc = b->alloc(dst, v.size());
+        if (!rc && !v.empty())
+            if (cudaMemcpy(*dst, v.data(), v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = fail(RBPS_ERR_CUDA, "upload failed");
+    };
+    up(&b->pos, pos);
+    up(&b->prev_pos, ppos);
+    up(&b->rot, rot);
+    up(&b->prev_rot, rot);
+    up(&b->lin, lin);
+    up(&b->ang, ang);
+    up(&b->force, frc);
+    up(&b->torque, trq);
+    up(&b->inertia, inr);
+    up(&b->inv_inertia, iinr);
+    if (rc)
+        return rc;
+    if ((rc = b->upload(&b->btype, btype)))
+        return rc;
+
+    // ---- hulls
+    {
+        std::vector<double> hv, ha;
+        std::vector<uint32_t> hoff(1, 0);
+        for (const auto &h : b->hulls)
+        {
+            hv.insert(hv.end(), h.verts.begin(), h.verts.end());
+            hoff.push_back((uint32_t)(hv.size() / 3));
+            ha.insert(ha.end(), h.aabb, h.aabb + 6);
+        }
+        if ((rc = b->upload(&b->hull_verts, hv)) || (rc = b->upload(&b->hull_voff, hoff)) ||
+            (rc = b->upload(&b->hull_aabb, ha)))
+            return rc;
+    }
+    HullSetDev hs_host{nullptr, nullptr, nullptr};
+
+    // ---- colliders + initial SAP state (broad_phase_insert, BroadPhase.cpp:169-197)
+    std::vector<ShapeDev> shp(nc);
+    std::vector<uint32_t> cbody(nc), bpc(nbp), epk(2 * (size_t)nbp), epi(2 * (size_t)nbp), epp(2 * (size_t)nbp);
+    std::vector<V4<double>> clp(nc);
+    std::vector<Q4<double>> clr(nc);
+    std::vector<uint8_t> cst(nc);
+    std::vector<char> cmat(nc * 4 * sizeof(T));
+    std::vector<FatBox> fat(nbp);
+    std::vector<uint2> pcs;
+    pcs.reserve(npc);
+    for (uint32_t w = 0; w < W; ++w)
+    {
+        const HostWorld &hw = b->worlds[w];
+        const WorldDev &d = b->wdev[w];
+        for (uint32_t c = 0; c < d.n_coll; ++c)
+        {
+            const rbps_collider_desc &cd = hw.colliders[c];
+            const size_t g = d.coll_off + c;
+            ShapeDev s{};
+            s.kind = cd.shape;
+            s.hull = (int)cd.hull;
+            for (int k = 0; k < 4; ++k)
+                s.p[k] = cd.params[k];
+            shp[g] = s;
+            cbody[g] = cd.body_id;
+            clp[g] = V4<double>{cd.local_pos[0], cd.local_pos[1], cd.local_pos[2], 0.0};
+            clr[g] = Q4<double>{cd.local_rot[0], cd.local_rot[1], cd.local_rot[2], cd.local_rot[3]};
+            cst[g] = cd.is_static ? 1 : 0;
+            put_v4<T>(cmat, g, cd.restitution, cd.static_friction, cd.dynamic_friction, 0);
+        }
+        for (uint32_t o = 0; o < d.n_bp; ++o)
+        {
+            const uint32_t c = bp_lists[w][o];
+            const rbps_collider_desc &cd = hw.colliders[c];
+            const rbps_body_desc &bd = hw.bodies[cd.body_id];
+            bpc[d.bp_off + o] = c;
+            tf<double> t;
+            const vec3<double> bp(bd.position[0], bd.position[1], bd.position[2]);
+            const quat<double> br(bd.orientation[0], bd.orientation[1], bd.orientation[2], bd.orientation[3]);
+            t.pos = bp + rotate(br, vec3<double>(cd.local_pos[0], cd.local_pos[1], cd.local_pos[2]));
+            t.rot = br * quat<double>(cd.local_rot[0], cd.local_rot[1], cd.local_rot[2], cd.local_rot[3]);
+            HullSetDev hs = hs_host;
+            std::vector<double> la;
+            if (cd.shape == RBPS_SHAPE_CONVEX_HULL)
+            {
+                la.assign(b->hulls[cd.hull].aabb, b->hulls[cd.hull].aabb + 6);
+                hs.local_aabb = la.data();
+            }
+            ShapeDev s = shp[d.coll_off + c];
+            s.hull = 0;
+            const aabb tight = compute_aabb(s, t, hs);
+            const aabb f = aabb_expand(tight, b->desc.fat_margin);
+            FatBox fb;
+            fb.mn[0] = f.mn.x; fb.mn[1] = f.mn.y; fb.mn[2] = f.mn.z;
+            fb.mx[0] = f.mx.x; fb.mx[1] = f.mx.y; fb.mx[2] = f.mx.z;
+            fat[d.bp_off + o] = fb;
+            const size_t e0 = 2 * (size_t)d.bp_off;
+            epk[e0 + 2 * o] = order_key_host((float)f.mn.x);
+            epk[e0 + 2 * o + 1] = order_key_host((float)f.mx.x);
+            epi[e0 + 2 * o] = 2 * o;
+            epi[e0 + 2 * o + 1] = 2 * o + 1;
+            epp[e0 + 2 * o] = 2 * o;
+            epp[e0 + 2 * o + 1] = 2 * o + 1;
+        }
+        pcs.insert(pcs.end(), pc_lists[w].begin(), pc_lists[w].end());
+    }
+    if ((rc = b->upload(&b->shape, shp)) || (rc = b->upload(&b->c_body, cbody)) || (rc = b->upload(&b->c_lpos, clp)) ||
+        (rc = b->upload(&b->c_lrot, clr)) || (rc = b->upload(&b->c_static, cst)) || (rc = b->upload(&b->bp_coll, bpc)) ||
+        (rc = b->upload(&b->fat, fat)) || (rc = b->upload(&b->ep_key, epk)) || (rc = b->upload(&b->ep_id, epi)) ||
+        (rc = b->upload(&b->ep_pos, epp)) || (rc = b->upload(&b->plane_cand, pcs)))
+        return rc;
+    up(&b->c_mat, cmat);
+    if (rc)
+        return rc;
+
+    // ---- joints and their constraint rows (JointAPI.hpp:191-267)
+    {
+        std::vector<Joint<T>> js(nj);
+        std::vector<Row<T>> rs(nr);
+        for (uint32_t w = 0; w < W; ++w)
+        {
+            const HostWorld &hw = b->worlds[w];
+            const WorldDev &d = b->wdev[w];
+            uint32_t row = d.row_off;
+            for (uint32_t j = 0; j < d.n_joints; ++j)
+            {
+                const rbps_joint_desc &jd = hw.joints[j];
+                Joint<T> J{};
+                J.r1 = V4<T>{T(jd.r_1[0]), T(jd.r_1[1]), T(jd.r_1[2]), T(0)};
+                J.r2 = V4<T>{T(jd.r_2[0]), T(jd.r_2[1]), T(jd.r_2[2]), T(0)};
+                J.axis = V4<T>{T(jd.axis[0]), T(jd.axis[1]), T(jd.axis[2]), T(0)};
+                if (jd.type == RBPS_JOINT_REVOLUTE)
+                    J.limit_axis = V4<T>{T(jd.limit_axis[0]), T(jd.limit_axis[1]), T(jd.limit_axis[2]), T(0)};
+                J.lower = T(jd.lower_limit);
+                J.upper = T(jd.upper_limit);
+                J.target_pos = T(jd.target_position);
+                J.target_speed = T(jd.target_speed);
+                J.damping = T(jd.damping);
+                // from_axis_angle of the clamped limit angle (quat.hpp:111-117)
+                const double hl = jd.lower_limit * 0.5, hu = jd.upper_limit * 0.5;
+                J.sin_lo = T(std::sin(hl));
+                J.cos_lo = T(std::cos(hl));
+                J.sin_hi = T(std::sin(hu));
+                J.cos_hi = T(std::cos(hu));
+                J.b1 = d.body_off + jd.body_1;
+                J.b2 = d.body_off + jd.body_2;
+                J.row0 = row;
+                J.type = jd.type;
+                J.act = jd.type == RBPS_JOINT_FIXED ? RBPS_ACTUATION_FREE : jd.actuation;
+                J.limited = jd.type == RBPS_JOINT_FIXED ? 0 : jd.limited;
+                int types[4];
+                double comp[4] = {0, 0, 0, 0};
+                int cnt;
+                if (jd.type == RBPS_JOINT_REVOLUTE)
+                {
+                    cnt = 4;
+                    types[0] = kRowRotational; types[1] = kRowPositional; types[2] = kRowRotational; types[3] = kRowRotational;
+                    comp[3] = jd.compliance;
+                }
+                else if (jd.type == RBPS_JOINT_PRISMATIC)
+                {
+                    cnt = 3;
+                    types[0] = kRowRotational; types[1] = kRowPositional; types[2] = kRowPositional;
+                    comp[2] = jd.compliance;
+                }
+                else
+                {
+                    cnt = 2;
+                    types[0] = kRowRotational; types[1] = kRowPositional;
+                }
+                J.count = cnt;
+                for (int r = 0; r < cnt; ++r)
+                {
+                    Row<T> R{};
+                    R.dir = V4<T>{T(1.0), T(0.0), T(0.0), T(0.0)};
+                    R.r1 = V4<T>{T(jd.r_1[0]), T(jd.r_1[1]), T(jd.r_1[2]), T(comp[r])};
+                    R.r2 = V4<T>{T(jd.r_2[0]), T(jd.r_2[1]), T(jd.r_2[2]), T(0.0)};
+                    R.b1 = J.b1;
+                    R.b2 = J.b2;
+                    R.type = types[r];
+                    rs[row + r] = R;
+                }
+                row += cnt;
+                js[d.joint_off + j] = J;
+            }
+        }
+        // joint orders are world-local; colour offsets index jorder world slices
+        std::vector<uint32_t> jord_g, jco_g;
+        for (uint32_t w = 0, jo = 0; w < W; ++w)
+        {
+            const WorldDev &d = b->wdev[w];
+            for (uint32_t k = 0; k < d.n_joints; ++k)
+                jord_g.push_back(jorders[w][k]);
+            for (uint32_t k = 0; k <= d.n_jcolors; ++k)
+                jco_g.push_back(joffs[w][k] + jo);
+            jo += d.n_joints;
+        }
+        std::vector<char> jb(js.size() * sizeof(Joint<T>)), rb(rs.size() * sizeof(Row<T>));
+        if (!js.empty())
+            std::memcpy(jb.data(), js.data(), jb.size());
+        if (!rs.empty())
+            std::memcpy(rb.data(), rs.data(), rb.size());
+        up(&b->joints_d, jb);
+        up(&b->rows_d, rb);
+        if (rc)
+            return rc;
+        if ((rc = b->upload(&b->jorder, jord_g)) || (rc = b->upload(&b->jcolor_off, jco_g)))
+            return rc;
+    }
+
+    // ---- executors: small worlds on persistent CTAs, large ones on the grid
+    b->small_ids.clear();
+    b->big_ids.clear();
+    std::vector<uint32_t> order(W);
+    for (uint32_t w = 0; w < W; ++w)
+        order[w] = w;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t c) { return b->wdev[a].n_bodies > b->wdev[c].n_bodies; });
+    uint32_t s_bp = 0, s_b = 0, s_pc = 0, s_npc = 0, g_bp = 0, g_b = 0, g_pc = 0, g_npc = 0;
+    for (uint32_t w : order)
+    {
+        const WorldDev &d = b->wdev[w];
+        if (d.n_bodies <= kSmallWorldBodies)
+        {
+            b->small_ids.push_back(w);
+            s_bp = std::max(s_bp, d.n_bp); s_b = std::max(s_b, d.n_bodies);
+            s_pc = std::max(s_pc, d.pair_cap); s_npc = std::max(s_npc, d.n_pc);
+        }
+        else
+        {
+            b->big_ids.push_back(w);
+            g_bp = std::max(g_bp, d.n_bp); g_b = std::max(g_b, d.n_bodies);
+            g_pc = std::max(g_pc, d.pair_cap); g_npc = std::max(g_npc, d.n_pc);
+        }
+    }
+    const size_t ccs = cc_size_of(b->desc.precision);
+    if (!b->small_ids.empty())
+    {
+        int per_sm = 0;
+        CU(occupancy_small<T, P>(b->block, &per_sm));
+        if (per_sm < 1)
+            return fail(RBPS_ERR_CUDA, "step kernel cannot be resident with %d threads", b->block);
+        b->grid_small = std::min<int>((int)b->small_ids.size(), per_sm * b->sm_count);
+        b->lay_small = make_layout(s_bp, s_b, s_pc, s_npc, b->block, ccs);
+        if ((rc = b->alloc((void **)&b->scratch_small, b->lay_small.stride * b->grid_small)))
+            return rc;
+        if ((rc = b->upload(&b->small_list, b->small_ids)))
+            return rc;
+    }
+    if (!b->big_ids.empty())
+    {
+        int per_sm = 0;
+        CU(occupancy_big<T, P>(b->block, &per_sm));
+        if (per_sm < 1)
+            return fail(RBPS_ERR_CUDA, "cooperative step kernel cannot be resident");
+        b->grid_big = per_sm * b->sm_count;
+        b->lay_big = make_layout(g_bp, g_b, g_pc, g_npc, b->block, ccs);
+        if ((rc = b->alloc((void **)&b->scratch_big, b->lay_big.stride)))
+            return rc;
+    }
+    if ((rc = b->alloc((void **)&b->work_counter, 64)) || (rc = b->alloc((void **)&b->error_d, 64)) ||
+        (rc = b->alloc((void **)&b->stats_d, sizeof(WorldStats) * W)))
+        return rc;
+    if ((rc = b->upload(&b->worlds_d, b->wdev)))
+        return rc;
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_commit(rbps_batch *b)
+{
+    if (!b)
+        return fail(RBPS_ERR_INVALID, "null batch");
+    if (b->committed)
+        return fail(RBPS_ERR_INVALID, "batch already committed");
+    CU(cudaSetDevice(b->desc.device));
+    int rc;
+    if (b->desc.precision == RBPS_PRECISION_FP64)
+        rc = commit_typed<double, double>(b);
+    else if (b->desc.precision == RBPS_PRECISION_FP32)
+        rc = commit_typed<float, float>(b);
+    else
+        rc = commit_typed<float, double>(b);
+    if (rc)
+        return rc;
+    CU(cudaDeviceSynchronize());
+    b->committed = true;
+    return RBPS_OK;
+}
+
+// ------------------------------------------------------------ dumps
+template <class T, class P>
+static int alloc_dumps(rbps_batch *b)
+{
+    if (b->dump_pairs)
+        return RBPS_OK;
+    uint32_t pc = 0, cc = 0;
+    for (auto &d : b->wdev)
+    {
+        pc = std::max(pc, d.pair_cap);
+        cc = std::max(cc, d.pair_cap + d.n_pc);
+    }
+    const size_t W = b->wdev.size();
+    b->dump_pair_cap = pc;
+    b->dump_cand_cap = cc;
+    int rc;
+    if ((rc = b->alloc((void **)&b->dump_pairs, W * 2 * pc * 4)) ||
+        (rc = b->alloc((void **)&b->dump_cand, W * cc * sizeof(Cand))) ||
+        (rc = b->alloc((void **)&b->dump_cc, W * cc * sizeof(CandContacts<T, P>))) ||
+        (rc = b->alloc((void **)&b->dump_color, W * cc * 4)))
+        return rc;
+    for (size_t w = 0; w < W; ++w)
+        b->wdev[w].dump_slot = (uint32_t)w;
+    CU(cudaMemcpy(b->worlds_d, b->wdev.data(), W * sizeof(WorldDev), cudaMemcpyHostToDevice));
+    // the zero fills above ran on the legacy stream; the step kernels run on
+    // the batch's non-blocking stream
+    CU(cudaDeviceSynchronize());
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_set_dump(rbps_batch *b, int32_t enable)
+{
+    if (!b || !b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_set_dump: commit first");
+    CU(cudaSetDevice(b->desc.device));
+    CU(cudaStreamSynchronize(b->stream));
+    b->dump = enable != 0;
+    if (!b->dump)
+        return RBPS_OK;
+    if (b->desc.precision == RBPS_PRECISION_FP64)
+        return alloc_dumps<double, double>(b);
+    if (b->desc.precision == RBPS_PRECISION_FP32)
+        return alloc_dumps<float, float>(b);
+    return alloc_dumps<float, double>(b);
+}
+
+// ------------------------------------------------------------ stepping
+template <class T, class P>
+static int step_typed(rbps_batch *b, int n)
+{
+    Engine<T, P> e = make_engine<T, P>(b);
+    e.scratch = b->scratch_small;
+    e.lay = b->lay_small;
+    uint64_t launches = 0;
+    for (int s = 0; s < n; ++s)
+    {
+        if (!b->small_ids.empty())
+        {
+            CU(cudaMemsetAsync(b->work_counter, 0, 4, b->stream));
+            CU(launch_step_small<T, P>(e, b->grid_small, b->block, b->stream));
+            ++launches;
+        }
+        if (!b->big_ids.empty())
+        {
+            Engine<T, P> eb = e;
+            eb.scratch = b->scratch_big;
+            eb.lay = b->lay_big;
+            for (uint32_t w : b->big_ids)
+            {
+                CU(launch_step_big<T, P>(eb, w, b->grid_big, b->block, b->stream));
+                ++launches;
+            }
+        }
+    }
+    b->launches_last = launches;
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_step(rbps_batch *b, int32_t n_steps)
+{
+    if (!b || !b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_step: commit first");
+    if (n_steps < 0)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_step: negative step count");
+    CU(cudaSetDevice(b->desc.device));
+    int rc;
+    // the small-world view needs its scratch / layout
+    if (b->desc.precision == RBPS_PRECISION_FP64)
+        rc = step_typed<double, double>(b, n_steps);
+    else if (b->desc.precision == RBPS_PRECISION_FP32)
+        rc = step_typed<float, float>(b, n_steps);
+    else
+        rc = step_typed<float, double>(b, n_steps);
+    if (!rc)
+        b->steps_done += (uint64_t)n_steps;
+    return rc;
+}
+
+static int check_device_error(rbps_batch *b)
+{
+    int err = 0;
+    CU(cudaMemcpy(&err, b->error_d, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err)
+    {
+        CU(cudaMemset(b->error_d, 0, sizeof(int)));
+        return fail(err, "device reported error %d (%s)", err,
+                    err == RBPS_ERR_CAPACITY ? "pair capacity exceeded: raise max_pairs_per_world" : "step failure");
+    }
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_synchronize(rbps_batch *b)
+{
+    if (!b || !b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_synchronize: commit first");
+    CU(cudaSetDevice(b->desc.device));
+    CU(cudaStreamSynchronize(b->stream));
+    return check_device_error(b);
+}
+
+// ------------------------------------------------------------ readback
+template <class T, class P>
+static int get_state_typed(rbps_batch *b, uint32_t first, uint32_t n, const rbps_state_view *v)
+{
+    std::vector<V4<P>> pos(n);
+    std::vector<Q4<T>> rot(n);
+    std::vector<V4<T>> lin(n), ang(n);
+    if (v->position)
+        CU(cudaMemcpy(pos.data(), (V4<P> *)b->pos + first, n * sizeof(V4<P>), cudaMemcpyDeviceToHost));
+    if (v->orientation)
+        CU(cudaMemcpy(rot.data(), (Q4<T> *)b->rot + first, n * sizeof(Q4<T>), cudaMemcpyDeviceToHost));
+    if (v->linear_velocity)
+        CU(cudaMemcpy(lin.data(), (V4<T> *)b->lin + first, n * sizeof(V4<T>), cudaMemcpyDeviceToHost));
+    if (v->angular_velocity)
+        CU(cudaMemcpy(ang.data(), (V4<T> *)b->ang + first, n * sizeof(V4<T>), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        if (v->position)
+        {
+            v->position[3 * i] = pos[i].x; v->position[3 * i + 1] = pos[i].y; v->position[3 * i + 2] = pos[i].z;
+        }
+        if (v->orientation)
+        {
+            v->orientation[4 * i] = rot[i].w; v->orientation[4 * i + 1] = rot[i].x;
+            v->orientation[4 * i + 2] = rot[i].y; v->orientation[4 * i + 3] = rot[i].z;
+        }
+        if (v->linear_velocity)
+        {
+            v->linear_velocity[3 * i] = lin[i].x; v->linear_velocity[3 * i + 1] = lin[i].y;
+            v->linear_velocity[3 * i + 2] = lin[i].z;
+        }
+        if (v->angular_velocity)
+        {
+            v->angular_velocity[3 * i] = ang[i].x; v->angular_velocity[3 * i + 1] = ang[i].y;
+            v->angular_velocity[3 * i + 2] = ang[i].z;
+        }
+    }
+    return RBPS_OK;
+}
+
+template <class T, class P>
+static int set_state_typed(rbps_batch *b, uint32_t first, uint32_t n, const rbps_state_view *v)
+{
+    std::vector<V4<P>> pos(n);
+    std::vector<Q4<T>> rot(n);
+    std::vector<V4<T>> lin(n), ang(n);
+    CU(cudaMemcpy(pos.data(), (V4<P> *)b->pos + first, n * sizeof(V4<P>), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(rot.data(), (Q4<T> *)b->rot + first, n * sizeof(Q4<T>), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(lin.data(), (V4<T> *)b->lin + first, n * sizeof(V4<T>), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(ang.data(), (V4<T> *)b->ang + first, n * sizeof(V4<T>), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        if (v->position)
+            pos[i] = V4<P>{P(v->position[3 * i]), P(v->position[3 * i + 1]), P(v->position[3 * i + 2]), P(0)};
+        if (v->orientation)
+            rot[i] = Q4<T>{T(v->orientation[4 * i]), T(v->orientation[4 * i + 1]), T(v->orientation[4 * i + 2]),
+                           T(v->orientation[4 * i + 3])};
+        if (v->linear_velocity)
+            lin[i] = V4<T>{T(v->linear_velocity[3 * i]), T(v->linear_velocity[3 * i + 1]),
+                           T(v->linear_velocity[3 * i + 2]), lin[i].w};
+        if (v->angular_velocity)
+            ang[i] = V4<T>{T(v->angular_velocity[3 * i]), T(v->angular_velocity[3 * i + 1]),
+                           T(v->angular_velocity[3 * i + 2]), T(0)};
+    }
+    CU(cudaMemcpy((V4<P> *)b->pos + first, pos.data(), n * sizeof(V4<P>), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy((Q4<T> *)b->rot + first, rot.data(), n * sizeof(Q4<T>), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy((V4<T> *)b->lin + first, lin.data(), n * sizeof(V4<T>), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy((V4<T> *)b->ang + first, ang.data(), n * sizeof(V4<T>), cudaMemcpyHostToDevice));
+    return RBPS_OK;
+}
+
+#define DISPATCH_PREC(b, fn, ...)                                        \
+    ((b)->desc.precision == RBPS_PRECISION_FP64   ? fn<double, double>(__VA_ARGS__) \
+     : (b)->desc.precision == RBPS_PRECISION_FP32 ? fn<float, float>(__VA_ARGS__)   \
+                                                  : fn<float, double>(__VA_ARGS__))
+
+static int ready(rbps_batch *b, const char *who)
+{
+    if (!b || !b->committed)
+        return fail(RBPS_ERR_INVALID, "%s: commit first", who);
+    CU(cudaSetDevice(b->desc.device));
+    CU(cudaStreamSynchronize(b->stream));
+    return check_device_error(b);
+}
+
+extern "C" int rbps_batch_get_state(rbps_batch *b, uint32_t world, const rbps_state_view *v)
+{
+    int rc = ready(b, "rbps_batch_get_state");
+    if (rc)
+        return rc;
+    if (!v || world >= b->wdev.size())
+        return fail(RBPS_ERR_INVALID, "rbps_batch_get_state: bad world or view");
+    return DISPATCH_PREC(b, get_state_typed, b, b->wdev[world].body_off, b->wdev[world].n_bodies, v);
+}
+
+extern "C" int rbps_batch_set_state(rbps_batch *b, uint32_t world, const rbps_state_view *v)
+{
+    int rc = ready(b, "rbps_batch_set_state");
+    if (rc)
+        return rc;
+    if (!v || world >= b->wdev.size())
+        return fail(RBPS_ERR_INVALID, "rbps_batch_set_state: bad world or view");
+    return DISPATCH_PREC(b, set_state_typed, b, b->wdev[world].body_off, b->wdev[world].n_bodies, v);
+}
+
+extern "C" int rbps_batch_get_state_all(rbps_batch *b, const rbps_state_view *v)
+{
+    int rc = ready(b, "rbps_batch_get_state_all");
+    if (rc)
+        return rc;
+    if (!v)
+        return fail(RBPS_ERR_INVALID, "null view");
+    return DISPATCH_PREC(b, get_state_typed, b, 0u, b->n_bodies_all, v);
+}
+
+template <class T, class P>
+static int set_forces_typed(rbps_batch *b, const double *f)
+{
+    std::vector<V4<T>> v(b->n_bodies_all);
+    for (uint32_t i = 0; i < b->n_bodies_all; ++i)
+        v[i] = V4<T>{T(f[3 * i]), T(f[3 * i + 1]), T(f[3 * i + 2]), T(0)};
+    CU(cudaMemcpyAsync(b->force, v.data(), v.size() * sizeof(V4<T>), cudaMemcpyHostToDevice, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_set_forces_all(rbps_batch *b, const double *force)
+{
+    if (!b || !b->committed || !force)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_set_forces_all: commit first / null forces");
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, set_forces_typed, b, force);
+}
+
+extern "C" int rbps_batch_body_count(rbps_batch *b, uint32_t world, uint32_t *n)
+{
+    if (!b || world >= b->worlds.size() || !n)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_body_count: bad argument");
+    *n = (uint32_t)b->worlds[world].bodies.size();
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_total_bodies(rbps_batch *b, uint64_t *n, uint64_t *nd)
+{
+    if (!b || !b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_total_bodies: commit first");
+    if (n)
+        *n = b->total_bodies;
+    if (nd)
+        *nd = b->total_dynamic;
+    return RBPS_OK;
+}
+
+static int world_stats(rbps_batch *b, uint32_t world, WorldStats *st)
+{
+    CU(cudaMemcpy(st, b->stats_d + world, sizeof(WorldStats), cudaMemcpyDeviceToHost));
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_get_pairs(rbps_batch *b, uint32_t world, uint32_t *pairs, uint32_t cap, uint32_t *n_out)
+{
+    int rc = ready(b, "rbps_batch_get_pairs");
+    if (rc)
+        return rc;
+    if (world >= b->wdev.size())
+        return fail(RBPS_ERR_INVALID, "world out of range");
+    if (!b->dump)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_get_pairs: enable rbps_batch_set_dump before stepping");
+    WorldStats st;
+    if ((rc = world_stats(b, world, &st)))
+        return rc;
+    const uint32_t n = std::min(st.n_pairs, b->dump_pair_cap);
+    if (n_out)
+        *n_out = n;
+    if (pairs && cap)
+        CU(cudaMemcpy(pairs, b->dump_pairs + (size_t)world * 2 * b->dump_pair_cap,
+                      std::min(n, cap) * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return RBPS_OK;
+}
+
+template <class T, class P>
+static int get_contacts_typed(rbps_batch *b, uint32_t world, rbps_contact *out, uint32_t cap, uint32_t *n_out)
+{
+    WorldStats st;
+    int rc = world_stats(b, world, &st);
+    if (rc)
+        return rc;
+    const uint32_t nc = std::min(st.n_cand, b->dump_cand_cap);
+    std::vector<Cand> cand(nc);
+    std::vector<CandContacts<T, P>> cc(nc);
+    const size_t o = (size_t)world * b->dump_cand_cap;
+    CU(cudaMemcpy(cand.data(), b->dump_cand + o, nc * sizeof(Cand), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(cc.data(), (CandContacts<T, P> *)b->dump_cc + o, nc * sizeof(CandContacts<T, P>),
+                  cudaMemcpyDeviceToHost));
+    uint32_t n = 0;
+    for (uint32_t c = 0; c < nc; ++c)
+        for (int k = 0; k < cc[c].n; ++k, ++n)
+        {
+            if (!out || n >= cap)
+                continue;
+            rbps_contact &r = out[n];
+            std::memset(&r, 0, sizeof(r));
+            const ContactPt<T, P> &p = cc[c].pt[k];
+            r.body_a = cand[c].ba; r.body_b = cand[c].bb;
+            r.collider_a = cand[c].ca; r.collider_b = cand[c].cb;
+            r.normal[0] = cc[c].normal.x; r.normal[1] = cc[c].normal.y; r.normal[2] = cc[c].normal.z;
+            r.r_a_local[0] = p.ra.x; r.r_a_local[1] = p.ra.y; r.r_a_local[2] = p.ra.z;
+            r.r_b_local[0] = p.rb.x; r.r_b_local[1] = p.rb.y; r.r_b_local[2] = p.rb.z;
+            r.point_on_a[0] = p.pa.x; r.point_on_a[1] = p.pa.y; r.point_on_a[2] = p.pa.z;
+            r.point_on_b[0] = p.pb.x; r.point_on_b[1] = p.pb.y; r.point_on_b[2] = p.pb.z;
+            r.penetration_depth = p.depth;
+            r.normal_lambda = p.lam_n;
+            r.tangent_lambda = p.lam_t;
+            r.relative_velocity = p.vrel;
+            r.restitution = cc[c].mat.x; r.static_friction = cc[c].mat.y; r.dynamic_friction = cc[c].mat.z;
+            r.collision = p.coll;
+        }
+    if (n_out)
+        *n_out = n;
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_get_contacts(rbps_batch *b, uint32_t world, rbps_contact *out, uint32_t cap, uint32_t *n_out)
+{
+    int rc = ready(b, "rbps_batch_get_contacts");
+    if (rc)
+        return rc;
+    if (world >= b->wdev.size())
+        return fail(RBPS_ERR_INVALID, "world out of range");
+    if (!b->dump)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_get_contacts: enable rbps_batch_set_dump before stepping");
+    return DISPATCH_PREC(b, get_contacts_typed, b, world, out, cap, n_out);
+}
+
+extern "C" int rbps_batch_get_colors(rbps_batch *b, uint32_t world, uint32_t *colors, uint32_t *ba, uint32_t *bb,
+                                     uint32_t cap, uint32_t *n_out)
+{
+    int rc = ready(b, "rbps_batch_get_colors");
+    if (rc)
+        return rc;
+    if (world >= b->wdev.size() || !b->dump)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_get_colors: bad world or dumps disabled");
+    WorldStats st;
+    if ((rc = world_stats(b, world, &st)))
+        return rc;
+    const uint32_t nc = std::min(st.n_cand, b->dump_cand_cap);
+    if (n_out)
+        *n_out = nc;
+    const uint32_t n = std::min(nc, cap);
+    std::vector<Cand> cand(n);
+    const size_t o = (size_t)world * b->dump_cand_cap;
+    if (colors && n)
+        CU(cudaMemcpy(colors, b->dump_color + o, n * 4, cudaMemcpyDeviceToHost));
+    if ((ba || bb) && n)
+    {
+        CU(cudaMemcpy(cand.data(), b->dump_cand + o, n * sizeof(Cand), cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            if (ba)
+                ba[i] = cand[i].ba;
+            if (bb)
+                bb[i] = cand[i].bb;
+        }
+    }
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_get_stats(rbps_batch *b, rbps_stats *s)
+{
+    int rc = ready(b, "rbps_batch_get_stats");
+    if (rc)
+        return rc;
+    if (!s)
+        return fail(RBPS_ERR_INVALID, "null stats");
+    std::vector<WorldStats> st(b->wdev.size());
+    CU(cudaMemcpy(st.data(), b->stats_d, st.size() * sizeof(WorldStats), cudaMemcpyDeviceToHost));
+    std::memset(s, 0, sizeof(*s));
+    s->steps = b->steps_done;
+    for (auto &x : st)
+    {
+        s->pairs += x.n_pairs;
+        s->candidates += x.n_cand;
+        s->contacts += x.n_contacts;
+        s->max_colors = std::max(s->max_colors, x.n_colors);
+        s->serial_overflow += x.n_serial;
+    }
+    s->kernel_launches = b->launches_last;
+    return RBPS_OK;
+}
+
+int rbps_internal_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+
+// Persistent SAP state of one world (BroadPhaseState::objects[].fat_aabb and
+// ::endpoints, BroadPhase.hpp:88-143): fat AABBs per SAP object (6 doubles,
+// object order = collider order without planes), endpoints in list order as
+// (object*2 + is_max) and their float values.
+extern "C" int rbps_batch_get_sap_state(rbps_batch *b, uint32_t world, double *fat, uint32_t *ep_ids,
+                                        float *ep_values, uint32_t *n_objects)
+{
+    int rc = ready(b, "rbps_batch_get_sap_state");
+    if (rc)
+        return rc;
+    if (world >= b->wdev.size())
+        return fail(RBPS_ERR_INVALID, "world out of range");
+    const WorldDev &d = b->wdev[world];
+    if (n_objects)
+        *n_objects = d.n_bp;
+    if (fat && d.n_bp)
+        CU(cudaMemcpy(fat, b->fat + d.bp_off, d.n_bp * sizeof(FatBox), cudaMemcpyDeviceToHost));
+    if ((ep_ids || ep_values) && d.n_bp)
+    {
+        std::vector<uint32_t> ids(2 * d.n_bp), keys(2 * d.n_bp);
+        CU(cudaMemcpy(ids.data(), b->ep_id + 2 * d.bp_off, ids.size() * 4, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(keys.data(), b->ep_key + 2 * d.bp_off, keys.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < ids.size(); ++i)
+        {
+            if (ep_ids)
+                ep_ids[i] = ids[i];
+            if (ep_values)
+            {
+                // invert the order-preserving key transform
+                const uint32_t k = keys[i];
+                const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+                float f;
+                std::memcpy(&f, &u, 4);
+                ep_values[i] = f;
+            }
+        }
+    }
+    return RBPS_OK;
+}
+
+// Diagnostics: runs only the broadphase + candidate build of `world` (on
+// the first executor's scratch) and returns the pair / candidate counts.
+template <class T, class P>
+static int debug_bp_typed(rbps_batch *b, uint32_t world, uint32_t *counts)
+{
+    Engine<T, P> e = make_engine<T, P>(b);
+    e.scratch = b->scratch_small;
+    e.lay = b->lay_small;
+    uint32_t *d = nullptr;
+    CU(cudaMalloc(&d, 16));
+    CU(cudaMemset(d, 0, 16));
+    CU(launch_debug_broadphase<T, P>(e, world, b->block, d, b->stream));
+    CU(cudaStreamSynchronize(b->stream));
+    CU(cudaMemcpy(counts, d, 8, cudaMemcpyDeviceToHost));
+    cudaFree(d);
+    return RBPS_OK;
+}
+
+extern "C" RBPS_API int rbps_debug_broadphase(rbps_batch *b, uint32_t world, uint32_t *counts)
+{
+    int rc = ready(b, "rbps_debug_broadphase");
+    if (rc)
+        return rc;
+    if (world >= b->wdev.size() || b->wdev[world].n_bodies > kSmallWorldBodies)
+        return fail(RBPS_ERR_INVALID, "rbps_debug_broadphase: small worlds only");
+    return DISPATCH_PREC(b, debug_bp_typed, b, world, counts);
+}

@@ -1,0 +1,763 @@
+// engine_impl.cuh - one world step (World::step, World.hpp:192-212) executed
+// by a team of CTAs, and the kernels that run it over a batch.
+//
+// Frame (once per step):
+//   1. SAP object update: tight AABB, velocity sweep, fat-AABB escape test,
+//      endpoint key refresh        (CollisionPipeline.cpp:14-53,
+//                                   BroadPhase.hpp:228-249, BroadPhase.cpp:211-232)
+//   2. stable radix sort of the endpoints by their float key, seeded with
+//      the previous frame's order (== the reference's insertion sort,
+//      BroadPhase.cpp:80-94)
+//   3. sweep: for every opening endpoint, the objects whose interval is
+//      open there, 3-D fat-AABB test; pairs ordered by (opening position of
+//      the later object, opening position of the earlier one), which is the
+//      order bp_sweep emits them (BroadPhase.cpp:104-152)
+//   4. narrowphase candidates: filtered SAP pairs, then the static
+//      plane-vs-collider list (CollisionPipeline.cpp:110-198)
+//   5. colored mode only: Jones-Plassmann colouring of the candidates by
+//      shared dynamic bodies
+// Substeps (World.hpp:203-211): narrowphase + contact emission, integrate,
+// position solve (contacts, joint errors, joint rows), velocity update,
+// velocity solve (contacts, joint damping).
+#pragma once
+#include "engine_types.cuh"
+#include "team.cuh"
+
+namespace rbps_gpu
+{
+    __device__ __forceinline__ uint32_t order_key(float f)
+    {
+        uint32_t u = __float_as_uint(f);
+        if ((u & 0x7fffffffu) == 0u)
+            u = 0u; // -0.0f and +0.0f compare equal in the reference's sort
+        return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    }
+
+    constexpr int kErrInternal = -6;
+
+    __device__ __forceinline__ void set_error(int *err, int code)
+    {
+        atomicCAS(err, 0, code);
+    }
+
+    __device__ __forceinline__ uint32_t hash32(uint32_t x)
+    {
+        x ^= x >> 16;
+        x *= 0x7feb352dU;
+        x ^= x >> 15;
+        x *= 0x846ca68bU;
+        x ^= x >> 16;
+        return x;
+    }
+
+    template <class T, class P>
+    struct Scr
+    {
+        uint32_t *ep_k2, *ep_v2, *counts, *tile_sums, *cnt, *pr_a, *pr_b, *pk, *pv, *pk2, *pv2, *cflag;
+        Cand *cand;
+        CandContacts<T, P> *cc;
+        uint32_t *color;
+        unsigned long long *bmask, *bprio;
+        uint32_t *corder, *misc;
+    };
+
+    template <class T, class P>
+    __device__ __forceinline__ Scr<T, P> scratch_ptrs(char *base, const ScratchLayout &L)
+    {
+        Scr<T, P> s;
+        s.ep_k2 = (uint32_t *)(base + L.ep_k2);
+        s.ep_v2 = (uint32_t *)(base + L.ep_v2);
+        s.counts = (uint32_t *)(base + L.counts);
+        s.tile_sums = (uint32_t *)(base + L.tile_sums);
+        s.cnt = (uint32_t *)(base + L.cnt);
+        s.pr_a = (uint32_t *)(base + L.pr_a);
+        s.pr_b = (uint32_t *)(base + L.pr_b);
+        s.pk = (uint32_t *)(base + L.pk);
+        s.pv = (uint32_t *)(base + L.pv);
+        s.pk2 = (uint32_t *)(base + L.pk2);
+        s.pv2 = (uint32_t *)(base + L.pv2);
+        s.cflag = (uint32_t *)(base + L.cflag);
+        s.cand = (Cand *)(base + L.cand);
+        s.cc = (CandContacts<T, P> *)(base + L.cc);
+        s.color = (uint32_t *)(base + L.color);
+        s.bmask = (unsigned long long *)(base + L.bmask);
+        s.bprio = (unsigned long long *)(base + L.bprio);
+        s.corder = (uint32_t *)(base + L.corder);
+        s.misc = (uint32_t *)(base + L.misc);
+        return s;
+    }
+
+    // collider_world_tf (Collider.hpp:73-80) in the solver scalar
+    template <class T, class P>
+    __device__ __forceinline__ tf<T> collider_tf(const Engine<T, P> &E, uint32_t gc, uint32_t gb)
+    {
+        const vec3<T> bp = E.B.x(gb);
+        const quat<T> br = E.B.q(gb);
+        const V4<double> lp = E.c_lpos[gc];
+        const Q4<double> lr = E.c_lrot[gc];
+        tf<T> t;
+        t.pos = bp + rotate(br, vec3<T>(T(lp.x), T(lp.y), T(lp.z)));
+        t.rot = br * quat<T>(T(lr.w), T(lr.x), T(lr.y), T(lr.z));
+        return t;
+    }
+
+    template <class T, class P>
+    __device__ __forceinline__ tf<double> collider_tf_d(const Engine<T, P> &E, uint32_t gc, uint32_t gb)
+    {
+        const V4<P> bpv = E.B.pos[gb];
+        const Q4<T> brv = E.B.rot[gb];
+        const vec3<double> bp(double(bpv.x), double(bpv.y), double(bpv.z));
+        const quat<double> br(double(brv.w), double(brv.x), double(brv.y), double(brv.z));
+        const V4<double> lp = E.c_lpos[gc];
+        const Q4<double> lr = E.c_lrot[gc];
+        tf<double> t;
+        t.pos = bp + rotate(br, vec3<double>(lp.x, lp.y, lp.z));
+        t.rot = br * quat<double>(lr.w, lr.x, lr.y, lr.z);
+        return t;
+    }
+
+    __device__ __forceinline__ aabb load_fat(const FatBox &f)
+    {
+        return {vec3<double>(f.mn[0], f.mn[1], f.mn[2]), vec3<double>(f.mx[0], f.mx[1], f.mx[2])};
+    }
+
+    __device__ __forceinline__ bool fat_overlap(const FatBox &a, const FatBox &b)
+    {
+        return (a.mn[0] <= b.mx[0] && a.mx[0] >= b.mn[0]) &&
+               (a.mn[1] <= b.mx[1] && a.mx[1] >= b.mn[1]) &&
+               (a.mn[2] <= b.mx[2] && a.mx[2] >= b.mn[2]);
+    }
+
+    // ------------------------------------------------------------ broadphase
+    // Sort + sweep of one SAP state (BroadPhase.cpp:80-152).  On return
+    // S.pk / S.pv hold the pairs in the reference emission order (pv indexes
+    // the raw object pairs S.pr_a / S.pr_b); returns the pair count.
+    // id_limit bounds the endpoint ids (2 * object slots; slots of removed
+    // objects leave gaps in the standalone broadphase).
+    template <class Team, class SC>
+    __device__ uint32_t sap_sort_sweep(const Team &tm, const FatBox *fat, uint32_t *ep_key, uint32_t *ep_id,
+                                       uint32_t *ep_pos, uint32_t nbp, uint32_t id_limit, uint32_t pair_cap,
+                                       int *error, const SC &S, BlockShared &sh)
+    {
+        const uint32_t nep = 2 * nbp;
+        // stable sort of the endpoints, previous order as the tie-break
+        team_radix_sort(tm, ep_key, ep_id, S.ep_k2, S.ep_v2, nep, 32, S.counts, S.tile_sums, sh);
+        // inverse permutation
+        for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+        {
+            const uint32_t id = ep_id[i];
+            if (id < id_limit)
+                ep_pos[id] = i;
+            else
+                set_error(error, kErrInternal);
+        }
+        tm.sync();
+        // count the pairs each opening endpoint emits
+        for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+        {
+            const uint32_t id = ep_id[i];
+            uint32_t c = 0;
+            if (!(id & 1u) && id < id_limit)
+            {
+                const FatBox fa = fat[id >> 1];
+                const uint32_t end = min(ep_pos[id + 1], nep);
+                for (uint32_t j = i + 1; j < end; ++j)
+                {
+                    const uint32_t id2 = ep_id[j];
+                    if (!(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]))
+                        ++c;
+                }
+            }
+            S.cnt[i] = c;
+        }
+        tm.sync();
+        uint32_t total = team_excl_scan(tm, S.cnt, S.cnt, nep, S.tile_sums, sh);
+        if (tm.leader())
+            S.misc[kMiscFlags + 4] = total; // unclamped pair count
+        if (total > pair_cap)
+        {
+            if (tm.leader())
+                set_error(error, -2);
+            total = pair_cap;
+        }
+        // emit (earlier-opening object, later object, later opening position)
+        for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+        {
+            const uint32_t id = ep_id[i];
+            if ((id & 1u) || id >= id_limit)
+                continue;
+            uint32_t k = S.cnt[i];
+            const FatBox fa = fat[id >> 1];
+            const uint32_t end = min(ep_pos[id + 1], nep);
+            for (uint32_t j = i + 1; j < end && k < total; ++j)
+            {
+                const uint32_t id2 = ep_id[j];
+                if (!(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]))
+                {
+                    S.pr_a[k] = id >> 1;
+                    S.pr_b[k] = id2 >> 1;
+                    S.pk[k] = j;
+                    S.pv[k] = k;
+                    ++k;
+                }
+            }
+        }
+        tm.sync();
+        // reference emission order: stable sort by the later opening position
+        const int bits = nep > 1 ? 32 - __clz(nep - 1) : 1;
+        team_radix_sort(tm, S.pk, S.pv, S.pk2, S.pv2, total, bits, S.counts, S.tile_sums, sh);
+        return total;
+    }
+
+    template <class T, class P, class Team>
+    __device__ uint32_t broadphase(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
+                                   BlockShared &sh)
+    {
+        const uint32_t nbp = W.n_bp;
+        const uint32_t eb = 2 * W.bp_off;
+        FatBox *fat = E.fat + W.bp_off;
+        uint32_t *ep_key = E.ep_key + eb;
+        uint32_t *ep_id = E.ep_id + eb;
+        uint32_t *ep_pos = E.ep_pos + eb;
+
+        // object update (update_broad_phase_aabbs + broad_phase_move_swept)
+        for (uint32_t o = tm.rank(); o < nbp; o += tm.size())
+        {
+            const uint32_t lc = E.bp_coll[W.bp_off + o];
+            const uint32_t gc = W.coll_off + lc;
+            if (E.c_static[gc])
+                continue;
+            const uint32_t gb = W.body_off + E.c_body[gc];
+            const tf<double> t = collider_tf_d(E, gc, gb);
+            aabb tight = compute_aabb(E.shape[gc], t, E.hulls);
+            if (E.use_vel_exp)
+            {
+                const V4<T> lv = E.B.lin[gb];
+                const vec3<double> dv = vec3<double>(double(lv.x), double(lv.y), double(lv.z)) * E.dt_frame;
+                const double m = E.fat_margin;
+                const vec3<double> emn(m + (dv.x < 0 ? -dv.x : 0.0), m + (dv.y < 0 ? -dv.y : 0.0), m + (dv.z < 0 ? -dv.z : 0.0));
+                const vec3<double> emx(m + (dv.x > 0 ? dv.x : 0.0), m + (dv.y > 0 ? dv.y : 0.0), m + (dv.z > 0 ? dv.z : 0.0));
+                tight = aabb{tight.mn - emn, tight.mx + emx};
+            }
+            const aabb f0 = load_fat(fat[o]);
+            if (aabb_contained(tight, f0))
+                continue;
+            const aabb f1 = aabb_expand(tight, E.fat_margin + E.reinsert_threshold);
+            FatBox fb;
+            fb.mn[0] = f1.mn.x; fb.mn[1] = f1.mn.y; fb.mn[2] = f1.mn.z;
+            fb.mx[0] = f1.mx.x; fb.mx[1] = f1.mx.y; fb.mx[2] = f1.mx.z;
+            fat[o] = fb;
+            ep_key[ep_pos[2 * o]] = order_key(__double2float_rn(f1.mn.x));
+            ep_key[ep_pos[2 * o + 1]] = order_key(__double2float_rn(f1.mx.x));
+        }
+        tm.sync();
+        return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, 2 * nbp, W.pair_cap, E.error, S, sh);
+    }
+
+    // Filtered SAP pairs followed by the plane candidates; returns the count.
+    template <class T, class P, class Team>
+    __device__ uint32_t build_candidates(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
+                                         uint32_t n_pairs, BlockShared &sh)
+    {
+        // SAP pair (lo, hi) user ids, filters of run_narrow_phase (CollisionPipeline.cpp:121-133)
+        for (uint32_t k = tm.rank(); k < n_pairs; k += tm.size())
+        {
+            const uint32_t r = S.pv[k];
+            const uint32_t oa = r < n_pairs ? S.pr_a[r] : ~0u;
+            const uint32_t ob = r < n_pairs ? S.pr_b[r] : ~0u;
+            if (oa >= W.n_bp || ob >= W.n_bp)
+            {
+                // corrupt pair record: report it and drop the pair
+                set_error(E.error, kErrInternal);
+                S.pk[k] = 0;
+                S.pk2[k] = 0;
+                S.cflag[k] = 0;
+                continue;
+            }
+            const uint32_t ua = E.bp_coll[W.bp_off + oa];
+            const uint32_t ub = E.bp_coll[W.bp_off + ob];
+            const uint32_t lo = ua < ub ? ua : ub;
+            const uint32_t hi = ua < ub ? ub : ua;
+            S.pk[k] = lo;
+            S.pk2[k] = hi;
+            const uint32_t ga = W.coll_off + lo, gb = W.coll_off + hi;
+            const bool keep = !(E.c_static[ga] && E.c_static[gb]) && (E.c_body[ga] != E.c_body[gb]);
+            S.cflag[k] = keep ? 1u : 0u;
+            if (E.dump_pairs && W.dump_slot != ~0u && k < E.dump_pair_cap)
+            {
+                uint32_t *dp = E.dump_pairs + (size_t)W.dump_slot * 2 * E.dump_pair_cap;
+                dp[2 * k] = lo;
+                dp[2 * k + 1] = hi;
+            }
+        }
+        tm.sync();
+        const uint32_t n_sap = team_excl_scan(tm, S.cflag, S.cflag, n_pairs, S.tile_sums, sh);
+        for (uint32_t k = tm.rank(); k < n_pairs; k += tm.size())
+        {
+            const uint32_t lo = S.pk[k], hi = S.pk2[k];
+            const uint32_t ga = W.coll_off + lo, gb = W.coll_off + hi;
+            const bool keep = lo != hi && !(E.c_static[ga] && E.c_static[gb]) && (E.c_body[ga] != E.c_body[gb]);
+            if (keep)
+                S.cand[S.cflag[k]] = Cand{lo, hi, E.c_body[ga], E.c_body[gb]};
+        }
+        for (uint32_t q = tm.rank(); q < W.n_pc; q += tm.size())
+        {
+            const uint2 pc = E.plane_cand[W.pc_off + q];
+            S.cand[n_sap + q] = Cand{pc.x, pc.y, E.c_body[W.coll_off + pc.x], E.c_body[W.coll_off + pc.y]};
+        }
+        tm.sync();
+        return n_sap + W.n_pc;
+    }
+
+    // Jones-Plassmann colouring: a candidate takes the lowest colour free
+    // on both of its dynamic bodies once it holds the highest priority
+    // among the uncoloured candidates sharing them.  Candidates whose bodies
+    // have used all 64 colours go to the serial colour.  Returns the number
+    // of regular colours; corder / colour offsets are filled.
+    template <class T, class P, class Team>
+    __device__ uint32_t color_candidates(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
+                                         uint32_t n_cand)
+    {
+        uint32_t *misc = S.misc;
+        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+            S.color[c] = 0xffffffffu;
+        for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+        {
+            S.bmask[b] = 0ull;
+            S.bprio[b] = 0ull;
+        }
+        for (uint32_t x = tm.rank(); x < kMaxColorRounds + 2 * 66; x += tm.size())
+            misc[kMiscCCount + x] = 0u;
+        tm.sync();
+        const uint8_t *type = E.B.type + W.body_off;
+        uint32_t round = 1;
+        for (; round <= kMaxColorRounds; ++round)
+        {
+            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+            {
+                if (S.color[c] != 0xffffffffu)
+                    continue;
+                const Cand cd = S.cand[c];
+                const unsigned long long val = ((unsigned long long)round << 56) |
+                                               ((unsigned long long)(hash32(c) & 0xffffffu) << 32) | c;
+                if (type[cd.ba] == kDynamic)
+                    atomicMax(&S.bprio[cd.ba], val);
+                if (type[cd.bb] == kDynamic)
+                    atomicMax(&S.bprio[cd.bb], val);
+            }
+            tm.sync();
+            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+            {
+                if (S.color[c] != 0xffffffffu)
+                    continue;
+                const Cand cd = S.cand[c];
+                const unsigned long long val = ((unsigned long long)round << 56) |
+                                               ((unsigned long long)(hash32(c) & 0xffffffu) << 32) | c;
+                const bool da = type[cd.ba] == kDynamic, db = type[cd.bb] == kDynamic;
+                const bool won = (!da || S.bprio[cd.ba] == val) && (!db || S.bprio[cd.bb] == val);
+                if (!won)
+                {
+                    atomicAdd(&misc[kMiscLeft + round - 1], 1u);
+                    continue;
+                }
+                const unsigned long long used = (da ? S.bmask[cd.ba] : 0ull) | (db ? S.bmask[cd.bb] : 0ull);
+                uint32_t col;
+                if (used == ~0ull)
+                    col = kColorSerial;
+                else
+                {
+                    col = (uint32_t)(__ffsll((long long)~used) - 1);
+                    const unsigned long long bit = 1ull << col;
+                    if (da)
+                        S.bmask[cd.ba] |= bit;
+                    if (db)
+                        S.bmask[cd.bb] |= bit;
+                }
+                S.color[c] = col;
+            }
+            tm.sync();
+            if (misc[kMiscLeft + round - 1] == 0u)
+                break;
+        }
+        if (round > kMaxColorRounds)
+        {
+            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+                if (S.color[c] == 0xffffffffu)
+                    S.color[c] = kColorSerial;
+            tm.sync();
+        }
+        // bucket by colour
+        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+            atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
+        tm.sync();
+        if (tm.leader())
+        {
+            uint32_t run = 0, ncol = 0;
+            for (uint32_t k = 0; k <= kColorSerial; ++k)
+            {
+                const uint32_t n = misc[kMiscCCount + k];
+                misc[kMiscCOff + k] = run;
+                misc[kMiscCCount + k] = run; // becomes the fill cursor
+                if (n && k < kColorSerial)
+                    ncol = k + 1;
+                run += n;
+            }
+            misc[kMiscCOff + kColorSerial + 1] = run;
+            misc[kMiscFlags + 1] = ncol;
+        }
+        tm.sync();
+        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+        {
+            const uint32_t slot = atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
+            S.corder[slot] = c;
+        }
+        tm.sync();
+        return misc[kMiscFlags + 1];
+    }
+
+    // Narrowphase of one candidate + emit_contact (CollisionPipeline.cpp:59-104).
+    template <class T, class P>
+    __device__ __forceinline__ void narrow_candidate(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+                                                     CandContacts<T, P> &out, uint32_t &n_gjk)
+    {
+        if (cd.ca >= W.n_coll || cd.cb >= W.n_coll || cd.ba >= W.n_bodies || cd.bb >= W.n_bodies)
+        {
+            set_error(E.error, kErrInternal);
+            out.n = 0;
+            return;
+        }
+        const uint32_t gca = W.coll_off + cd.ca, gcb = W.coll_off + cd.cb;
+        const uint32_t gba = W.body_off + cd.ba, gbb = W.body_off + cd.bb;
+        const tf<T> ta = collider_tf(E, gca, gba);
+        const tf<T> tb = collider_tf(E, gcb, gbb);
+        Manifold<T> m;
+        m.n = 0;
+        const int res = dispatch_pair(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, m);
+        if (res == kNeedsGjk)
+            ++n_gjk;
+        const int n = (res == kHit) ? m.n : 0;
+        out.n = n;
+        if (n == 0)
+            return;
+        out.normal = v4(m.normal);
+        const V4<T> ma = E.c_mat[gca], mb = E.c_mat[gcb];
+        out.mat = V4<T>{rmin(ma.x, mb.x), (ma.y + mb.y) * T(0.5), (ma.z + mb.z) * T(0.5), T(0)};
+        const vec3<T> xa = E.B.x(gba), xb = E.B.x(gbb);
+        const quat<T> qa = conjugate(E.B.q(gba)), qb = conjugate(E.B.q(gbb));
+        for (int k = 0; k < n; ++k)
+        {
+            const T half = m.depth[k] * T(0.5);
+            const vec3<T> pa = m.pos[k] + m.normal * half;
+            const vec3<T> pb = m.pos[k] - m.normal * half;
+            ContactPt<T, P> &c = out.pt[k];
+            c.ra = v4(rotate(qa, pa - xa));
+            c.rb = v4(rotate(qb, pb - xb));
+            c.pa = V4<P>{P(pa.x), P(pa.y), P(pa.z), P(0)};
+            c.pb = V4<P>{P(pb.x), P(pb.y), P(pb.z), P(0)};
+            c.lam_n = T(0.0);
+            c.lam_t = T(0.0);
+            c.vrel = T(0.0);
+            c.depth = m.depth[k];
+            c.coll = 0;
+        }
+    }
+
+    template <class T, class P>
+    __device__ __forceinline__ void solve_cand_position(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+                                                        CandContacts<T, P> &cc)
+    {
+        const int n = cc.n;
+        if (n == 0)
+            return;
+        const vec3<T> nrm = v3(cc.normal);
+        const T sf = cc.mat.y;
+        const uint32_t ba = W.body_off + cd.ba, bb = W.body_off + cd.bb;
+        for (int k = 0; k < n; ++k)
+            contact_position(E.B, ba, bb, nrm, sf, cc.pt[k], E.inv_h);
+    }
+
+    template <class T, class P>
+    __device__ __forceinline__ void solve_cand_velocity(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+                                                        const CandContacts<T, P> &cc)
+    {
+        const int n = cc.n;
+        if (n == 0)
+            return;
+        const vec3<T> nrm = v3(cc.normal);
+        const uint32_t ba = W.body_off + cd.ba, bb = W.body_off + cd.bb;
+        for (int k = 0; k < n; ++k)
+            contact_velocity(E.B, ba, bb, nrm, cc.mat.x, cc.mat.z, cc.pt[k], E.h);
+    }
+
+    template <class T, class P>
+    __device__ __forceinline__ Row<T> *joint_rows(const Engine<T, P> &E, const Joint<T> &j)
+    {
+        return E.rows + j.row0;
+    }
+
+    // ------------------------------------------------------------ the step
+    template <class T, class P, class Team>
+    __device__ void world_step(const Engine<T, P> &E, const Team &tm, uint32_t w, char *scratch_base, BlockShared &sh)
+    {
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = scratch_ptrs<T, P>(scratch_base, E.lay);
+        if (tm.leader())
+            S.misc[kMiscFlags + 3] = 0u;
+        const uint32_t n_pairs = broadphase(E, tm, W, S, sh);
+        const uint32_t n_cand = build_candidates(E, tm, W, S, n_pairs, sh);
+        const bool colored = E.solve_mode == 1;
+        uint32_t n_colors = 0;
+        if (colored)
+            n_colors = color_candidates(E, tm, W, S, n_cand);
+        const uint32_t *coff = S.misc + kMiscCOff;
+        Bodies<T, P> B = E.B;
+        uint32_t n_gjk = 0;
+
+        for (int sub = 0; sub < E.substeps; ++sub)
+        {
+            // narrowphase + contacts.clear() / emit (every substep, World.hpp:205-206)
+            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+                narrow_candidate(E, W, S.cand[c], S.cc[c], n_gjk);
+            tm.sync();
+            // integrate (Body.cpp:18-39)
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+                integrate_body(B, W.body_off + b, E.h);
+            tm.sync();
+            // position solve (World.hpp:168-173)
+            if (!colored)
+            {
+                if (tm.leader())
+                {
+                    for (uint32_t c = 0; c < n_cand; ++c)
+                        solve_cand_position(E, W, S.cand[c], S.cc[c]);
+                    for (uint32_t j = 0; j < W.n_joints; ++j)
+                    {
+                        Joint<T> jt = E.joints[W.joint_off + j];
+                        joint_errors(B, jt, joint_rows(E, jt), E.h);
+                        E.joints[W.joint_off + j].target_pos = jt.target_pos;
+                    }
+                    for (uint32_t r = 0; r < W.n_rows; ++r)
+                        solve_row(B, E.rows[W.row_off + r], E.inv_h);
+                }
+                tm.sync();
+            }
+            else
+            {
+                for (uint32_t col = 0; col < n_colors; ++col)
+                {
+                    for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
+                    {
+                        const uint32_t c = S.corder[q];
+                        solve_cand_position(E, W, S.cand[c], S.cc[c]);
+                    }
+                    tm.sync();
+                }
+                if (tm.leader())
+                    for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
+                    {
+                        const uint32_t c = S.corder[q];
+                        solve_cand_position(E, W, S.cand[c], S.cc[c]);
+                    }
+                tm.sync();
+                for (uint32_t j = tm.rank(); j < W.n_joints; j += tm.size())
+                {
+                    Joint<T> jt = E.joints[W.joint_off + j];
+                    joint_errors(B, jt, joint_rows(E, jt), E.h);
+                    E.joints[W.joint_off + j].target_pos = jt.target_pos;
+                }
+                tm.sync();
+                const uint32_t *jco = E.jcolor_off + W.jc_off;
+                for (uint32_t jc = 0; jc < W.n_jcolors; ++jc)
+                {
+                    for (uint32_t q = jco[jc] + tm.rank(); q < jco[jc + 1]; q += tm.size())
+                    {
+                        const Joint<T> &jt = E.joints[W.joint_off + E.jorder[q]];
+                        Row<T> *rows = joint_rows(E, jt);
+                        for (int r = 0; r < jt.count; ++r)
+                            solve_row(B, rows[r], E.inv_h);
+                    }
+                    tm.sync();
+                }
+            }
+            // velocity update (Body.cpp:41-57)
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+                update_velocity_body(B, W.body_off + b, E.inv_h);
+            tm.sync();
+            // velocity solve (World.hpp:176-180)
+            if (!colored)
+            {
+                if (tm.leader())
+                {
+                    for (uint32_t c = 0; c < n_cand; ++c)
+                        solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
+                    for (uint32_t j = 0; j < W.n_joints; ++j)
+                        joint_damping(B, E.joints[W.joint_off + j], E.h);
+                }
+                tm.sync();
+            }
+            else
+            {
+                for (uint32_t col = 0; col < n_colors; ++col)
+                {
+                    for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
+                    {
+                        const uint32_t c = S.corder[q];
+                        solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
+                    }
+                    tm.sync();
+                }
+                if (tm.leader())
+                    for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
+                    {
+                        const uint32_t c = S.corder[q];
+                        solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
+                    }
+                tm.sync();
+                const uint32_t *jco = E.jcolor_off + W.jc_off;
+                for (uint32_t jc = 0; jc < W.n_jcolors; ++jc)
+                {
+                    for (uint32_t q = jco[jc] + tm.rank(); q < jco[jc + 1]; q += tm.size())
+                        joint_damping(B, E.joints[W.joint_off + E.jorder[q]], E.h);
+                    tm.sync();
+                }
+            }
+        }
+
+        // statistics and parity dumps of the last substep
+        uint32_t *ncon = S.misc + kMiscFlags + 2;
+        if (tm.leader())
+            *ncon = 0;
+        tm.sync();
+        uint32_t local = 0;
+        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+        {
+            local += S.cc[c].n;
+            if (E.dump_cc && W.dump_slot != ~0u && c < E.dump_cand_cap)
+            {
+                const size_t o = (size_t)W.dump_slot * E.dump_cand_cap + c;
+                E.dump_cand[o] = S.cand[c];
+                E.dump_cc[o] = S.cc[c];
+                E.dump_color[o] = colored ? S.color[c] : 0u;
+            }
+        }
+        if (local)
+            atomicAdd(ncon, local);
+        if (n_gjk)
+            atomicAdd(S.misc + kMiscFlags + 3, n_gjk);
+        tm.sync();
+        if (tm.leader())
+        {
+            WorldStats st;
+            st.n_pairs = n_pairs;
+            st.n_cand = n_cand;
+            st.n_contacts = *ncon;
+            st.n_colors = n_colors;
+            st.n_serial = colored ? coff[kColorSerial + 1] - coff[kColorSerial] : 0u;
+            st.n_gjk = S.misc[kMiscFlags + 3];
+            st.pad_[0] = st.pad_[1] = 0;
+            E.stats[w] = st;
+            S.misc[kMiscFlags + 3] = 0;
+        }
+        tm.sync();
+    }
+
+    // ------------------------------------------------------------ kernels
+    constexpr int kMaxBlock = 256;
+
+    // Persistent CTAs pull whole worlds (largest first) from a work counter.
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_step_small(const Engine<T, P> E)
+    {
+        __shared__ BlockShared sh;
+        __shared__ uint32_t next;
+        BlockTeam tm;
+        char *scratch = E.scratch + (size_t)blockIdx.x * E.lay.stride;
+        if (threadIdx.x == 0)
+            scratch_ptrs<T, P>(scratch, E.lay).misc[kMiscFlags + 3] = 0;
+        for (;;)
+        {
+            if (threadIdx.x == 0)
+                next = atomicAdd(E.work_counter, 1u);
+            __syncthreads();
+            const uint32_t q = next;
+            __syncthreads();
+            if (q >= E.n_small)
+                break;
+            world_step(E, tm, E.small_worlds[q], scratch, sh);
+        }
+    }
+
+    // One large world on the whole cooperative grid.
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_step_big(const Engine<T, P> E, uint32_t w)
+    {
+        __shared__ BlockShared sh;
+        GridTeam tm;
+        world_step(E, tm, w, E.scratch, sh);
+    }
+
+    template <class T, class P>
+    cudaError_t launch_step_small(const Engine<T, P> &e, int grid, int block, cudaStream_t stream)
+    {
+        k_step_small<T, P><<<grid, block, 0, stream>>>(e);
+        return cudaGetLastError();
+    }
+
+    template <class T, class P>
+    cudaError_t launch_step_big(const Engine<T, P> &e, uint32_t world, int grid, int block, cudaStream_t stream)
+    {
+        Engine<T, P> ec = e;
+        void *args[] = {(void *)&ec, (void *)&world};
+        return cudaLaunchCooperativeKernel((const void *)k_step_big<T, P>, dim3(grid), dim3(block), args, 0, stream);
+    }
+
+    template <class T, class P>
+    cudaError_t occupancy_small(int block, int *blocks_per_sm)
+    {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_small<T, P>, block, 0);
+    }
+
+    template <class T, class P>
+    cudaError_t occupancy_big(int block, int *blocks_per_sm)
+    {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_big<T, P>, block, 0);
+    }
+} // namespace rbps_gpu
+
+#define RBPS_INSTANTIATE_ENGINE(T, P)                                                                          \
+    template cudaError_t rbps_gpu::launch_step_small<T, P>(const rbps_gpu::Engine<T, P> &, int, int, cudaStream_t); \
+    template cudaError_t rbps_gpu::launch_step_big<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int, int,        \
+                                                         cudaStream_t);                                           \
+    template cudaError_t rbps_gpu::occupancy_small<T, P>(int, int *);                                              \
+    template cudaError_t rbps_gpu::occupancy_big<T, P>(int, int *);                                               \
+    template cudaError_t rbps_gpu::launch_debug_broadphase<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int,    \
+                                                                 uint32_t *, cudaStream_t);
+
+namespace rbps_gpu
+{
+    // Diagnostics: only the frame's broadphase + candidate build of one
+    // world on one CTA (the first phase of world_step).
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_debug_broadphase(const Engine<T, P> E, uint32_t w, uint32_t *out)
+    {
+        __shared__ BlockShared sh;
+        BlockTeam tm;
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = scratch_ptrs<T, P>(E.scratch, E.lay);
+        const uint32_t n_pairs = broadphase(E, tm, W, S, sh);
+        const uint32_t n_cand = build_candidates(E, tm, W, S, n_pairs, sh);
+        if (threadIdx.x == 0)
+        {
+            out[0] = n_pairs;
+            out[1] = n_cand;
+        }
+    }
+
+    template <class T, class P>
+    cudaError_t launch_debug_broadphase(const Engine<T, P> &e, uint32_t w, int block, uint32_t *out,
+                                        cudaStream_t stream)
+    {
+        k_debug_broadphase<T, P><<<1, block, 0, stream>>>(e, w, out);
+        return cudaGetLastError();
+    }
+} // namespace rbps_gpu

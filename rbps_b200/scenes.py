@@ -1,0 +1,347 @@
+"""Seeded synthetic scenes for the RBPS hot-path workloads.
+
+Every scene is plain data (numpy arrays of the C ABI descriptor structs), so
+the identical scene can be built in the GPU engine and in the reference
+engine.  One ``numpy.random.Generator(PCG64(seed))`` per scene draws, per
+body and in this order: shape type, size, orientation (normalised 4-D
+Gaussian), position, velocity.
+
+Mass properties use density 1000 kg/m^3 and the reference's unit-density
+formulas (Sphere.hpp:54-80, Box.hpp:72-86, Capsule.hpp:83-118); gravity is
+set explicitly through the body force, ``(0, -g*m, 0)``.
+"""
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+import math
+
+import numpy as np
+
+from . import abi
+
+DENSITY = 1000.0
+PI = 3.14159265358979323846
+
+
+@dataclass
+class WorldSpec:
+    bodies: np.ndarray                 # abi.BODY_DT
+    forces: np.ndarray                 # (n, 3) float64
+    colliders: np.ndarray              # abi.COLLIDER_DT
+    joints: np.ndarray                 # abi.JOINT_DT
+    hulls: List[Tuple[np.ndarray, np.ndarray]] = field(default_factory=list)
+
+    @property
+    def n_bodies(self):
+        return len(self.bodies)
+
+    @property
+    def n_dynamic(self):
+        return int(np.count_nonzero(self.bodies["type"] == abi.BODY_DYNAMIC))
+
+
+@dataclass
+class Scene:
+    name: str
+    timestep: float
+    substeps: int
+    steps: int
+    worlds: List[WorldSpec]
+    description: str = ""
+
+    @property
+    def n_bodies(self):
+        return sum(w.n_bodies for w in self.worlds)
+
+    @property
+    def n_dynamic(self):
+        return sum(w.n_dynamic for w in self.worlds)
+
+
+# ------------------------------------------------------------ mass properties
+def sphere_mass(r):
+    vol = (4.0 / 3.0) * PI * r * r * r
+    i = (2.0 / 5.0) * vol * r * r
+    return vol * DENSITY, np.array([i, i, i, 0.0, 0.0, 0.0]) * DENSITY
+
+
+def box_mass(h):
+    x2, y2, z2 = 4.0 * h[0] * h[0], 4.0 * h[1] * h[1], 4.0 * h[2] * h[2]
+    vol = 8.0 * h[0] * h[1] * h[2]
+    return vol * DENSITY, np.array([(1.0 / 12.0) * vol * (y2 + z2),
+                                    (1.0 / 12.0) * vol * (x2 + z2),
+                                    (1.0 / 12.0) * vol * (x2 + y2), 0.0, 0.0, 0.0]) * DENSITY
+
+
+def capsule_mass(hh, r):
+    r2, h2 = r * r, hh * hh
+    vol = PI * r * r * (2.0 * hh + (4.0 / 3.0) * r)
+    m_cyl = PI * r2 * 2.0 * hh
+    m_hemi = vol - m_cyl
+    iyy = (m_cyl * r2 / 2.0) + (m_hemi * 2.0 * r2 / 5.0)
+    d = hh + 3.0 * r / 8.0
+    ixx = m_cyl * (r2 / 4.0 + h2 / 3.0) + m_hemi * (2.0 * r2 / 5.0 + d * d)
+    return vol * DENSITY, np.array([ixx, iyy, ixx, 0.0, 0.0, 0.0]) * DENSITY
+
+
+def hull_mass(verts, tris):
+    """Volume and inertia about the origin of a closed CCW triangle mesh
+    (signed tetrahedra from the origin), scaled by the density."""
+    a, b, c = verts[tris[:, 0]], verts[tris[:, 1]], verts[tris[:, 2]]
+    det = np.einsum("ij,ij->i", a, np.cross(b, c))
+    vol = det.sum() / 6.0
+    # second moments of each tetra (origin, a, b, c)
+    def s(u, v):
+        return (a[:, u] * a[:, v] + b[:, u] * b[:, v] + c[:, u] * c[:, v]
+                + (a[:, u] + b[:, u] + c[:, u]) * (a[:, v] + b[:, v] + c[:, v])) / 120.0 * det
+    sxx, syy, szz = s(0, 0).sum(), s(1, 1).sum(), s(2, 2).sum()
+    sxy, sxz, syz = s(0, 1).sum(), s(0, 2).sum(), s(1, 2).sum()
+    inertia = np.array([syy + szz, sxx + szz, sxx + syy, -sxy, -sxz, -syz])
+    return vol * DENSITY, inertia * DENSITY
+
+
+# ------------------------------------------------------------------ helpers
+def random_quats(rng, n):
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    return q
+
+
+def _ground(bodies, colliders, forces, friction, restitution, offset=(0.0, 0.0, 0.0)):
+    """Static ground body (id 0) with Plane{(0,1,0), 0} (Plane.hpp:32-58)."""
+    b = abi.body_default()
+    b["type"] = abi.BODY_STATIC
+    b["mass"] = 0.0
+    b["position"] = offset
+    bodies.append(b)
+    forces.append((0.0, 0.0, 0.0))
+    c = abi.collider_default()
+    c["shape"] = abi.SHAPE_PLANE
+    c["params"] = (0.0, 1.0, 0.0, 0.0)
+    c["body_id"] = 0
+    c["is_static"] = 1
+    c["restitution"] = restitution
+    c["static_friction"] = friction
+    c["dynamic_friction"] = friction
+    colliders.append(c)
+
+
+def _dyn_body(pos, quat, mass, inertia, vel=(0.0, 0.0, 0.0), g=9.81):
+    b = abi.body_default()
+    b["type"] = abi.BODY_DYNAMIC
+    b["mass"] = mass
+    b["inertia"] = inertia
+    b["position"] = pos
+    b["orientation"] = quat
+    b["linear_velocity"] = vel
+    return b, (0.0, -g * mass, 0.0)
+
+
+def _collider(shape, params, body, friction, restitution, hull=0):
+    c = abi.collider_default()
+    c["shape"] = shape
+    p = list(params) + [0.0] * (4 - len(params))
+    c["params"] = p
+    c["hull"] = hull
+    c["body_id"] = body
+    c["restitution"] = restitution
+    c["static_friction"] = friction
+    c["dynamic_friction"] = friction
+    return c
+
+
+def _finish(bodies, forces, colliders, joints, hulls=None):
+    return WorldSpec(
+        bodies=np.array(bodies, dtype=abi.BODY_DT),
+        forces=np.array(forces, dtype=np.float64).reshape(-1, 3),
+        colliders=np.array(colliders, dtype=abi.COLLIDER_DT),
+        joints=np.array(joints, dtype=abi.JOINT_DT) if joints else np.zeros(0, abi.JOINT_DT),
+        hulls=hulls or [])
+
+
+def box_sphere_world(rng, n, friction=0.5, restitution=0.0,
+                     lo=(-5.0, 1.0, -5.0), hi=(5.0, 21.0, 5.0), g=9.81,
+                     ground=True, size=(0.2, 0.5)):
+    """A ground plane plus n bodies, each a box (half-extents U[size]^3) or a
+    sphere (radius U[size]) with probability 1/2, uniform random orientation,
+    position uniform in [lo, hi], at rest.  Returns lists (not yet arrays)."""
+    bodies, forces, colliders = [], [], []
+    if ground:
+        _ground(bodies, colliders, forces, friction, restitution)
+    is_box = rng.random(n) < 0.5
+    box_h = rng.uniform(size[0], size[1], (n, 3))
+    sph_r = rng.uniform(size[0], size[1], n)
+    quats = random_quats(rng, n)
+    pos = rng.uniform(lo, hi, (n, 3))
+    for i in range(n):
+        bid = len(bodies)
+        if is_box[i]:
+            m, inertia = box_mass(box_h[i])
+            b, f = _dyn_body(pos[i], quats[i], m, inertia, g=g)
+            c = _collider(abi.SHAPE_BOX, box_h[i], bid, friction, restitution)
+        else:
+            m, inertia = sphere_mass(sph_r[i])
+            b, f = _dyn_body(pos[i], quats[i], m, inertia, g=g)
+            c = _collider(abi.SHAPE_SPHERE, [sph_r[i]], bid, friction, restitution)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(c)
+    return bodies, forces, colliders
+
+
+def capsule_chain(bodies, forces, colliders, joints, origin, n_links=13, radius=0.1,
+                  half_height=0.2, friction=0.5, restitution=0.0, g=9.81,
+                  limit=None, compliance=0.0, damping=0.0, gap=0.02):
+    """n_links capsules laid along +X from `origin`, each link's local Y axis
+    mapped to world X, joined by revolute joints about world Z
+    (RevoluteJointParams, JointAPI.hpp:43-57) at anchors `gap` beyond the
+    capsule tips.  The defaults are the settings under which the reference
+    engine stays finite: with tips touching (gap=0), or with joint damping /
+    angle limits among falling bodies, the reference's joint rows and
+    contacts fight and its chains blow up to NaN within a few hundred steps."""
+    q = (math.cos(-PI / 4.0), 0.0, 0.0, math.sin(-PI / 4.0))  # local +Y -> world +X
+    reach = half_height + radius + gap
+    m, inertia = capsule_mass(half_height, radius)
+    first = len(bodies)
+    for k in range(n_links):
+        pos = (origin[0] + k * 2.0 * reach, origin[1], origin[2])
+        b, f = _dyn_body(pos, q, m, inertia, g=g)
+        bid = len(bodies)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(_collider(abi.SHAPE_CAPSULE, [half_height, radius], bid, friction, restitution))
+    for k in range(n_links - 1):
+        j = abi.joint_default(abi.JOINT_REVOLUTE)
+        j["body_1"] = first + k
+        j["body_2"] = first + k + 1
+        j["axis"] = (0.0, 0.0, 1.0)
+        j["limit_axis"] = (0.0, 1.0, 0.0)
+        j["r_1"] = (0.0, reach, 0.0)
+        j["r_2"] = (0.0, -reach, 0.0)
+        j["compliance"] = compliance
+        j["damping"] = damping
+        j["limited"] = 1 if limit is not None else 0
+        j["lower_limit"] = -(limit or 0.0)
+        j["upper_limit"] = (limit or 0.0)
+        joints.append(j)
+
+
+# ------------------------------------------------------------------ configs
+def config0(seed=0, n_bodies=512, steps=600):
+    """Plain single world, FP64: 256 boxes + 256 spheres (equal split of the
+    types, shuffled), sizes U[0.2,0.5], random orientation, positions in
+    [-5,5]x[1,21]x[-5,5] over a static ground plane, at rest, g=-9.81,
+    dt=1/60, 10 substeps, friction 0.5, restitution 0."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    bodies, forces, colliders = [], [], []
+    _ground(bodies, colliders, forces, 0.5, 0.0)
+    types = np.array([1] * (n_bodies // 2) + [0] * (n_bodies - n_bodies // 2))
+    rng.shuffle(types)
+    box_h = rng.uniform(0.2, 0.5, (n_bodies, 3))
+    sph_r = rng.uniform(0.2, 0.5, n_bodies)
+    quats = random_quats(rng, n_bodies)
+    pos = rng.uniform((-5.0, 1.0, -5.0), (5.0, 21.0, 5.0), (n_bodies, 3))
+    for i in range(n_bodies):
+        bid = len(bodies)
+        if types[i]:
+            m, inertia = box_mass(box_h[i])
+            c = _collider(abi.SHAPE_BOX, box_h[i], bid, 0.5, 0.0)
+        else:
+            m, inertia = sphere_mass(sph_r[i])
+            c = _collider(abi.SHAPE_SPHERE, [sph_r[i]], bid, 0.5, 0.0)
+        b, f = _dyn_body(pos[i], quats[i], m, inertia)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(c)
+    w = _finish(bodies, forces, colliders, [])
+    return Scene("config0_plain_fp64", 1.0 / 60.0, 10, steps, [w],
+                 f"{n_bodies} boxes+spheres over a ground plane, seed {seed}")
+
+
+def config3(seed=0, n_worlds=4096, steps=1000, lo_bodies=8, hi_bodies=512):
+    """Batched uneven worlds: per world n ~ log-uniform[8,512] boxes/spheres
+    (as config0) + one 13-link revolute capsule chain + ground plane,
+    dt=1/120, 4 substeps."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    counts = np.floor(np.exp(rng.uniform(math.log(lo_bodies), math.log(hi_bodies + 1), n_worlds))).astype(int)
+    counts = np.clip(counts, lo_bodies, hi_bodies)
+    worlds = []
+    for w in range(n_worlds):
+        bodies, forces, colliders = box_sphere_world(rng, int(counts[w]))
+        joints = []
+        origin = (rng.uniform(-4.5, -3.5), rng.uniform(1.0, 21.0), rng.uniform(-5.0, 5.0))
+        capsule_chain(bodies, forces, colliders, joints, origin)
+        worlds.append(_finish(bodies, forces, colliders, joints))
+    return Scene("config3_batched_fp32", 1.0 / 120.0, 4, steps, worlds,
+                 f"{n_worlds} worlds, bodies log-uniform[{lo_bodies},{hi_bodies}] + 13-link chain, seed {seed}")
+
+
+def config4(seed=0, n_worlds=256, steps=2000, height=64, offset=1.0e4):
+    """Precision stress: per world a tower of `height` boxes (half-extent
+    0.5), densities alternating 1:1000, offset `offset` m from the origin
+    plus a uniform horizontal jitter, ground plane at the offset, friction
+    0.8, 20 substeps."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    worlds = []
+    for w in range(n_worlds):
+        ox = offset + rng.uniform(-50.0, 50.0)
+        oz = offset + rng.uniform(-50.0, 50.0)
+        bodies, forces, colliders = [], [], []
+        _ground(bodies, colliders, forces, 0.8, 0.0, offset=(ox, 0.0, oz))
+        h = np.array([0.5, 0.5, 0.5])
+        for k in range(height):
+            m, inertia = box_mass(h)
+            scale = 1.0 if k % 2 == 0 else 1.0e-3
+            b, f = _dyn_body((ox, 0.5 + k * 1.0, oz), (1.0, 0.0, 0.0, 0.0), m * scale, inertia * scale)
+            bid = len(bodies)
+            bodies.append(b)
+            forces.append(f)
+            colliders.append(_collider(abi.SHAPE_BOX, h, bid, 0.8, 0.0))
+        worlds.append(_finish(bodies, forces, colliders, []))
+    return Scene("config4_precision", 1.0 / 60.0, 20, steps, worlds,
+                 f"{n_worlds} towers of {height} boxes at {offset} m, seed {seed}")
+
+
+def small_world(seed=0, n=64, **kw):
+    """A config0-style world with n bodies (for fast parity tests)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    bodies, forces, colliders = box_sphere_world(rng, n, **kw)
+    return _finish(bodies, forces, colliders, [])
+
+
+def chain_world(seed=0, n_bodies=16, n_links=13, **kw):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    bodies, forces, colliders = box_sphere_world(rng, n_bodies)
+    joints = []
+    origin = (rng.uniform(-4.5, -3.5), rng.uniform(1.0, 21.0), rng.uniform(-5.0, 5.0))
+    capsule_chain(bodies, forces, colliders, joints, origin, n_links=n_links, **kw)
+    return _finish(bodies, forces, colliders, joints)
+
+
+def capsule_world(seed=0, n=48, friction=0.5, restitution=0.0):
+    """Ground plane + a mix of capsules, boxes and spheres (exercises the
+    capsule pair routines)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    bodies, forces, colliders = [], [], []
+    _ground(bodies, colliders, forces, friction, restitution)
+    kind = rng.integers(0, 3, n)
+    quats = random_quats(rng, n)
+    pos = rng.uniform((-3.0, 1.0, -3.0), (3.0, 9.0, 3.0), (n, 3))
+    for i in range(n):
+        bid = len(bodies)
+        if kind[i] == 0:
+            hh, r = rng.uniform(0.1, 0.5), rng.uniform(0.1, 0.3)
+            m, inertia = capsule_mass(hh, r)
+            c = _collider(abi.SHAPE_CAPSULE, [hh, r], bid, friction, restitution)
+        elif kind[i] == 1:
+            h = rng.uniform(0.2, 0.5, 3)
+            m, inertia = box_mass(h)
+            c = _collider(abi.SHAPE_BOX, h, bid, friction, restitution)
+        else:
+            r = rng.uniform(0.2, 0.5)
+            m, inertia = sphere_mass(r)
+            c = _collider(abi.SHAPE_SPHERE, [r], bid, friction, restitution)
+        b, f = _dyn_body(pos[i], quats[i], m, inertia)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(c)
+    return _finish(bodies, forces, colliders, [])

@@ -1,0 +1,60 @@
+"""Colored (graph-coloured Gauss-Seidel) FP32 path.
+
+Colour validity is checked exactly: no two candidates of one colour share a
+dynamic body.  Physics is checked against the FP64 reference one step ahead
+(tolerance 1e-2 relative: Gauss-Seidel order differs, FP32 arithmetic) and
+for plausibility over many steps (finite, resting on the ground).
+"""
+import numpy as np
+import pytest
+
+from rbps_b200 import abi, scenes
+from helpers import load_golden, state_err
+
+pytestmark = pytest.mark.gpu
+
+
+def colour_valid(colors, ba, bb, dynamic):
+    seen = {}
+    for c, a, b in zip(colors, ba, bb):
+        if c == 64:      # serial overflow colour
+            continue
+        for x in (a, b):
+            if dynamic[x]:
+                key = (int(c), int(x))
+                if key in seen:
+                    return False
+                seen[key] = True
+    return True
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP32, abi.PRECISION_FP64])
+def test_colouring_is_valid(rbps, precision):
+    sc, _ = load_golden("boxsphere64_settled")
+    b = rbps.Batch.from_scene(sc, precision, abi.SOLVE_COLORED)
+    b.set_dump(True)
+    b.step(3)
+    col, ba, bb = b.colors(0)
+    dyn = sc.worlds[0].bodies["type"] == abi.BODY_DYNAMIC
+    assert len(col) > 0
+    assert colour_valid(col, ba, bb, dyn)
+    assert b.stats()["max_colors"] >= 2
+
+
+def test_colored_fp32_one_step_close(rbps):
+    sc, g = load_golden("boxsphere64_settled")
+    b = rbps.Batch.from_scene(sc, abi.PRECISION_FP32, abi.SOLVE_COLORED)
+    b.step(1)
+    ref1 = {k: g["s1_" + k] for k in ("position", "orientation", "linear_velocity", "angular_velocity")}
+    err = state_err(b.state(0), ref1)
+    assert err["position"] < 1e-2 and err["orientation"] < 1e-2, err
+
+
+def test_colored_batch_settles(rbps):
+    sc = scenes.config3(seed=5, n_worlds=16, steps=240)
+    b = rbps.Batch.from_scene(sc, abi.PRECISION_FP32, abi.SOLVE_COLORED)
+    b.step(240)
+    st = b.state_all(("position",))
+    assert np.isfinite(st["position"]).all()
+    # everything has fallen onto the ground plane (y >= -0.1) and stays low
+    assert st["position"][:, 1].min() > -0.2
