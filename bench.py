@@ -1,0 +1,311 @@
+#!/usr/bin/env python
+"""Batched-world step throughput on B200: body-substeps/s.
+
+Workload: 4,096 independent worlds, bodies per world log-uniform in [8,512]
+(random boxes and spheres, sizes U[0.2,0.5] m) plus one 13-link revolute
+capsule chain per world, over a ground plane; dt = 1/120 s, 4 substeps, FP32
+state, graph-coloured Gauss-Seidel; all worlds step in one launch per step.
+Seeded synthetic scene (rbps_b200.scenes.config3); under torchrun every rank
+steps its own 4,096 worlds (weak scaling, no collective on the step path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rbps|reference]
+
+Prints one JSON line (rank 0).  `value` = whole-job body-substeps/s from CUDA
+events on the step stream (max over ranks); `e2e` = the same metric through
+rbps_batch_step_io with page-locked host buffers (forces in, poses out,
+copies inside the timed region); `roofline` = the step kernel against the
+measured HBM copy bandwidth with the algorithmic byte model below;
+`cpu_baseline` = the reference engine (oracle/_ref, built from the
+reference's own sources) on a bounded sample of the same worlds, all host
+threads.  `--impl reference` times the reference CPU engine alone.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "body-substeps/s (batched FP32, 4096 uneven worlds + 13-link revolute chain each, 1 B200)"
+UNIT = "body-substeps/s"
+WORKLOAD = "config3_batched_uneven_worlds"
+
+
+def bytes_model(n_dyn, substeps, contacts, candidates, pairs, joints, colliders):
+    """Algorithmic bytes of one step (FP32 SoA, every compulsory element once
+    per phase that touches it):
+      per dynamic body per substep     336 B  (integrate 128R+104W, velocity update 56R+48W)
+      per contact point per substep    704 B  (position solve, velocity solve, narrowphase emit)
+      per narrowphase candidate / sub   88 B
+      per revolute joint per substep  1116 B  (4 rows, errors, damping)
+      per collider per frame           208 B  (AABB / fat update, endpoint sort, sweep)
+      per SAP pair per frame            56 B
+    """
+    per_sub = n_dyn * 336 + contacts * 704 + candidates * 88 + joints * 1116
+    return substeps * per_sub + colliders * 208 + pairs * 56
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id=None):
+        self.bus_id = bus_id  # PCI bus number (int) of the timed device, None = all rows
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = open(os.path.join(ROOT, ".clocks_tmp.csv"), "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.out.close()
+        path = os.path.join(ROOT, ".clocks_tmp.csv")
+        rows = []
+        with open(path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                if self.bus_id is not None:
+                    try:
+                        if int(parts[1].split(":")[1], 16) != int(self.bus_id):
+                            continue
+                    except (IndexError, ValueError):
+                        pass
+                rows.append(parts)
+        os.remove(path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_run(scene, warmup, steps, max_seconds, threads):
+    """The reference engine on the host cores: RefWorlds of the scene's worlds
+    (a prefix sample if needed to stay within max_seconds), `warmup` untimed
+    steps then `steps` timed; returns (body-substeps/s, info)."""
+    from oracle import ref
+    worlds = scene.worlds
+    # calibrate on a small prefix, then size the sample to the time budget
+    probe = [ref.RefWorld(w, scene.timestep, scene.substeps) for w in worlds[:256]]
+    t = ref.step_worlds(probe, 2, threads)
+    dyn_probe = sum(w.n_dynamic for w in worlds[:256])
+    rate = dyn_probe * scene.substeps * 2 / max(t, 1e-9) / 3.0  # contacts make later steps ~3x costlier
+    budget_bs = rate * max_seconds
+    total_bs = 0
+    n = 0
+    for w in worlds:
+        need = w.n_dynamic * scene.substeps * (steps + warmup)
+        if n >= 64 and total_bs + need > budget_bs:
+            break
+        total_bs += need
+        n += 1
+    del probe
+    sample = worlds[:n]
+    refs = [ref.RefWorld(w, scene.timestep, scene.substeps) for w in sample]
+    if warmup:
+        ref.step_worlds(refs, warmup, threads)
+    secs = ref.step_worlds(refs, steps, threads)
+    n_dyn = sum(w.n_dynamic for w in sample)
+    value = n_dyn * scene.substeps * steps / secs
+    info = f"{n} of {len(worlds)} worlds ({n_dyn} dynamic bodies), {warmup} untimed + {steps} timed steps, {secs:.2f} s"
+    return value, info
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="rbps", choices=["rbps", "reference"])
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--block", type=int, default=0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    ws, rank, local = dist_info()
+    from rbps_b200 import abi, scenes
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        scene = scenes.config3(seed=args.seed, n_worlds=args.worlds)
+        value, info = cpu_reference_run(scene, args.warmup, args.steps, max_seconds=150.0, threads=threads)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD, "worlds": args.worlds, "substeps": 4, "dt": 1 / 120,
+                           "solver": "reference sequential Gauss-Seidel (CPU)"},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                 "sample": info},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import rbps_b200
+
+    scene = scenes.config3(seed=args.seed + rank, n_worlds=args.worlds)
+    stream = torch.cuda.Stream()  # a real stream: the legacy NULL stream would not order our launches
+    torch.cuda.set_stream(stream)
+    batch = rbps_b200.Batch.from_scene(scene, abi.PRECISION_FP32, abi.SOLVE_COLORED, device=local,
+                                       stream=stream.cuda_stream, block_threads=args.block)
+    n_tot, n_dyn = batch.total_bodies()
+    n_coll = sum(len(w.colliders) for w in scene.worlds)
+    n_joints = sum(len(w.joints) for w in scene.worlds)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (untimed)
+    batch.step(args.warmup)
+    batch.synchronize()
+
+    # timed region: K steps, device events on the step stream
+    bus = None
+    try:
+        bus = torch.cuda.get_device_properties(local).pci_bus_id
+    except Exception:
+        pass
+    clocks = ClockSampler(bus)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    batch.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    st = batch.stats()
+    value = n_dyn * scene.substeps * args.steps * ws / (ms / 1e3)
+    ms_step = ms / args.steps
+
+    # roofline of the step kernel (one launch per step)
+    bmodel = bytes_model(n_dyn, scene.substeps, st["contacts"], st["candidates"], st["pairs"], n_joints, n_coll)
+    peak, peak_kind = measured_peaks()
+    achieved = bmodel / (ms_step / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f)
+        # DRAM bytes per launch from ncu on a smaller batch, scaled by dynamic bodies
+        traffic = tr["dram_bytes_per_launch"] * n_dyn / tr["dynamic_bodies"]
+
+    # end-to-end through the C ABI: forces in, poses out, pinned host buffers
+    f_host = torch.empty((n_tot, 3), dtype=torch.float64, pin_memory=True)
+    f_host.copy_(torch.from_numpy(np.concatenate([w.forces for w in scene.worlds])))
+    p_host = torch.empty((n_tot, 3), dtype=torch.float64, pin_memory=True)
+    q_host = torch.empty((n_tot, 4), dtype=torch.float64, pin_memory=True)
+    batch.step_io(f_host.data_ptr(), p_host.data_ptr(), q_host.data_ptr())  # stage buffers
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        batch.step_io(f_host.data_ptr(), p_host.data_ptr(), q_host.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = n_dyn * scene.substeps * args.e2e_steps * ws / (e2e_ms / 1e3)
+    finite = bool(np.isfinite(p_host.numpy()).all())
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            cv, info = cpu_reference_run(scene, args.warmup, min(args.steps, 40), args.cpu_seconds, threads)
+            cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "reference", "sample": info}
+        except Exception as e:  # the oracle library is missing
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "worlds_per_gpu": args.worlds, "bodies_per_gpu": n_tot,
+                           "dynamic_bodies_per_gpu": n_dyn, "substeps": scene.substeps, "dt": scene.timestep,
+                           "precision": "fp32", "solver": "graph-coloured Gauss-Seidel",
+                           "l2": "inputs larger than L2 (world state + per-CTA scratch >> 126 MB)",
+                           "parallelism": f"world-sharded replicas x{ws}", "seed": args.seed,
+                           "state_finite": finite},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "algorithmic_bytes_per_launch": bmodel, "kernel": "k_step_small"},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_tot * 24,
+                        "d2h_bytes_per_step": n_tot * 56, "steps": args.e2e_steps},
+                "clocks": clk,
+                "gpu_launches": int(st["kernel_launches"]),
+                "stats_last_step": {"pairs": st["pairs"], "candidates": st["candidates"],
+                                    "contacts": st["contacts"], "max_colors": st["max_colors"],
+                                    "serial_overflow": st["serial_overflow"]}}
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -213,6 +213,10 @@ RBPS_API int rbps_world_add_body(rbps_batch *batch, uint32_t world,
 /* Bulk form: n bodies, ids first_id .. first_id+n-1. */
 RBPS_API int rbps_world_add_bodies(rbps_batch *batch, uint32_t world, uint32_t n,
                                    const rbps_body_desc *descs, uint32_t *first_id);
+/* Bulk form of rbps_world_set_body_force for bodies first .. first+n-1
+ * (3 doubles each). */
+RBPS_API int rbps_world_set_body_forces(rbps_batch *batch, uint32_t world, uint32_t first, uint32_t n,
+                                        const double *force);
 /* Writes bodies.force / bodies.torque (Body.hpp BODY_FIELDS) of one body. */
 RBPS_API int rbps_world_set_body_force(rbps_batch *batch, uint32_t world, uint32_t body,
                                        const double force[3], const double torque[3]);
@@ -235,6 +239,15 @@ RBPS_API int rbps_batch_commit(rbps_batch *batch);
  * rbps_batch_synchronize / get_* call. */
 RBPS_API int rbps_batch_step(rbps_batch *batch, int32_t n_steps);
 RBPS_API int rbps_batch_synchronize(rbps_batch *batch);
+/* One World::step of every world with host I/O, for callers that feed
+ * forces and read poses every frame: copies force_in (3 doubles per body,
+ * all worlds in world order; NULL keeps the current forces) host -> device,
+ * steps, and copies positions (3 doubles per body) and orientations (4
+ * doubles, w,x,y,z) device -> host (either may be NULL).  Returns when the
+ * outputs are written.  Host buffers should be page-locked for full copy
+ * bandwidth. */
+RBPS_API int rbps_batch_step_io(rbps_batch *batch, const double *force_in, double *position_out,
+                                double *orientation_out);
 
 /* Per-world body state, host doubles (converted from the device precision). */
 RBPS_API int rbps_batch_get_state(rbps_batch *batch, uint32_t world, const rbps_state_view *view);

@@ -72,6 +72,8 @@ def lib():
             "rbps_world_add_body": (i, [_P, C.c_uint32, _P, _U]),
             "rbps_world_add_bodies": (i, [_P, C.c_uint32, C.c_uint32, _P, _U]),
             "rbps_world_set_body_force": (i, [_P, C.c_uint32, C.c_uint32, _D, _D]),
+            "rbps_world_set_body_forces": (i, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _D]),
+            "rbps_batch_step_io": (i, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
             "rbps_world_add_collider": (i, [_P, C.c_uint32, _P, _U]),
             "rbps_world_add_colliders": (i, [_P, C.c_uint32, C.c_uint32, _P, _U]),
             "rbps_world_add_joint": (i, [_P, C.c_uint32, _P, _U]),
@@ -141,7 +143,7 @@ class Batch:
 
     def __init__(self, n_worlds, timestep, substeps, precision=abi.PRECISION_FP64,
                  solve_mode=abi.SOLVE_REFERENCE_ORDER, fat_margin=0.1, reinsert_threshold=0.05,
-                 device=0, max_pairs_per_world=0, block_threads=0):
+                 device=0, max_pairs_per_world=0, block_threads=0, stream=None):
         L = lib()
         d = BatchDesc()
         L.rbps_batch_desc_default(C.byref(d))
@@ -155,6 +157,7 @@ class Batch:
         d.device = device
         d.max_pairs_per_world = max_pairs_per_world
         d.block_threads = block_threads
+        d.stream = stream
         h = _P()
         _check(L.rbps_batch_create(C.byref(d), C.byref(h)))
         self.h = h
@@ -184,8 +187,8 @@ class Batch:
         first = C.c_uint32(0)
         _check(L.rbps_world_add_bodies(self.h, w, len(bodies), C.c_void_p(bodies.ctypes.data), C.byref(first)))
         forces = np.ascontiguousarray(spec.forces, np.float64)
-        for i in range(len(bodies)):
-            _check(L.rbps_world_set_body_force(self.h, w, first.value + i, _dp(forces[i]), None))
+        if len(bodies):
+            _check(L.rbps_world_set_body_forces(self.h, w, first.value, len(bodies), _dp(forces)))
         cols = np.ascontiguousarray(spec.colliders).copy()
         if hull_base:
             m = cols["shape"] == abi.SHAPE_CONVEX_HULL
@@ -206,6 +209,10 @@ class Batch:
 
     def synchronize(self):
         _check(lib().rbps_batch_synchronize(self.h))
+
+    def step_io(self, force_ptr, pos_ptr, rot_ptr):
+        """One step with host I/O through raw host pointers (ints or None)."""
+        _check(lib().rbps_batch_step_io(self.h, force_ptr, pos_ptr, rot_ptr))
 
     def set_dump(self, on=True):
         _check(lib().rbps_batch_set_dump(self.h, 1 if on else 0))

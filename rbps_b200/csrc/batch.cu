@@ -161,6 +161,9 @@ struct rbps_batch
     uint64_t steps_done = 0;
     uint64_t launches_last = 0;
 
+    // host I/O staging (rbps_batch_step_io)
+    double *io_force = nullptr, *io_pos = nullptr, *io_rot = nullptr;
+
     // dumps
     bool dump = false;
     uint32_t *dump_pairs = nullptr;
@@ -1448,4 +1451,59 @@ extern "C" RBPS_API int rbps_debug_broadphase(rbps_batch *b, uint32_t world, uin
     if (world >= b->wdev.size() || b->wdev[world].n_bodies > kSmallWorldBodies)
         return fail(RBPS_ERR_INVALID, "rbps_debug_broadphase: small worlds only");
     return DISPATCH_PREC(b, debug_bp_typed, b, world, counts);
+}
+
+// One step with host I/O (see rbps_batch_step_io in rbps_gpu.h).
+template <class T, class P>
+static int step_io_typed(rbps_batch *b, const double *force_in, double *pos_out, double *rot_out)
+{
+    const uint32_t n = b->n_bodies_all;
+    int rc;
+    if (!b->io_force)
+    {
+        if ((rc = b->alloc((void **)&b->io_force, (size_t)n * 3 * 8)) || (rc = b->alloc((void **)&b->io_pos, (size_t)n * 3 * 8)) ||
+            (rc = b->alloc((void **)&b->io_rot, (size_t)n * 4 * 8)))
+            return rc;
+        CU(cudaDeviceSynchronize());
+    }
+    Engine<T, P> e = make_engine<T, P>(b);
+    const int grid = std::max(1, std::min<int>(b->sm_count * 8, (int)((n + 255) / 256)));
+    if (force_in)
+    {
+        CU(cudaMemcpyAsync(b->io_force, force_in, (size_t)n * 3 * 8, cudaMemcpyHostToDevice, b->stream));
+        CU(launch_io<T, P>(e, 0, b->io_force, nullptr, n, grid, b->stream));
+    }
+    if ((rc = step_typed<T, P>(b, 1)))
+        return rc;
+    b->steps_done += 1;
+    if (pos_out || rot_out)
+    {
+        CU(launch_io<T, P>(e, 1, b->io_pos, b->io_rot, n, grid, b->stream));
+        if (pos_out)
+            CU(cudaMemcpyAsync(pos_out, b->io_pos, (size_t)n * 3 * 8, cudaMemcpyDeviceToHost, b->stream));
+        if (rot_out)
+            CU(cudaMemcpyAsync(rot_out, b->io_rot, (size_t)n * 4 * 8, cudaMemcpyDeviceToHost, b->stream));
+    }
+    CU(cudaStreamSynchronize(b->stream));
+    return check_device_error(b);
+}
+
+extern "C" int rbps_batch_step_io(rbps_batch *b, const double *force_in, double *position_out, double *orientation_out)
+{
+    if (!b || !b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_step_io: commit first");
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, step_io_typed, b, force_in, position_out, orientation_out);
+}
+
+extern "C" int rbps_world_set_body_forces(rbps_batch *b, uint32_t world, uint32_t first, uint32_t n, const double *force)
+{
+    int rc = check_world(b, world, true);
+    if (rc)
+        return rc;
+    HostWorld &w = b->worlds[world];
+    if (!force || (uint64_t)first + n > w.bodies.size())
+        return fail(RBPS_ERR_INVALID, "rbps_world_set_body_forces: range out of bounds");
+    std::memcpy(w.force.data() + 3 * (size_t)first, force, (size_t)n * 3 * sizeof(double));
+    return RBPS_OK;
 }

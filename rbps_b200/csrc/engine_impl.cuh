@@ -731,10 +731,49 @@ namespace rbps_gpu
     template cudaError_t rbps_gpu::occupancy_small<T, P>(int, int *);                                              \
     template cudaError_t rbps_gpu::occupancy_big<T, P>(int, int *);                                               \
     template cudaError_t rbps_gpu::launch_debug_broadphase<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int,    \
-                                                                 uint32_t *, cudaStream_t);
+                                                                 uint32_t *, cudaStream_t);                         \
+    template cudaError_t rbps_gpu::launch_io<T, P>(const rbps_gpu::Engine<T, P> &, int, double *, double *,       \
+                                                   uint32_t, int, cudaStream_t);
 
 namespace rbps_gpu
 {
+    // Host I/O staging: per-body forces in (3 doubles), poses out
+    // (3 + 4 doubles), converted to / from the device precision.
+    template <class T, class P>
+    __global__ void k_forces_in(const Engine<T, P> E, const double *f, uint32_t n)
+    {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            E.B.force[i] = V4<T>{T(f[3 * i]), T(f[3 * i + 1]), T(f[3 * i + 2]), T(0)};
+    }
+
+    template <class T, class P>
+    __global__ void k_pose_out(const Engine<T, P> E, double *pos, double *rot, uint32_t n)
+    {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        {
+            const V4<P> x = E.B.pos[i];
+            const Q4<T> q = E.B.rot[i];
+            pos[3 * i] = double(x.x);
+            pos[3 * i + 1] = double(x.y);
+            pos[3 * i + 2] = double(x.z);
+            rot[4 * i] = double(q.w);
+            rot[4 * i + 1] = double(q.x);
+            rot[4 * i + 2] = double(q.y);
+            rot[4 * i + 3] = double(q.z);
+        }
+    }
+
+    template <class T, class P>
+    cudaError_t launch_io(const Engine<T, P> &e, int dir, double *a, double *b, uint32_t n, int grid,
+                          cudaStream_t stream)
+    {
+        if (dir == 0)
+            k_forces_in<T, P><<<grid, 256, 0, stream>>>(e, a, n);
+        else
+            k_pose_out<T, P><<<grid, 256, 0, stream>>>(e, a, b, n);
+        return cudaGetLastError();
+    }
+
     // Diagnostics: only the frame's broadphase + candidate build of one
     // world on one CTA (the first phase of world_step).
     template <class T, class P>

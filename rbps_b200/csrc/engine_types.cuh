@@ -139,6 +139,9 @@ namespace rbps_gpu
     template <class T, class P>
     cudaError_t occupancy_big(int block, int *blocks_per_sm);
     template <class T, class P>
+    cudaError_t launch_io(const Engine<T, P> &e, int dir, double *a, double *b, uint32_t n, int grid,
+                          cudaStream_t stream);
+    template <class T, class P>
     cudaError_t launch_debug_broadphase(const Engine<T, P> &e, uint32_t world, int block, uint32_t *out,
                                         cudaStream_t stream);
 } // namespace rbps_gpu

@@ -28,6 +28,16 @@ namespace rbps_gpu
     RBPS_HD float sqrt_t(float x) { return sqrtf(x); }
     RBPS_HD double inv_sqrt(double x) { return 1.0 / sqrt(x); }
     RBPS_HD float inv_sqrt(float x) { return 1.0f / sqrtf(x); }
+    // Squared-length threshold below which a cross product of two unit axes
+    // counts as degenerate (parallel edges).  The reference uses EPSILON^2 in
+    // double (BoxBox.hpp:45, CapsuleBox.hpp:112); in float the rounding noise
+    // of a cross product of nearly parallel unit vectors is ~1e-14, so the
+    // FP32 instantiation uses sin^2(1e-5 rad) instead of normalising noise
+    // into a separating axis.
+    template <class T> RBPS_HD T axis_eps_sq();
+    template <> RBPS_HD double axis_eps_sq<double>() { return kEpsilon * kEpsilon; }
+    template <> RBPS_HD float axis_eps_sq<float>() { return 1e-10f; }
+
     // std::min / std::max semantics (operand order matters for -0 and NaN).
     template <class T> RBPS_HD T rmin(T a, T b) { return (b < a) ? b : a; }
     template <class T> RBPS_HD T rmax(T a, T b) { return (a < b) ? b : a; }

@@ -309,7 +309,7 @@ namespace rbps_gpu
         {
             vec3<T> axis = cross(ax[i], l);
             const T len_sq = length_sq(axis);
-            if (len_sq < T(kEpsilon * kEpsilon))
+            if (len_sq < axis_eps_sq<T>())
                 continue;
             axis = axis / sqrt_t(len_sq);
             const T r_box = e[0] * rabs(dot(ax[0], axis)) + e[1] * rabs(dot(ax[1], axis)) + e[2] * rabs(dot(ax[2], axis));
@@ -405,7 +405,7 @@ namespace rbps_gpu
                                               T &best_depth, vec3<T> &best_normal, int feat, int &best_feat, T bias)
     {
         const T len_sq = length_sq(axis);
-        if (len_sq < T(kEpsilon * kEpsilon))
+        if (len_sq < axis_eps_sq<T>())
             return true;
         const vec3<T> na = axis / sqrt_t(len_sq);
         const T rA = obb_radius(ha, axA, na);

@@ -399,12 +399,25 @@ namespace rbps_gpu
         int type, act, limited, count;
     };
 
-    // set_value (Constraint.cpp:5-12)
+    // set_value (Constraint.cpp:5-12).  The reference keeps the direction
+    // whenever |value| > EPSILON, but normalize() returns the zero vector
+    // below |value|^2 < EPSILON, so an error in (1e-9, 3.2e-5) gets a zero
+    // direction and a rotational row then divides by w1 + w2 = 0.  Double
+    // precision reproduces that exactly; in float the alignment noise
+    // (~1e-7) lands in that band every substep, so the FP32 instantiation
+    // divides by the magnitude directly.
     template <class T>
     __device__ __forceinline__ void row_set_value(Row<T> &r, const vec3<T> &value)
     {
         const T mag = length(value);
-        const vec3<T> d = (mag > T(kEpsilon)) ? normalize(value) : vec3<T>(T(1.0), T(0.0), T(0.0));
+        vec3<T> d(T(1.0), T(0.0), T(0.0));
+        if (mag > T(kEpsilon))
+        {
+            if constexpr (sizeof(T) == 8)
+                d = normalize(value);
+            else
+                d = value * (T(1) / mag);
+        }
         r.dir = V4<T>{d.x, d.y, d.z, mag};
     }
 

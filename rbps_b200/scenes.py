@@ -163,7 +163,8 @@ def box_sphere_world(rng, n, friction=0.5, restitution=0.0,
                      ground=True, size=(0.2, 0.5)):
     """A ground plane plus n bodies, each a box (half-extents U[size]^3) or a
     sphere (radius U[size]) with probability 1/2, uniform random orientation,
-    position uniform in [lo, hi], at rest.  Returns lists (not yet arrays)."""
+    position uniform in [lo, hi], at rest.  Returns lists of descriptor
+    records (bodies, forces, colliders) that callers may extend."""
     bodies, forces, colliders = [], [], []
     if ground:
         _ground(bodies, colliders, forces, friction, restitution)
@@ -172,19 +173,37 @@ def box_sphere_world(rng, n, friction=0.5, restitution=0.0,
     sph_r = rng.uniform(size[0], size[1], n)
     quats = random_quats(rng, n)
     pos = rng.uniform(lo, hi, (n, 3))
-    for i in range(n):
-        bid = len(bodies)
-        if is_box[i]:
-            m, inertia = box_mass(box_h[i])
-            b, f = _dyn_body(pos[i], quats[i], m, inertia, g=g)
-            c = _collider(abi.SHAPE_BOX, box_h[i], bid, friction, restitution)
-        else:
-            m, inertia = sphere_mass(sph_r[i])
-            b, f = _dyn_body(pos[i], quats[i], m, inertia, g=g)
-            c = _collider(abi.SHAPE_SPHERE, [sph_r[i]], bid, friction, restitution)
-        bodies.append(b)
-        forces.append(f)
-        colliders.append(c)
+    # vectorised mass properties (same formulas as box_mass / sphere_mass)
+    hx, hy, hz = box_h[:, 0], box_h[:, 1], box_h[:, 2]
+    bvol = 8.0 * hx * hy * hz
+    x2, y2, z2 = 4.0 * hx * hx, 4.0 * hy * hy, 4.0 * hz * hz
+    binert = np.stack([(1.0 / 12.0) * bvol * (y2 + z2), (1.0 / 12.0) * bvol * (x2 + z2),
+                       (1.0 / 12.0) * bvol * (x2 + y2)], 1)
+    svol = (4.0 / 3.0) * PI * sph_r * sph_r * sph_r
+    sinert = (2.0 / 5.0) * svol * sph_r * sph_r
+    b = np.zeros(n, abi.BODY_DT)
+    b["type"] = abi.BODY_DYNAMIC
+    b["mass"] = np.where(is_box, bvol, svol) * DENSITY
+    inert = np.zeros((n, 6))
+    inert[:, :3] = np.where(is_box[:, None], binert, sinert[:, None]) * DENSITY
+    b["inertia"] = inert
+    b["position"] = pos
+    b["orientation"] = quats
+    c = np.zeros(n, abi.COLLIDER_DT)
+    c["shape"] = np.where(is_box, abi.SHAPE_BOX, abi.SHAPE_SPHERE)
+    params = np.zeros((n, 4))
+    params[:, :3] = np.where(is_box[:, None], box_h, np.stack([sph_r, np.zeros(n), np.zeros(n)], 1))
+    c["params"] = params
+    c["body_id"] = np.arange(len(bodies), len(bodies) + n)
+    c["local_rot"] = (1.0, 0.0, 0.0, 0.0)
+    c["restitution"] = restitution
+    c["static_friction"] = friction
+    c["dynamic_friction"] = friction
+    f = np.zeros((n, 3))
+    f[:, 1] = -g * b["mass"]
+    bodies.extend(list(b))
+    forces.extend(list(map(tuple, f)))
+    colliders.extend(list(c))
     return bodies, forces, colliders
 
 
