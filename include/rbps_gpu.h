@@ -303,6 +303,27 @@ RBPS_API int rbps_bp_get_fat_aabb(rbps_bp *bp, uint32_t handle, double aabb[6]);
  * cooperative grid (cheaper for small object counts). */
 RBPS_API int rbps_bp_configure(rbps_bp *bp, int32_t single_cta, int32_t block_threads);
 
+/* ------------------------------------------------- allocation-free query
+ * No counterpart in the reference: it serves callers that cannot allocate
+ * device memory once running (real-time loops, where cudaMalloc can block and
+ * synchronise the device; hosts that own a fixed device-memory budget).  The
+ * SAP sort + sweep of n_objects fat AABBs as a freshly filled broadphase holds
+ * them (endpoints in object order), with no allocation: working memory is a
+ * file-scope device array of about 2.3 MB per GPU, held until exit.
+ *   fat_aabbs : device, 6 doubles per object {min.xyz, max.xyz}
+ *   user_ids  : device, 1 per object
+ *   pairs     : device, 2 * pair_cap; (id_a, id_b), id_a < id_b, in the
+ *               reference emission order
+ *   n_pairs   : device, receives the pair count (may exceed pair_cap), or
+ *               0xFFFFFFFF when more than 65,536 pairs were found
+ * At most 8,192 objects (larger counts return RBPS_ERR_INVALID).  Runs
+ * asynchronously on `stream`.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race, so order them
+ * on one stream. */
+RBPS_API int rbps_sap_pairs_static(const double *fat_aabbs, const uint32_t *user_ids, uint32_t n_objects,
+                                   uint32_t *pairs, uint32_t pair_cap, uint32_t *n_pairs, void *stream);
+
 /* ------------------------------------------------------------ self tests
  * Self-checking runs of the device primitives every step phase is built on:
  * a stable radix sort of keys (values = original positions) by their low

@@ -103,6 +103,8 @@ def lib():
             "rbps_bp_get_pairs": (i, [_P, _U, C.c_uint32, _U]),
             "rbps_bp_get_fat_aabb": (i, [_P, C.c_uint32, _D]),
             "rbps_bp_configure": (i, [_P, C.c_int32, C.c_int32]),
+            "rbps_sap_pairs_static": (i, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                          C.c_void_p]),
             "rbps_selftest_sort": (i, [_U, C.c_uint32, C.c_int32, C.c_int32, C.c_int32, _U, _U]),
             "rbps_selftest_scan": (i, [_U, C.c_uint32, C.c_int32, C.c_int32, _U, _U]),
             "rbps_last_error": (i, [C.c_char_p, C.c_size_t]),

@@ -32,6 +32,7 @@ UNITS = {
     "batch.cu": [],
     "bp_api.cu": [],
     "selftest.cu": [],
+    "sap_static.cu": [],
     "quickhull.cpp": [],
 }
 
