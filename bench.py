@@ -236,6 +236,7 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
+    batch.synchronize()  # raises if the device reported an error during the timed steps
     barrier()
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     st = batch.stats()

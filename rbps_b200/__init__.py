@@ -23,7 +23,7 @@ from . import abi
 __all__ = ["lib", "Batch", "World", "BroadPhase", "RbpsError", "abi", "quickhull"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "librbps_b200.so")
+LIB_PATH = os.environ.get("RBPS_B200_LIB") or os.path.join(_HERE, "librbps_b200.so")
 _lib = None
 
 _P = C.c_void_p

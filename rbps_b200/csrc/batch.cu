@@ -1073,13 +1073,19 @@ extern "C" int rbps_batch_step(rbps_batch *b, int32_t n_steps)
 
 static int check_device_error(rbps_batch *b)
 {
-    int err = 0;
-    CU(cudaMemcpy(&err, b->error_d, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err)
+    int err[4] = {0, 0, 0, 0};
+    CU(cudaMemcpy(err, b->error_d, sizeof(err), cudaMemcpyDeviceToHost));
+    if (err[0])
     {
-        CU(cudaMemset(b->error_d, 0, sizeof(int)));
-        return fail(err, "device reported error %d (%s)", err,
-                    err == RBPS_ERR_CAPACITY ? "pair capacity exceeded: raise max_pairs_per_world" : "step failure");
+        CU(cudaMemset(b->error_d, 0, sizeof(err)));
+        CU(cudaDeviceSynchronize());
+        static const char *sites[] = {"", "endpoint id out of range", "corrupt SAP pair record",
+                                      "narrowphase candidate out of range", "endpoint keys not ordered after sort",
+                                      "pair keys not ordered after sort"};
+        const int site = (err[1] > 0 && err[1] < 6) ? err[1] : 0;
+        return fail(err[0], "device reported error %d (%s%s%s, value %d)", err[0],
+                    err[0] == RBPS_ERR_CAPACITY ? "pair capacity exceeded: raise max_pairs_per_world" : "step failure",
+                    site ? ": " : "", sites[site], err[2]);
     }
     return RBPS_OK;
 }

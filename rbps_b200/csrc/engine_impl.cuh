@@ -40,6 +40,17 @@ namespace rbps_gpu
         atomicCAS(err, 0, code);
     }
 
+    // First failing consistency check: err[0] = code, err[1] = site,
+    // err[2] = offending value (the host reports them in the error message).
+    __device__ __forceinline__ void set_error_at(int *err, int code, int site, uint32_t value)
+    {
+        if (atomicCAS(err, 0, code) == 0)
+        {
+            err[1] = site;
+            err[2] = (int)value;
+        }
+    }
+
     __device__ __forceinline__ uint32_t hash32(uint32_t x)
     {
         x ^= x >> 16;
@@ -135,7 +146,7 @@ namespace rbps_gpu
     // id_limit bounds the endpoint ids (2 * object slots; slots of removed
     // objects leave gaps in the standalone broadphase).
     template <class Team, class SC>
-    __device__ uint32_t sap_sort_sweep(const Team &tm, const FatBox *fat, uint32_t *ep_key, uint32_t *ep_id,
+    __device__ __noinline__ uint32_t sap_sort_sweep(const Team &tm, const FatBox *fat, uint32_t *ep_key, uint32_t *ep_id,
                                        uint32_t *ep_pos, uint32_t nbp, uint32_t id_limit, uint32_t pair_cap,
                                        int *error, const SC &S, BlockShared &sh)
     {
@@ -149,7 +160,9 @@ namespace rbps_gpu
             if (id < id_limit)
                 ep_pos[id] = i;
             else
-                set_error(error, kErrInternal);
+                set_error_at(error, kErrInternal, 1, id);
+            if (i + 1 < nep && ep_key[i] > ep_key[i + 1])
+                set_error_at(error, kErrInternal, 4, i); // the endpoint sort must leave the keys ordered
         }
         tm.sync();
         // count the pairs each opening endpoint emits
@@ -206,6 +219,10 @@ namespace rbps_gpu
         // reference emission order: stable sort by the later opening position
         const int bits = nep > 1 ? 32 - __clz(nep - 1) : 1;
         team_radix_sort(tm, S.pk, S.pv, S.pk2, S.pv2, total, bits, S.counts, S.tile_sums, sh);
+        for (uint32_t k = tm.rank(); k + 1 < total; k += tm.size())
+            if (S.pk[k] > S.pk[k + 1])
+                set_error_at(error, kErrInternal, 5, k); // pair sort must leave the keys ordered
+        tm.sync(); // the caller rewrites S.pk next
         return total;
     }
 
@@ -268,7 +285,7 @@ namespace rbps_gpu
             if (oa >= W.n_bp || ob >= W.n_bp)
             {
                 // corrupt pair record: report it and drop the pair
-                set_error(E.error, kErrInternal);
+                set_error_at(E.error, kErrInternal, 2, r);
                 S.pk[k] = 0;
                 S.pk2[k] = 0;
                 S.cflag[k] = 0;
@@ -297,7 +314,7 @@ namespace rbps_gpu
             const uint32_t lo = S.pk[k], hi = S.pk2[k];
             const uint32_t ga = W.coll_off + lo, gb = W.coll_off + hi;
             const bool keep = lo != hi && !(E.c_static[ga] && E.c_static[gb]) && (E.c_body[ga] != E.c_body[gb]);
-            if (keep)
+            if (keep && S.cflag[k] < n_pairs)
                 S.cand[S.cflag[k]] = Cand{lo, hi, E.c_body[ga], E.c_body[gb]};
         }
         for (uint32_t q = tm.rank(); q < W.n_pc; q += tm.size())
@@ -422,7 +439,7 @@ namespace rbps_gpu
     {
         if (cd.ca >= W.n_coll || cd.cb >= W.n_coll || cd.ba >= W.n_bodies || cd.bb >= W.n_bodies)
         {
-            set_error(E.error, kErrInternal);
+            set_error_at(E.error, kErrInternal, 3, cd.ca);
             out.n = 0;
             return;
         }
@@ -462,6 +479,8 @@ namespace rbps_gpu
         }
     }
 
+    // All contact rows of one candidate, in list order, with both bodies in
+    // registers (load once, relax, store once).
     template <class T, class P>
     __device__ __forceinline__ void solve_cand_position(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
                                                         CandContacts<T, P> &cc)
@@ -472,8 +491,13 @@ namespace rbps_gpu
         const vec3<T> nrm = v3(cc.normal);
         const T sf = cc.mat.y;
         const uint32_t ba = W.body_off + cd.ba, bb = W.body_off + cd.bb;
+        BodyR<T, P> A, Bb;
+        load_body(E.B, ba, A, true);
+        load_body(E.B, bb, Bb, true);
         for (int k = 0; k < n; ++k)
-            contact_position(E.B, ba, bb, nrm, sf, cc.pt[k], E.inv_h);
+            contact_position(A, Bb, nrm, sf, cc.pt[k], E.inv_h);
+        store_pose(E.B, ba, A);
+        store_pose(E.B, bb, Bb);
     }
 
     template <class T, class P>
@@ -485,8 +509,13 @@ namespace rbps_gpu
             return;
         const vec3<T> nrm = v3(cc.normal);
         const uint32_t ba = W.body_off + cd.ba, bb = W.body_off + cd.bb;
+        BodyR<T, P> A, Bb;
+        load_body(E.B, ba, A, false);
+        load_body(E.B, bb, Bb, false);
         for (int k = 0; k < n; ++k)
-            contact_velocity(E.B, ba, bb, nrm, cc.mat.x, cc.mat.z, cc.pt[k], E.h);
+            contact_velocity(A, Bb, nrm, cc.mat.x, cc.mat.z, cc.pt[k], E.h);
+        store_vel(E.B, ba, A);
+        store_vel(E.B, bb, Bb);
     }
 
     template <class T, class P>
@@ -536,8 +565,11 @@ namespace rbps_gpu
                         joint_errors(B, jt, joint_rows(E, jt), E.h);
                         E.joints[W.joint_off + j].target_pos = jt.target_pos;
                     }
-                    for (uint32_t r = 0; r < W.n_rows; ++r)
-                        solve_row(B, E.rows[W.row_off + r], E.inv_h);
+                    for (uint32_t j = 0; j < W.n_joints; ++j)
+                    {
+                        const Joint<T> &jt = E.joints[W.joint_off + j];
+                        solve_joint_rows(B, jt, joint_rows(E, jt), E.inv_h);
+                    }
                 }
                 tm.sync();
             }
@@ -572,9 +604,7 @@ namespace rbps_gpu
                     for (uint32_t q = jco[jc] + tm.rank(); q < jco[jc + 1]; q += tm.size())
                     {
                         const Joint<T> &jt = E.joints[W.joint_off + E.jorder[q]];
-                        Row<T> *rows = joint_rows(E, jt);
-                        for (int r = 0; r < jt.count; ++r)
-                            solve_row(B, rows[r], E.inv_h);
+                        solve_joint_rows(B, jt, joint_rows(E, jt), E.inv_h);
                     }
                     tm.sync();
                 }

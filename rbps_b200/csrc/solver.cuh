@@ -117,85 +117,121 @@ namespace rbps_gpu
         B.ang[i] = v4(w);
     }
 
-    // apply_positional_constraint_impulse (Body.cpp:59-68); Iw = world
-    // inverse inertia refreshed by the caller's inverse-mass query.
+    // ------------------------------------------------------- register-resident bodies
+    // The two bodies of a pair are loaded once per candidate (all its contact
+    // rows) or per joint (all its rows), relaxed in registers and stored
+    // once: every row reads the state the previous row wrote, exactly as the
+    // reference's in-place updates do, without a memory round trip on the
+    // serial critical path.
     template <class T, class P>
-    __device__ __forceinline__ void apply_pos_impulse(const Bodies<T, P> &B, uint32_t i, const smat3<T> &Iw,
-                                                      const vec3<T> &impulse, const vec3<T> &r)
+    struct BodyR
     {
-        if (B.is_static(i))
-            return;
-        vec3<T> x = B.x(i);
-        x += impulse * B.inv_mass(i);
-        B.set_x(i, x);
-        const vec3<T> rv = Iw * cross(r, impulse) * T(0.5);
-        const quat<T> rq(T(0.0), rv.x, rv.y, rv.z);
-        const quat<T> q = B.q(i);
-        B.set_q(i, normalize(q + rq * q));
+        vec3<T> x, v, w, xp;
+        quat<T> q, qp;
+        smat3<T> Iinv; // body-frame inverse inertia
+        T inv_mass;
+        bool stat;
+    };
+
+    template <class T, class P>
+    __device__ __forceinline__ void load_body(const Bodies<T, P> &B, uint32_t i, BodyR<T, P> &b, bool prev)
+    {
+        b.stat = B.is_static(i);
+        b.x = B.x(i);
+        b.q = B.q(i);
+        const V4<T> l = B.lin[i];
+        b.v = v3(l);
+        b.inv_mass = l.w;
+        b.w = v3(B.ang[i]);
+        b.Iinv = s3(B.inv_inertia[i]);
+        if (prev)
+        {
+            b.xp = vec3<T>(v3(B.prev_pos[i]));
+            b.qp = q4(B.prev_rot[i]);
+        }
     }
 
-    // apply_rotational_constraint_impulse (Body.cpp:70-77)
     template <class T, class P>
-    __device__ __forceinline__ void apply_rot_impulse(const Bodies<T, P> &B, uint32_t i, const smat3<T> &Iw,
-                                                      const vec3<T> &impulse)
+    __device__ __forceinline__ void store_pose(const Bodies<T, P> &B, uint32_t i, const BodyR<T, P> &b)
     {
-        if (B.is_static(i))
+        if (b.stat)
             return;
-        const vec3<T> rv = Iw * impulse * T(0.5);
-        const quat<T> rq(T(0.0), rv.x, rv.y, rv.z);
-        const quat<T> q = B.q(i);
-        B.set_q(i, normalize(q + rq * q));
+        B.set_x(i, b.x);
+        B.set_q(i, b.q);
     }
 
-    // apply_positional_velocity_constraint_impulse (Body.cpp:79-85)
     template <class T, class P>
-    __device__ __forceinline__ void apply_pos_vel_impulse(const Bodies<T, P> &B, uint32_t i, const smat3<T> &Iw,
-                                                          const vec3<T> &impulse, const vec3<T> &r)
+    __device__ __forceinline__ void store_vel(const Bodies<T, P> &B, uint32_t i, const BodyR<T, P> &b)
     {
-        if (B.is_static(i))
+        if (b.stat)
             return;
-        V4<T> l = B.lin[i];
-        vec3<T> v = v3(l);
-        v += impulse * l.w;
-        B.lin[i] = v4(v, l.w);
-        vec3<T> w = v3(B.ang[i]);
-        w += Iw * cross(r, impulse);
-        B.ang[i] = v4(w);
+        B.lin[i] = v4(b.v, b.inv_mass);
+        B.ang[i] = v4(b.w);
     }
 
-    // apply_rotational_velocity_constraint_impulse (Body.cpp:87-92)
+    // get_positional_generalized_inverse_mass (Body.cpp:94-101); Iw receives
+    // the refreshed world inverse inertia for the impulse appliers.
     template <class T, class P>
-    __device__ __forceinline__ void apply_rot_vel_impulse(const Bodies<T, P> &B, uint32_t i, const smat3<T> &Iw,
-                                                          const vec3<T> &impulse)
+    __device__ __forceinline__ T pos_w(const BodyR<T, P> &b, const vec3<T> &r, const vec3<T> &n, smat3<T> &Iw)
     {
-        if (B.is_static(i))
-            return;
-        vec3<T> w = v3(B.ang[i]);
-        w += Iw * impulse;
-        B.ang[i] = v4(w);
-    }
-
-    // get_positional_generalized_inverse_mass (Body.cpp:94-101); also
-    // returns the refreshed world inverse inertia for the impulse appliers.
-    template <class T, class P>
-    __device__ __forceinline__ T pos_inv_mass(const Bodies<T, P> &B, uint32_t i, const vec3<T> &r, const vec3<T> &n,
-                                              smat3<T> &Iw)
-    {
-        if (B.is_static(i))
+        if (b.stat)
             return T(0.0);
-        Iw = B.inv_inertia_world(i);
+        Iw = world_tensor(b.q, b.Iinv);
         const vec3<T> c = cross(r, n);
-        return B.inv_mass(i) + dot(c, Iw * c);
+        return b.inv_mass + dot(c, Iw * c);
     }
 
     // get_rotational_generalized_inverse_mass (Body.cpp:103-109)
     template <class T, class P>
-    __device__ __forceinline__ T rot_inv_mass(const Bodies<T, P> &B, uint32_t i, const vec3<T> &n, smat3<T> &Iw)
+    __device__ __forceinline__ T rot_w(const BodyR<T, P> &b, const vec3<T> &n, smat3<T> &Iw)
     {
-        if (B.is_static(i))
+        if (b.stat)
             return T(0.0);
-        Iw = B.inv_inertia_world(i);
+        Iw = world_tensor(b.q, b.Iinv);
         return dot(n, Iw * n);
+    }
+
+    // apply_positional_constraint_impulse (Body.cpp:59-68)
+    template <class T, class P>
+    __device__ __forceinline__ void pos_impulse(BodyR<T, P> &b, const smat3<T> &Iw, const vec3<T> &J, const vec3<T> &r)
+    {
+        if (b.stat)
+            return;
+        b.x += J * b.inv_mass;
+        const vec3<T> rv = Iw * cross(r, J) * T(0.5);
+        const quat<T> rq(T(0.0), rv.x, rv.y, rv.z);
+        b.q = normalize(b.q + rq * b.q);
+    }
+
+    // apply_rotational_constraint_impulse (Body.cpp:70-77)
+    template <class T, class P>
+    __device__ __forceinline__ void rot_impulse(BodyR<T, P> &b, const smat3<T> &Iw, const vec3<T> &J)
+    {
+        if (b.stat)
+            return;
+        const vec3<T> rv = Iw * J * T(0.5);
+        const quat<T> rq(T(0.0), rv.x, rv.y, rv.z);
+        b.q = normalize(b.q + rq * b.q);
+    }
+
+    // apply_positional_velocity_constraint_impulse (Body.cpp:79-85)
+    template <class T, class P>
+    __device__ __forceinline__ void pos_vel_impulse(BodyR<T, P> &b, const smat3<T> &Iw, const vec3<T> &J,
+                                                    const vec3<T> &r)
+    {
+        if (b.stat)
+            return;
+        b.v += J * b.inv_mass;
+        b.w += Iw * cross(r, J);
+    }
+
+    // apply_rotational_velocity_constraint_impulse (Body.cpp:87-92)
+    template <class T, class P>
+    __device__ __forceinline__ void rot_vel_impulse(BodyR<T, P> &b, const smat3<T> &Iw, const vec3<T> &J)
+    {
+        if (b.stat)
+            return;
+        b.w += Iw * J;
     }
 
     // ------------------------------------------------------- contacts
@@ -226,13 +262,12 @@ namespace rbps_gpu
     // apply_constraint_position_level + solve_normal_constraint +
     // solve_tangent_constraint (Contact.cpp:35-195) for one contact row.
     template <class T, class P>
-    __device__ void contact_position(const Bodies<T, P> &B, uint32_t ba, uint32_t bb, const vec3<T> &n,
-                                     T static_friction, ContactPt<T, P> &c, T inv_h)
+    __device__ __noinline__ void contact_position(BodyR<T, P> &A, BodyR<T, P> &Bb, const vec3<T> &n, T static_friction,
+                                     ContactPt<T, P> &c, T inv_h)
     {
         const vec3<T> ra_l = v3(c.ra), rb_l = v3(c.rb);
-        const vec3<T> xa = B.x(ba), xb = B.x(bb);
-        const vec3<T> p_a = xa + rotate(B.q(ba), ra_l);
-        const vec3<T> p_b = xb + rotate(B.q(bb), rb_l);
+        const vec3<T> p_a = A.x + rotate(A.q, ra_l);
+        const vec3<T> p_b = Bb.x + rotate(Bb.q, rb_l);
         c.pa = V4<P>{P(p_a.x), P(p_a.y), P(p_a.z), P(0)};
         c.pb = V4<P>{P(p_b.x), P(p_b.y), P(p_b.z), P(0)};
         const T d = dot(p_a - p_b, n);
@@ -242,18 +277,16 @@ namespace rbps_gpu
             return;
         }
         c.coll = 1;
-        const vec3<T> r_a = p_a - xa;
-        const vec3<T> r_b = p_b - xb;
+        const vec3<T> r_a = p_a - A.x;
+        const vec3<T> r_b = p_b - Bb.x;
         {
-            const vec3<T> v_rel = (v3(B.lin[ba]) + cross(v3(B.ang[ba]), r_a)) -
-                                  (v3(B.lin[bb]) + cross(v3(B.ang[bb]), r_b));
+            const vec3<T> v_rel = (A.v + cross(A.w, r_a)) - (Bb.v + cross(Bb.w, r_b));
             c.vrel = dot(v_rel, n);
         }
-        // normal
         {
             smat3<T> Ia, Ib;
-            const T w_a = pos_inv_mass(B, ba, r_a, n, Ia);
-            const T w_b = pos_inv_mass(B, bb, r_b, n, Ib);
+            const T w_a = pos_w(A, r_a, n, Ia);
+            const T w_b = pos_w(Bb, r_b, n, Ib);
             const T denom = w_a + w_b;
             if (!(denom < T(kEpsilon)))
             {
@@ -262,21 +295,19 @@ namespace rbps_gpu
                 if (c.lam_n > T(0.0))
                     c.lam_n = T(0.0);
                 const vec3<T> imp = dl * n;
-                apply_pos_impulse(B, ba, Ia, imp, r_a);
-                apply_pos_impulse(B, bb, Ib, -imp, r_b);
+                pos_impulse(A, Ia, imp, r_a);
+                pos_impulse(Bb, Ib, -imp, r_b);
             }
         }
-        // tangent (friction)
         {
-            const quat<T> qa = B.q(ba), qb = B.q(bb);
-            const vec3<T> ra_wc = rotate(qa, ra_l);
-            const vec3<T> rb_wc = rotate(qb, rb_l);
-            const vec3<T> pa_cur = B.x(ba) + ra_wc;
-            const vec3<T> pb_cur = B.x(bb) + rb_wc;
+            const vec3<T> ra_wc = rotate(A.q, ra_l);
+            const vec3<T> rb_wc = rotate(Bb.q, rb_l);
+            const vec3<T> pa_cur = A.x + ra_wc;
+            const vec3<T> pb_cur = Bb.x + rb_wc;
             c.pa = V4<P>{P(pa_cur.x), P(pa_cur.y), P(pa_cur.z), P(0)};
             c.pb = V4<P>{P(pb_cur.x), P(pb_cur.y), P(pb_cur.z), P(0)};
-            const vec3<T> prev_pa = vec3<T>(v3(B.prev_pos[ba])) + rotate(q4(B.prev_rot[ba]), ra_l);
-            const vec3<T> prev_pb = vec3<T>(v3(B.prev_pos[bb])) + rotate(q4(B.prev_rot[bb]), rb_l);
+            const vec3<T> prev_pa = A.xp + rotate(A.qp, ra_l);
+            const vec3<T> prev_pb = Bb.xp + rotate(Bb.qp, rb_l);
             const vec3<T> dp = (pa_cur - prev_pa) - (pb_cur - prev_pb);
             const vec3<T> dpt = dp - dot(dp, n) * n;
             const T slip = length(dpt);
@@ -284,8 +315,8 @@ namespace rbps_gpu
                 return;
             const vec3<T> t = normalize(dpt);
             smat3<T> Ia, Ib;
-            const T w_a = pos_inv_mass(B, ba, ra_wc, t, Ia);
-            const T w_b = pos_inv_mass(B, bb, rb_wc, t, Ib);
+            const T w_a = pos_w(A, ra_wc, t, Ia);
+            const T w_b = pos_w(Bb, rb_wc, t, Ib);
             const T denom = w_a + w_b;
             if (denom < T(kEpsilon))
                 return;
@@ -299,22 +330,21 @@ namespace rbps_gpu
             if (rabs(actual) < T(kEpsilon))
                 return;
             const vec3<T> imp = actual * t;
-            apply_pos_impulse(B, ba, Ia, imp, ra_wc);
-            apply_pos_impulse(B, bb, Ib, -imp, rb_wc);
+            pos_impulse(A, Ia, imp, ra_wc);
+            pos_impulse(Bb, Ib, -imp, rb_wc);
         }
     }
 
     // apply_constraint_velocity_level (Contact.cpp:206-289) for one row.
     template <class T, class P>
-    __device__ void contact_velocity(const Bodies<T, P> &B, uint32_t ba, uint32_t bb, const vec3<T> &n,
-                                     T restitution, T dynamic_friction, const ContactPt<T, P> &c, T h)
+    __device__ __noinline__ void contact_velocity(BodyR<T, P> &A, BodyR<T, P> &Bb, const vec3<T> &n, T restitution,
+                                     T dynamic_friction, const ContactPt<T, P> &c, T h)
     {
         if (!c.coll)
             return;
-        const vec3<T> r_a = vec3<T>(v3(c.pa)) - B.x(ba);
-        const vec3<T> r_b = vec3<T>(v3(c.pb)) - B.x(bb);
-        const vec3<T> v_rel = (v3(B.lin[ba]) + cross(v3(B.ang[ba]), r_a)) -
-                              (v3(B.lin[bb]) + cross(v3(B.ang[bb]), r_b));
+        const vec3<T> r_a = vec3<T>(v3(c.pa)) - A.x;
+        const vec3<T> r_b = vec3<T>(v3(c.pb)) - Bb.x;
+        const vec3<T> v_rel = (A.v + cross(A.w, r_a)) - (Bb.v + cross(Bb.w, r_b));
         const T v_n = dot(v_rel, n);
         const vec3<T> v_t = v_rel - n * v_n;
         const T v_t_mag = length(v_t);
@@ -330,26 +360,26 @@ namespace rbps_gpu
             dv_t = -rmin(limit, v_t_mag);
         }
         smat3<T> Ia, Ib;
-        const T w_a_n = pos_inv_mass(B, ba, r_a, n, Ia);
-        const T w_b_n = pos_inv_mass(B, bb, r_b, n, Ib);
+        const T w_a_n = pos_w(A, r_a, n, Ia);
+        const T w_b_n = pos_w(Bb, r_b, n, Ib);
         const T denom_n = w_a_n + w_b_n;
         if (denom_n > T(kEpsilon) && rabs(dv_n) > T(kEpsilon))
         {
             const vec3<T> imp = (dv_n / denom_n) * n;
-            apply_pos_vel_impulse(B, ba, Ia, imp, r_a);
-            apply_pos_vel_impulse(B, bb, Ib, -imp, r_b);
+            pos_vel_impulse(A, Ia, imp, r_a);
+            pos_vel_impulse(Bb, Ib, -imp, r_b);
         }
         if (v_t_mag > T(kEpsilon) && rabs(dv_t) > T(kEpsilon))
         {
             const vec3<T> t = v_t / v_t_mag;
-            const T w_a_t = pos_inv_mass(B, ba, r_a, t, Ia);
-            const T w_b_t = pos_inv_mass(B, bb, r_b, t, Ib);
+            const T w_a_t = pos_w(A, r_a, t, Ia);
+            const T w_b_t = pos_w(Bb, r_b, t, Ib);
             const T denom_t = w_a_t + w_b_t;
             if (denom_t > T(kEpsilon))
             {
                 const vec3<T> imp = (dv_t / denom_t) * t;
-                apply_pos_vel_impulse(B, ba, Ia, imp, r_a);
-                apply_pos_vel_impulse(B, bb, Ib, -imp, r_b);
+                pos_vel_impulse(A, Ia, imp, r_a);
+                pos_vel_impulse(Bb, Ib, -imp, r_b);
             }
         }
     }
@@ -431,31 +461,31 @@ namespace rbps_gpu
 
     // compute_{rotational,positional}_constraint_impulse (Constraint.cpp:20-46)
     template <class T, class P>
-    __device__ void solve_row(const Bodies<T, P> &B, Row<T> &r, T inv_h)
+    __device__ void solve_row(BodyR<T, P> &b1, BodyR<T, P> &b2, Row<T> &r, T inv_h)
     {
         const vec3<T> dir = v3(r.dir);
         smat3<T> I1, I2;
         if (r.type == kRowRotational)
         {
-            const T w1 = rot_inv_mass(B, r.b1, dir, I1);
-            const T w2 = rot_inv_mass(B, r.b2, dir, I2);
+            const T w1 = rot_w(b1, dir, I1);
+            const T w2 = rot_w(b2, dir, I2);
             const T dl = row_delta_lambda(r, w1, w2, inv_h);
             r.r2.w += dl;
             const vec3<T> imp = dl * dir;
-            apply_rot_impulse(B, r.b1, I1, imp);
-            apply_rot_impulse(B, r.b2, I2, -imp);
+            rot_impulse(b1, I1, imp);
+            rot_impulse(b2, I2, -imp);
         }
         else
         {
-            const vec3<T> r1 = rotate(B.q(r.b1), v3(r.r1));
-            const vec3<T> r2 = rotate(B.q(r.b2), v3(r.r2));
-            const T w1 = pos_inv_mass(B, r.b1, r1, dir, I1);
-            const T w2 = pos_inv_mass(B, r.b2, r2, dir, I2);
+            const vec3<T> r1 = rotate(b1.q, v3(r.r1));
+            const vec3<T> r2 = rotate(b2.q, v3(r.r2));
+            const T w1 = pos_w(b1, r1, dir, I1);
+            const T w2 = pos_w(b2, r2, dir, I2);
             const T dl = row_delta_lambda(r, w1, w2, inv_h);
             r.r2.w += dl;
             const vec3<T> imp = dl * dir;
-            apply_pos_impulse(B, r.b1, I1, imp, r1);
-            apply_pos_impulse(B, r.b2, I2, -imp, r2);
+            pos_impulse(b1, I1, imp, r1);
+            pos_impulse(b2, I2, -imp, r2);
         }
     }
 
@@ -477,15 +507,14 @@ namespace rbps_gpu
             row_set_value(rows[1], p1 - p2);
             const vec3<T> b1l = rotate(q1, v3(j.limit_axis));
             const vec3<T> b2l = rotate(q2, v3(j.limit_axis));
-            T phi = atan2(dot(cross(b1l, b2l), a1), dot(b1l, b2l));
             vec3<T> err_limit(T(0.0), T(0.0), T(0.0));
             if (j.limited)
             {
                 // compute_angle_limit_correction (Joint.cpp:73-90)
+                const T phi = atan2(dot(cross(b1l, b2l), a1), dot(b1l, b2l));
                 if (phi < j.lower || phi > j.upper)
                 {
                     const bool lo = phi < j.lower; // clamp(phi, lower, upper)
-                    phi = lo ? j.lower : j.upper;
                     const T s = lo ? j.sin_lo : j.sin_hi;
                     const T c = lo ? j.cos_lo : j.cos_hi;
                     const vec3<T> nn = normalize(a1);
@@ -548,38 +577,57 @@ namespace rbps_gpu
         }
     }
 
+    // All rows of one joint, in row order, its two bodies held in registers.
+    template <class T, class P>
+    __device__ __noinline__ void solve_joint_rows(const Bodies<T, P> &B, const Joint<T> &j, Row<T> *rows, T inv_h)
+    {
+        BodyR<T, P> b1, b2;
+        load_body(B, j.b1, b1, false);
+        load_body(B, j.b2, b2, false);
+        for (int r = 0; r < j.count; ++r)
+            solve_row(b1, b2, rows[r], inv_h);
+        store_pose(B, j.b1, b1);
+        store_pose(B, j.b2, b2);
+    }
+
     // apply_{prismatic,revolute}_joint_damping (Joint.cpp:184-220)
     template <class T, class P>
-    __device__ void joint_damping(const Bodies<T, P> &B, const Joint<T> &j, T h)
+    __device__ __noinline__ void joint_damping(const Bodies<T, P> &B, const Joint<T> &j, T h)
     {
-        const uint32_t b1 = j.b1, b2 = j.b2;
+        BodyR<T, P> b1, b2;
+        load_body(B, j.b1, b1, false);
+        load_body(B, j.b2, b2, false);
         if (j.type == kRevolute)
         {
-            const vec3<T> dw = (v3(B.ang[b2]) - v3(B.ang[b1])) * rmin(j.damping * h, T(1.0));
+            const vec3<T> dw = (b2.w - b1.w) * rmin(j.damping * h, T(1.0));
             if (length_sq(dw) < T(kEpsilon))
                 return;
             const vec3<T> n = normalize(dw);
             smat3<T> I1, I2;
-            const T w1 = rot_inv_mass(B, b1, n, I1);
-            const T w2 = rot_inv_mass(B, b2, n, I2);
+            const T w1 = rot_w(b1, n, I1);
+            const T w2 = rot_w(b2, n, I2);
             const vec3<T> imp = dw / (w1 + w2);
-            apply_rot_vel_impulse(B, b1, I1, imp);
-            apply_rot_vel_impulse(B, b2, I2, -imp);
+            rot_vel_impulse(b1, I1, imp);
+            rot_vel_impulse(b2, I2, -imp);
         }
         else if (j.type == kPrismatic)
         {
-            const vec3<T> dv = (v3(B.lin[b2]) - v3(B.lin[b1])) * rmin(j.damping * h, T(1.0));
+            const vec3<T> dv = (b2.v - b1.v) * rmin(j.damping * h, T(1.0));
             if (length_sq(dv) < T(kEpsilon))
                 return;
-            const vec3<T> r1 = rotate(B.q(b1), v3(j.r1));
-            const vec3<T> r2 = rotate(B.q(b2), v3(j.r2));
+            const vec3<T> r1 = rotate(b1.q, v3(j.r1));
+            const vec3<T> r2 = rotate(b2.q, v3(j.r2));
             const vec3<T> n = normalize(dv);
             smat3<T> I1, I2;
-            const T w1 = pos_inv_mass(B, b1, r1, n, I1);
-            const T w2 = pos_inv_mass(B, b2, r2, n, I2);
+            const T w1 = pos_w(b1, r1, n, I1);
+            const T w2 = pos_w(b2, r2, n, I2);
             const vec3<T> imp = dv / (w1 + w2);
-            apply_pos_vel_impulse(B, b1, I1, imp, r1);
-            apply_pos_vel_impulse(B, b2, I2, -imp, r2);
+            pos_vel_impulse(b1, I1, imp, r1);
+            pos_vel_impulse(b2, I2, -imp, r2);
         }
+        else
+            return;
+        store_vel(B, j.b1, b1);
+        store_vel(B, j.b2, b2);
     }
 } // namespace rbps_gpu

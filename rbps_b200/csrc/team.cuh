@@ -10,7 +10,8 @@
 // exclusive scan and a stable LSD radix sort of (u32 key, u32 value) over
 // global-memory arrays.  Tiles are blockDim.x items; every thread of a CTA
 // runs every tile iteration of its CTA, so block barriers inside tile loops
-// are uniform.
+// are uniform.  The primitives are compiled as separate (non-inlined)
+// functions so their code does not depend on the kernel that calls them.
 #pragma once
 #include <cooperative_groups.h>
 #include <cstdint>
@@ -94,7 +95,7 @@ namespace rbps_gpu
     // tile_sums needs ceil(n / blockDim.x) + 1 words of global scratch.
     // Returns the total to every thread.  Ends with a team barrier.
     template <class Team>
-    __device__ uint32_t team_excl_scan(const Team &tm, const uint32_t *in, uint32_t *out, uint32_t n,
+    __device__ __noinline__ uint32_t team_excl_scan(const Team &tm, const uint32_t *in, uint32_t *out, uint32_t n,
                                        uint32_t *tile_sums, BlockShared &sh)
     {
         const uint32_t B = blockDim.x;
@@ -142,7 +143,7 @@ namespace rbps_gpu
     // One stable counting pass on 8-bit digit `shift` of keys: (k0,v0) -> (k1,v1).
     // counts needs 256 * ntiles words, tile_sums ntiles*256/B + 2 words.
     template <class Team>
-    __device__ void radix_pass(const Team &tm, const uint32_t *k0, const uint32_t *v0, uint32_t *k1, uint32_t *v1,
+    __device__ __noinline__ void radix_pass(const Team &tm, const uint32_t *k0, const uint32_t *v0, uint32_t *k1, uint32_t *v1,
                                uint32_t n, int shift, uint32_t *counts, uint32_t *tile_sums, BlockShared &sh)
     {
         const uint32_t B = blockDim.x;
@@ -195,8 +196,11 @@ namespace rbps_gpu
             if (live)
             {
                 const uint32_t dst = counts[d * ntiles + t] + sh.wdig[warp_id() * 256 + d] + lane_rank;
-                k1[dst] = key;
-                v1[dst] = v0[i];
+                if (dst < n) // a corrupted count must never write outside the buffer
+                {
+                    k1[dst] = key;
+                    v1[dst] = v0[i];
+                }
             }
             __syncthreads();
         }
@@ -206,7 +210,7 @@ namespace rbps_gpu
     // Stable sort of (keys, vals)[0..n) by the low `bits` bits of the key.
     // The result is left in (keys, vals); (kt, vt) are ping-pong buffers.
     template <class Team>
-    __device__ void team_radix_sort(const Team &tm, uint32_t *keys, uint32_t *vals, uint32_t *kt, uint32_t *vt,
+    __device__ __noinline__ void team_radix_sort(const Team &tm, uint32_t *keys, uint32_t *vals, uint32_t *kt, uint32_t *vt,
                                     uint32_t n, int bits, uint32_t *counts, uint32_t *tile_sums, BlockShared &sh)
     {
         if (n <= 1)
