@@ -59,6 +59,25 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def reduce_over_ranks(x, op, ws):
+    """x (a float) reduced over the process group: op "max" or "sum"; the
+    identity at one rank.  NCCL reduces a CUDA tensor, gloo a CPU one."""
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def rank_seed(seed, rank):
+    """Each rank steps its own scene (weak scaling): same distribution,
+    independent draw."""
+    return seed + rank
+
+
 def dist_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -118,9 +137,12 @@ class ClockSampler:
 
 
 def cpu_reference_run(scene, warmup, steps, max_seconds, threads):
-    """The reference engine on the host cores: RefWorlds of the scene's worlds
-    (a prefix sample if needed to stay within max_seconds), `warmup` untimed
-    steps then `steps` timed; returns (body-substeps/s, info)."""
+    """The reference engine (oracle/_ref, built from the reference's own
+    sources) on the host cores, one World per thread at a time: a prefix of
+    the scene's worlds sized so that `steps` steps take about max_seconds,
+    `warmup` untimed steps, then timed chunks of steps until at least
+    `steps` steps and max_seconds / 2 of wall clock have passed.  Returns
+    (body-substeps/s, description of the sample)."""
     from oracle import ref
     worlds = scene.worlds
     # calibrate on a small prefix, then size the sample to the time budget
@@ -132,7 +154,7 @@ def cpu_reference_run(scene, warmup, steps, max_seconds, threads):
     total_bs = 0
     n = 0
     for w in worlds:
-        need = w.n_dynamic * scene.substeps * (steps + warmup)
+        need = w.n_dynamic * scene.substeps * steps
         if n >= 64 and total_bs + need > budget_bs:
             break
         total_bs += need
@@ -142,10 +164,15 @@ def cpu_reference_run(scene, warmup, steps, max_seconds, threads):
     refs = [ref.RefWorld(w, scene.timestep, scene.substeps) for w in sample]
     if warmup:
         ref.step_worlds(refs, warmup, threads)
-    secs = ref.step_worlds(refs, steps, threads)
+    secs, done = 0.0, 0
+    chunk = max(1, min(steps, 10))
+    while done < steps or (secs < 0.5 * max_seconds and done < 20 * steps):
+        secs += ref.step_worlds(refs, chunk, threads)
+        done += chunk
     n_dyn = sum(w.n_dynamic for w in sample)
-    value = n_dyn * scene.substeps * steps / secs
-    info = f"{n} of {len(worlds)} worlds ({n_dyn} dynamic bodies), {warmup} untimed + {steps} timed steps, {secs:.2f} s"
+    value = n_dyn * scene.substeps * done / secs
+    info = (f"{n} of {len(worlds)} worlds ({n_dyn} dynamic bodies), {warmup} untimed + {done} timed steps, "
+            f"{secs:.2f} s on {threads} threads")
     return value, info
 
 
@@ -173,7 +200,8 @@ def main():
         if rank != 0:
             return
         scene = scenes.config3(seed=args.seed, n_worlds=args.worlds)
-        value, info = cpu_reference_run(scene, args.warmup, args.steps, max_seconds=150.0, threads=threads)
+        budget = float(os.environ.get("RBPS_BENCH_REF_SECONDS", "150"))
+        value, info = cpu_reference_run(scene, args.warmup, args.steps, max_seconds=budget, threads=threads)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
@@ -195,7 +223,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import rbps_b200
 
-    scene = scenes.config3(seed=args.seed + rank, n_worlds=args.worlds)
+    scene = scenes.config3(seed=rank_seed(args.seed, rank), n_worlds=args.worlds)
     stream = torch.cuda.Stream()  # a real stream: the legacy NULL stream would not order our launches
     torch.cuda.set_stream(stream)
     batch = rbps_b200.Batch.from_scene(scene, abi.PRECISION_FP32, abi.SOLVE_COLORED, device=local,
@@ -207,13 +235,6 @@ def main():
     def barrier():
         if ws > 1:
             torch.distributed.barrier()
-
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
 
     # warm-up (untimed)
     batch.step(args.warmup)
@@ -238,9 +259,11 @@ def main():
     clk = clocks.stop()
     batch.synchronize()  # raises if the device reported an error during the timed steps
     barrier()
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms = reduce_over_ranks(ev0.elapsed_time(ev1), "max", ws)
     st = batch.stats()
-    value = n_dyn * scene.substeps * args.steps * ws / (ms / 1e3)
+    n_dyn_all = reduce_over_ranks(n_dyn, "sum", ws)  # scenes differ per rank
+    n_tot_all = reduce_over_ranks(n_tot, "sum", ws)
+    value = n_dyn_all * scene.substeps * args.steps / (ms / 1e3)
     ms_step = ms / args.steps
 
     # roofline of the step kernel (one launch per step)
@@ -269,8 +292,8 @@ def main():
         batch.step_io(f_host.data_ptr(), p_host.data_ptr(), q_host.data_ptr())
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = n_dyn * scene.substeps * args.e2e_steps * ws / (e2e_ms / 1e3)
+    e2e_ms = reduce_over_ranks(e0.elapsed_time(e1), "max", ws)
+    e2e_value = n_dyn_all * scene.substeps * args.e2e_steps / (e2e_ms / 1e3)
     finite = bool(np.isfinite(p_host.numpy()).all())
 
     cpu = None
@@ -295,8 +318,8 @@ def main():
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "algorithmic_bytes_per_launch": bmodel, "kernel": "k_step_small"},
                 "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_tot * 24,
-                        "d2h_bytes_per_step": n_tot * 56, "steps": args.e2e_steps},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n_tot_all) * 24,
+                        "d2h_bytes_per_step": int(n_tot_all) * 56, "steps": args.e2e_steps},
                 "clocks": clk,
                 "gpu_launches": int(st["kernel_launches"]),
                 "stats_last_step": {"pairs": st["pairs"], "candidates": st["candidates"],

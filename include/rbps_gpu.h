@@ -185,6 +185,21 @@ typedef struct rbps_stats {
     uint64_t kernel_launches;  /* kernels launched by the last rbps_batch_step  */
 } rbps_stats;
 
+/* Result of one shape-pair test (rbc::ContactManifold, Contact.hpp:37-51). */
+enum {
+    RBPS_COLLIDE_MISS = 0,        /* no overlap                                  */
+    RBPS_COLLIDE_HIT = 1,         /* overlap; n_points >= 1 points are valid     */
+    RBPS_COLLIDE_UNSUPPORTED = 2  /* pair needs GJK/EPA, not built on the device */
+};
+
+typedef struct rbps_manifold {
+    int32_t status;           /* RBPS_COLLIDE_*                                 */
+    int32_t n_points;         /* 0..4                                           */
+    double normal[3];         /* unit, from shape A toward shape B              */
+    double position[4][3];    /* world-space contact points                     */
+    double depth[4];          /* penetration depth of each point (> 0 overlap)  */
+} rbps_manifold;
+
 typedef struct rbps_batch rbps_batch;
 
 /* ---------------------------------------------------------------- batch */
@@ -281,6 +296,21 @@ RBPS_API int rbps_batch_get_stats(rbps_batch *batch, rbps_stats *stats);
  * may be NULL; *n_objects receives the object count. */
 RBPS_API int rbps_batch_get_sap_state(rbps_batch *batch, uint32_t world, double *fat, uint32_t *ep_ids,
                                       float *ep_values, uint32_t *n_objects);
+
+/* Narrowphase on the device for n independent shape pairs: the GPU
+ * counterpart of rbc::dispatch(a, tf_a, b, tf_b, manifold)
+ * (rbc/Dispatcher.hpp:208-213), in the batch's precision.  Shapes are
+ * collider descriptors (only shape, params and hull are read; hull ids name
+ * hulls created on this batch, which must be committed when any is used).
+ * tf_a / tf_b: 7 doubles per pair (position xyz, orientation wxyz).  Host
+ * buffers; synchronous. */
+RBPS_API int rbps_batch_collide(rbps_batch *batch, uint32_t n, const rbps_collider_desc *a, const double *tf_a,
+                                const rbps_collider_desc *b, const double *tf_b, rbps_manifold *out);
+/* Diagnostics: the broadphase + candidate build of one world (the first
+ * phase of a step) on its own, at the current poses; counts[0] = SAP pairs,
+ * counts[1] = narrowphase candidates.  It updates the SAP state as a step
+ * would (a repeat at unchanged poses changes nothing). */
+RBPS_API int rbps_debug_broadphase(rbps_batch *batch, uint32_t world, uint32_t *counts);
 
 /* ------------------------------------------------- standalone broadphase
  * GPU drop-in for the rbc SAP API (rbc/BroadPhase.hpp:151-260): objects are

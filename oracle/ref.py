@@ -42,6 +42,9 @@ def lib():
         L.ref_add_collider.argtypes = [_P, _P]
         L.ref_add_joint.restype = C.c_uint32
         L.ref_add_joint.argtypes = [_P, _P]
+        L.ref_collide.restype = C.c_int
+        L.ref_collide.argtypes = [_P, C.c_uint32, _P, _D, _P, _D, _P]
+        L.ref_default_descs.argtypes = [_P, _P, _P, _P, _P, _D]
         L.ref_step.argtypes = [_P, C.c_int]
         L.ref_body_count.restype = C.c_uint32
         L.ref_body_count.argtypes = [_P]
@@ -150,11 +153,39 @@ class RefWorld:
         L.ref_get_sap_state(self.h, _dp(fat), ids.ctypes.data_as(_U), vals.ctypes.data_as(C.POINTER(C.c_float)))
         return fat[:n], ids[:2 * n], vals[:2 * n]
 
+    def collide(self, a, tf_a, b, tf_b):
+        """rbc::dispatch on n shape pairs (collider descriptors; hull ids name
+        this world's hulls); tf_*: (n, 7) position + quaternion wxyz."""
+        a = np.ascontiguousarray(a, abi.COLLIDER_DT)
+        b = np.ascontiguousarray(b, abi.COLLIDER_DT)
+        ta = np.ascontiguousarray(tf_a, np.float64).reshape(-1, 7)
+        tb = np.ascontiguousarray(tf_b, np.float64).reshape(-1, 7)
+        n = len(a)
+        out = np.zeros(max(n, 1), abi.MANIFOLD_DT)
+        rc = lib().ref_collide(self.h, n, C.c_void_p(a.ctypes.data), _dp(ta), C.c_void_p(b.ctypes.data), _dp(tb),
+                               C.c_void_p(out.ctypes.data))
+        if rc != 0:
+            raise ValueError("ref_collide: unknown shape or hull")
+        return out[:n]
+
     def collision_groups(self):
         c = self.contacts()
         colors = np.zeros(max(len(c), 1), np.uint32)
         ng = lib().ref_collision_groups(self.h, colors.ctypes.data_as(_U), len(c))
         return colors[:len(c)], ng
+
+
+def default_descs():
+    """The reference's parameter defaults as descriptor records:
+    (body, collider, revolute, prismatic, fixed, world_cfg)."""
+    body = np.zeros(1, abi.BODY_DT)
+    coll = np.zeros(1, abi.COLLIDER_DT)
+    joints = np.zeros(3, abi.JOINT_DT)
+    cfg = np.zeros(4)
+    jp = joints.ctypes.data
+    lib().ref_default_descs(C.c_void_p(body.ctypes.data), C.c_void_p(coll.ctypes.data), C.c_void_p(jp),
+                            C.c_void_p(jp + joints.itemsize), C.c_void_p(jp + 2 * joints.itemsize), _dp(cfg))
+    return body[0], coll[0], joints[0], joints[1], joints[2], cfg
 
 
 def step_worlds(worlds, steps, threads):

@@ -12,6 +12,7 @@
 
 #include "rbps/API/World.hpp"
 #include "rbc/BroadPhase.hpp"
+#include "rbc/Dispatcher.hpp"
 #include "rbps_gpu.h"
 
 #include <chrono>
@@ -45,6 +46,23 @@ namespace
     {
         out.min = m3d::vec3(a[0], a[1], a[2]);
         out.max = m3d::vec3(a[3], a[4], a[5]);
+    }
+    // rbc::Shape of a collider descriptor (hull ids index the world's hulls).
+    bool make_shape(RefWorld *rw, const rbps_collider_desc *d, rbc::Shape &out)
+    {
+        switch (d->shape)
+        {
+        case RBPS_SHAPE_SPHERE: out = rbc::Sphere(d->params[0]); return true;
+        case RBPS_SHAPE_BOX: out = rbc::Box(v3(d->params)); return true;
+        case RBPS_SHAPE_CAPSULE: out = rbc::Capsule(d->params[0], d->params[1]); return true;
+        case RBPS_SHAPE_PLANE: out = rbc::Plane(v3(d->params), d->params[3]); return true;
+        case RBPS_SHAPE_CONVEX_HULL:
+            if (d->hull >= rw->hulls.size())
+                return false;
+            out = rbc::ConvexHull(rw->hulls[d->hull]->data);
+            return true;
+        default: return false;
+        }
     }
 } // namespace
 
@@ -106,15 +124,8 @@ extern "C"
     {
         auto *rw = static_cast<RefWorld *>(h);
         rbps::ColliderParams p;
-        switch (d->shape)
-        {
-        case RBPS_SHAPE_SPHERE: p.shape = rbc::Sphere(d->params[0]); break;
-        case RBPS_SHAPE_BOX: p.shape = rbc::Box(v3(d->params)); break;
-        case RBPS_SHAPE_CAPSULE: p.shape = rbc::Capsule(d->params[0], d->params[1]); break;
-        case RBPS_SHAPE_PLANE: p.shape = rbc::Plane(v3(d->params), d->params[3]); break;
-        case RBPS_SHAPE_CONVEX_HULL: p.shape = rbc::ConvexHull(rw->hulls.at(d->hull)->data); break;
-        default: return UINT32_MAX;
-        }
+        if (!make_shape(rw, d, p.shape))
+            return UINT32_MAX;
         p.body_id = d->body_id;
         p.is_static = d->is_static != 0;
         p.local_pos = v3(d->local_pos);
@@ -164,6 +175,107 @@ extern "C"
             rw->w.joints.target_speed[j] = d->target_speed;
         }
         return id;
+    }
+
+    // rbc::dispatch (Dispatcher.hpp:208-213) on n shape pairs.  tf_* hold 7
+    // doubles per pair (position xyz, orientation wxyz).  out receives one
+    // rbps_manifold per pair (hit flag, points, normal A->B, depths).
+    // Returns -1 when a descriptor names an unknown shape or hull.
+    int ref_collide(void *h, uint32_t n, const rbps_collider_desc *a, const double *tf_a,
+                    const rbps_collider_desc *b, const double *tf_b, rbps_manifold *out)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            rbc::Shape sa, sb;
+            if (!make_shape(rw, a + i, sa) || !make_shape(rw, b + i, sb))
+                return -1;
+            const m3d::tf ta(v3(tf_a + 7 * i), q4(tf_a + 7 * i + 3));
+            const m3d::tf tb(v3(tf_b + 7 * i), q4(tf_b + 7 * i + 3));
+            rbc::ContactManifold m;
+            const bool hit = rbc::dispatch(sa, ta, sb, tb, m);
+            rbps_manifold &o = out[i];
+            std::memset(&o, 0, sizeof(o));
+            o.status = hit ? RBPS_COLLIDE_HIT : RBPS_COLLIDE_MISS;
+            o.n_points = hit ? m.num_points : 0;
+            if (hit)
+            {
+                put3(o.normal, m.normal);
+                for (int k = 0; k < m.num_points && k < 4; ++k)
+                {
+                    put3(o.position[k], m.points[k].position);
+                    o.depth[k] = m.points[k].penetration_depth;
+                }
+            }
+        }
+        return 0;
+    }
+
+    // The reference's parameter defaults (BodyParams{}, ColliderParams{},
+    // Revolute/Prismatic/FixedJointParams{}, World{}, BroadPhaseConfig{})
+    // written into the C ABI descriptors; world_cfg = {timestep, substeps,
+    // fat_margin, reinsert_threshold}.
+    void ref_default_descs(rbps_body_desc *body, rbps_collider_desc *coll, rbps_joint_desc *revolute,
+                           rbps_joint_desc *prismatic, rbps_joint_desc *fixed, double *world_cfg)
+    {
+        const rbps::BodyParams bp{};
+        std::memset(body, 0, sizeof(*body));
+        body->type = bp.type == rbps::STATIC ? RBPS_BODY_STATIC : RBPS_BODY_DYNAMIC;
+        body->mass = bp.mass;
+        const m3d::smat3 &I = bp.inertia_tensor;
+        const double iv[6] = {I.xx, I.yy, I.zz, I.xy, I.xz, I.yz};
+        std::memcpy(body->inertia, iv, sizeof(iv));
+        put3(body->position, bp.position);
+        put4(body->orientation, bp.orientation);
+        put3(body->linear_velocity, bp.linear_velocity);
+        put3(body->angular_velocity, bp.angular_velocity);
+
+        const rbps::ColliderParams cp{};
+        std::memset(coll, 0, sizeof(*coll));
+        coll->shape = static_cast<int32_t>(cp.shape.v.index());
+        coll->params[0] = std::get<rbc::Sphere>(cp.shape.v).radius;
+        coll->body_id = cp.body_id;
+        coll->is_static = cp.is_static ? 1 : 0;
+        put3(coll->local_pos, cp.local_pos);
+        put4(coll->local_rot, cp.local_rot);
+        coll->restitution = cp.restitution;
+        coll->static_friction = cp.static_friction;
+        coll->dynamic_friction = cp.dynamic_friction;
+
+        const rbps::RevoluteJointParams rp{};
+        std::memset(revolute, 0, sizeof(*revolute));
+        revolute->type = RBPS_JOINT_REVOLUTE;
+        revolute->body_1 = (uint32_t)rp.body_1; revolute->body_2 = (uint32_t)rp.body_2;
+        put3(revolute->axis, rp.aligned_axis); put3(revolute->limit_axis, rp.limit_axis);
+        put3(revolute->r_1, rp.r_1); put3(revolute->r_2, rp.r_2);
+        revolute->actuation = static_cast<int32_t>(rp.actuation_type);
+        revolute->compliance = rp.compliance; revolute->damping = rp.damping;
+        revolute->limited = rp.limited ? 1 : 0;
+        revolute->lower_limit = rp.lower_limit; revolute->upper_limit = rp.upper_limit;
+
+        const rbps::PrismaticJointParams pp{};
+        std::memset(prismatic, 0, sizeof(*prismatic));
+        prismatic->type = RBPS_JOINT_PRISMATIC;
+        prismatic->body_1 = (uint32_t)pp.body_1; prismatic->body_2 = (uint32_t)pp.body_2;
+        put3(prismatic->axis, pp.moving_axis);
+        put3(prismatic->r_1, pp.r_1); put3(prismatic->r_2, pp.r_2);
+        prismatic->actuation = static_cast<int32_t>(pp.actuation_type);
+        prismatic->compliance = pp.compliance; prismatic->damping = pp.damping;
+        prismatic->limited = pp.limited ? 1 : 0;
+        prismatic->lower_limit = pp.lower_limit; prismatic->upper_limit = pp.upper_limit;
+
+        const rbps::FixedJointParams fp{};
+        std::memset(fixed, 0, sizeof(*fixed));
+        fixed->type = RBPS_JOINT_FIXED;
+        fixed->body_1 = (uint32_t)fp.body_1; fixed->body_2 = (uint32_t)fp.body_2;
+        put3(fixed->r_1, fp.r_1); put3(fixed->r_2, fp.r_2);
+
+        const rbps::World w{};
+        const rbc::BroadPhaseConfig bc{};
+        world_cfg[0] = w.timestep;
+        world_cfg[1] = w.substeps;
+        world_cfg[2] = bc.fat_margin;
+        world_cfg[3] = bc.reinsert_threshold;
     }
 
     void ref_step(void *h, int n)

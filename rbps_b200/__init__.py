@@ -93,6 +93,7 @@ def lib():
             "rbps_batch_get_stats": (i, [_P, C.POINTER(Stats)]),
             "rbps_batch_get_sap_state": (i, [_P, C.c_uint32, _D, _U, C.POINTER(C.c_float), _U]),
             "rbps_debug_broadphase": (i, [_P, C.c_uint32, _U]),
+            "rbps_batch_collide": (i, [_P, C.c_uint32, _P, _D, _P, _D, _P]),
             "rbps_bp_create": (i, [C.c_double, C.c_double, C.POINTER(_P)]),
             "rbps_bp_destroy": (i, [_P]),
             "rbps_bp_insert": (i, [_P, C.c_uint32, _D, _U]),
@@ -202,9 +203,33 @@ class Batch:
             _check(L.rbps_world_add_joint(self.h, w, C.c_void_p(joints.ctypes.data + i * joints.itemsize), None))
         self._counts[w] = len(bodies)
 
+    def add_hull(self, verts, tris):
+        """Registers a convex hull (before commit); returns its hull id."""
+        v = np.ascontiguousarray(verts, np.float64)
+        t = np.ascontiguousarray(tris, np.uint32)
+        hid = C.c_uint32(0)
+        _check(lib().rbps_hull_create(self.h, _dp(v), len(v), t.ctypes.data_as(_U), len(t), C.byref(hid)))
+        return hid.value
+
     def commit(self):
         _check(lib().rbps_batch_commit(self.h))
         self.committed = True
+
+    def collide(self, a, tf_a, b, tf_b):
+        """Device narrowphase (rbc::dispatch) of n shape pairs: collider
+        descriptors a, b (abi.COLLIDER_DT) and transforms (n, 7) = position +
+        quaternion wxyz.  Returns abi.MANIFOLD_DT records."""
+        a = np.ascontiguousarray(a, abi.COLLIDER_DT)
+        b = np.ascontiguousarray(b, abi.COLLIDER_DT)
+        ta = np.ascontiguousarray(tf_a, np.float64).reshape(-1, 7)
+        tb = np.ascontiguousarray(tf_b, np.float64).reshape(-1, 7)
+        n = len(a)
+        if not (len(b) == n and len(ta) == n and len(tb) == n):
+            raise ValueError("collide: a, b, tf_a and tf_b must have the same length")
+        out = np.zeros(max(n, 1), abi.MANIFOLD_DT)
+        _check(lib().rbps_batch_collide(self.h, n, C.c_void_p(a.ctypes.data), _dp(ta), C.c_void_p(b.ctypes.data),
+                                        _dp(tb), C.c_void_p(out.ctypes.data)))
+        return out[:n]
 
     def step(self, n=1):
         _check(lib().rbps_batch_step(self.h, n))

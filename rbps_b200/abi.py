@@ -13,6 +13,11 @@ ERR_CAPACITY = -2
 ERR_CUDA = -3
 ERR_NOT_CONVERGED = -4
 ERR_STATE = -5
+ERR_INTERNAL = -6
+
+COLLIDE_MISS = 0
+COLLIDE_HIT = 1
+COLLIDE_UNSUPPORTED = 2
 
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
@@ -99,8 +104,19 @@ CONTACT_DT = np.dtype([
     ("pad_", np.int32),
 ], align=True)
 
-# byte sizes the C header fixes (checked by tests/test_abi.py)
-STRUCT_SIZES = {"body": 168, "collider": 136, "joint": 176, "contact": 240}
+MANIFOLD_DT = np.dtype([
+    ("status", np.int32),
+    ("n_points", np.int32),
+    ("normal", np.float64, 3),
+    ("position", np.float64, (4, 3)),
+    ("depth", np.float64, 4),
+], align=True)
+
+# byte sizes of the C structs (the CPU tests compile the header to check them)
+STRUCT_SIZES = {"rbps_body_desc": 168, "rbps_collider_desc": 136, "rbps_joint_desc": 176, "rbps_contact": 200,
+                "rbps_manifold": 160}
+DTYPES = {"rbps_body_desc": BODY_DT, "rbps_collider_desc": COLLIDER_DT, "rbps_joint_desc": JOINT_DT,
+          "rbps_contact": CONTACT_DT, "rbps_manifold": MANIFOLD_DT}
 
 
 def body_default():
@@ -129,7 +145,8 @@ def joint_default(jtype=JOINT_REVOLUTE):
     """Revolute/Prismatic/FixedJointParams{} (JointAPI.hpp:24-57)."""
     j = np.zeros(1, JOINT_DT)[0]
     j["type"] = jtype
-    j["axis"] = (1.0, 0.0, 0.0)
+    if jtype != JOINT_FIXED:
+        j["axis"] = (1.0, 0.0, 0.0)
     if jtype == JOINT_REVOLUTE:
         j["limit_axis"] = (0.0, 1.0, 0.0)
     return j

@@ -243,7 +243,8 @@ extern "C" void rbps_joint_desc_default(rbps_joint_desc *d, int32_t type)
 {
     std::memset(d, 0, sizeof(*d));
     d->type = type;
-    d->axis[0] = 1.0;
+    if (type != RBPS_JOINT_FIXED) // FixedJointParams has no axis (JointAPI.hpp:63-69)
+        d->axis[0] = 1.0;
     if (type == RBPS_JOINT_REVOLUTE)
         d->limit_axis[1] = 1.0;
 }
@@ -1457,6 +1458,78 @@ extern "C" RBPS_API int rbps_debug_broadphase(rbps_batch *b, uint32_t world, uin
     if (world >= b->wdev.size() || b->wdev[world].n_bodies > kSmallWorldBodies)
         return fail(RBPS_ERR_INVALID, "rbps_debug_broadphase: small worlds only");
     return DISPATCH_PREC(b, debug_bp_typed, b, world, counts);
+}
+
+// Device narrowphase of independent shape pairs (see rbps_batch_collide in
+// rbps_gpu.h).
+static_assert(sizeof(CollideOut) == sizeof(rbps_manifold), "CollideOut must mirror rbps_manifold");
+
+template <class T, class P>
+static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> &sa, const double *tf_a,
+                         const std::vector<ShapeDev> &sb, const double *tf_b, rbps_manifold *out)
+{
+    HullSetDev hs{b->hull_verts, b->hull_voff, b->hull_aabb};
+    const size_t shape_bytes = (size_t)n * sizeof(ShapeDev), tf_bytes = (size_t)n * 7 * sizeof(double);
+    char *d = nullptr;
+    const size_t total = 2 * shape_bytes + 2 * tf_bytes + (size_t)n * sizeof(CollideOut);
+    CU(cudaMalloc(&d, total));
+    ShapeDev *dsa = (ShapeDev *)d, *dsb = (ShapeDev *)(d + shape_bytes);
+    double *dta = (double *)(d + 2 * shape_bytes), *dtb = (double *)(d + 2 * shape_bytes + tf_bytes);
+    CollideOut *dout = (CollideOut *)(d + 2 * shape_bytes + 2 * tf_bytes);
+    cudaError_t e = cudaMemcpyAsync(dsa, sa.data(), shape_bytes, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dsb, sb.data(), shape_bytes, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dta, tf_a, tf_bytes, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dtb, tf_b, tf_bytes, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = launch_collide<T, P>(dsa, dta, dsb, dtb, hs, n, dout, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dout, (size_t)n * sizeof(CollideOut), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(b->stream);
+    cudaFree(d);
+    if (e != cudaSuccess)
+        return fail(RBPS_ERR_CUDA, "rbps_batch_collide: %s", cudaGetErrorString(e));
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_collide(rbps_batch *b, uint32_t n, const rbps_collider_desc *a, const double *tf_a,
+                                  const rbps_collider_desc *bd, const double *tf_b, rbps_manifold *out)
+{
+    if (!b)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_collide: null batch");
+    if (n == 0)
+        return RBPS_OK;
+    if (!a || !bd || !tf_a || !tf_b || !out)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_collide: null buffer");
+    std::vector<ShapeDev> sa(n), sb(n);
+    bool uses_hull = false;
+    for (uint32_t i = 0; i < n; ++i)
+        for (int side = 0; side < 2; ++side)
+        {
+            const rbps_collider_desc &c = side ? bd[i] : a[i];
+            if (c.shape != RBPS_SHAPE_SPHERE && c.shape != RBPS_SHAPE_BOX && c.shape != RBPS_SHAPE_CAPSULE &&
+                c.shape != RBPS_SHAPE_PLANE && c.shape != RBPS_SHAPE_CONVEX_HULL)
+                return fail(RBPS_ERR_INVALID, "rbps_batch_collide: pair %u has an unknown shape %d", i, c.shape);
+            if (c.shape == RBPS_SHAPE_CONVEX_HULL)
+            {
+                if (c.hull >= b->hulls.size())
+                    return fail(RBPS_ERR_INVALID, "rbps_batch_collide: hull %u does not exist", c.hull);
+                uses_hull = true;
+            }
+            ShapeDev s{};
+            s.kind = c.shape;
+            s.hull = (int)c.hull;
+            for (int k = 0; k < 4; ++k)
+                s.p[k] = c.params[k];
+            (side ? sb : sa)[i] = s;
+        }
+    if (uses_hull && !b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_collide: commit the batch before colliding hulls");
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, collide_typed, b, n, sa, tf_a, sb, tf_b, out);
 }
 
 // One step with host I/O (see rbps_batch_step_io in rbps_gpu.h).

@@ -760,6 +760,10 @@ namespace rbps_gpu
                                                          cudaStream_t);                                           \
     template cudaError_t rbps_gpu::occupancy_small<T, P>(int, int *);                                              \
     template cudaError_t rbps_gpu::occupancy_big<T, P>(int, int *);                                               \
+    template cudaError_t rbps_gpu::launch_collide<T, P>(const rbps_gpu::ShapeDev *, const double *,               \
+                                                       const rbps_gpu::ShapeDev *, const double *,               \
+                                                       const rbps_gpu::HullSetDev &, uint32_t,                   \
+                                                       rbps_gpu::CollideOut *, cudaStream_t);                    \
     template cudaError_t rbps_gpu::launch_debug_broadphase<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int,    \
                                                                  uint32_t *, cudaStream_t);                         \
     template cudaError_t rbps_gpu::launch_io<T, P>(const rbps_gpu::Engine<T, P> &, int, double *, double *,       \
@@ -827,6 +831,59 @@ namespace rbps_gpu
                                         cudaStream_t stream)
     {
         k_debug_broadphase<T, P><<<1, block, 0, stream>>>(e, w, out);
+        return cudaGetLastError();
+    }
+
+    // rbc::dispatch (Dispatcher.hpp:208-213) on independent shape pairs, one
+    // thread per pair; transforms are 7 doubles (position, quaternion wxyz).
+    template <class T, class P>
+    __global__ void k_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
+                              const HullSetDev hulls, uint32_t n, CollideOut *out)
+    {
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n)
+            return;
+        auto load_tf = [](const double *p) {
+            tf<T> t;
+            t.pos = vec3<T>(T(p[0]), T(p[1]), T(p[2]));
+            t.rot = quat<T>(T(p[3]), T(p[4]), T(p[5]), T(p[6]));
+            return t;
+        };
+        const tf<T> a = load_tf(ta + 7 * (size_t)i), b = load_tf(tb + 7 * (size_t)i);
+        Manifold<T> m;
+        m.n = 0;
+        const int res = dispatch_pair(sa[i], a, sb[i], b, hulls, m);
+        CollideOut o;
+        o.status = res;
+        o.n_points = res == kHit ? m.n : 0;
+        o.normal[0] = o.normal[1] = o.normal[2] = 0.0;
+        for (int k = 0; k < 4; ++k)
+        {
+            o.depth[k] = 0.0;
+            o.position[k][0] = o.position[k][1] = o.position[k][2] = 0.0;
+        }
+        if (res == kHit)
+        {
+            o.normal[0] = double(m.normal.x);
+            o.normal[1] = double(m.normal.y);
+            o.normal[2] = double(m.normal.z);
+            for (int k = 0; k < m.n && k < 4; ++k)
+            {
+                o.position[k][0] = double(m.pos[k].x);
+                o.position[k][1] = double(m.pos[k].y);
+                o.position[k][2] = double(m.pos[k].z);
+                o.depth[k] = double(m.depth[k]);
+            }
+        }
+        out[i] = o;
+    }
+
+    template <class T, class P>
+    cudaError_t launch_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
+                               const HullSetDev &hulls, uint32_t n, CollideOut *out, cudaStream_t stream)
+    {
+        if (n)
+            k_collide<T, P><<<(n + 127) / 128, 128, 0, stream>>>(sa, ta, sb, tb, hulls, n, out);
         return cudaGetLastError();
     }
 } // namespace rbps_gpu

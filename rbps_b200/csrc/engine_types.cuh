@@ -141,6 +141,17 @@ namespace rbps_gpu
     template <class T, class P>
     cudaError_t launch_io(const Engine<T, P> &e, int dir, double *a, double *b, uint32_t n, int grid,
                           cudaStream_t stream);
+    // Output of one device narrowphase test; the layout of rbps_manifold.
+    struct CollideOut
+    {
+        int32_t status, n_points;
+        double normal[3];
+        double position[4][3];
+        double depth[4];
+    };
+    template <class T, class P>
+    cudaError_t launch_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
+                               const HullSetDev &hulls, uint32_t n, CollideOut *out, cudaStream_t stream);
     template <class T, class P>
     cudaError_t launch_debug_broadphase(const Engine<T, P> &e, uint32_t world, int block, uint32_t *out,
                                         cudaStream_t stream);

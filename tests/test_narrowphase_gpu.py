@@ -1,0 +1,174 @@
+"""Narrowphase parity: the device rbc::dispatch (rbps_batch_collide) against
+the oracle (the reference's own rbc::dispatch, Dispatcher.hpp:208-213).
+
+* the reference's analytic test cases (tests/rbc/analytic/*.cpp), FP64:
+  manifold bit-identical to the oracle, and the reference test's own
+  assertion holds;
+* collide(A, B) against collide(B, A) for the reference's symmetry tests;
+* seeded pose sweeps of every analytic shape pairing, FP64 bit-identical;
+  FP32 within a stated tolerance where both engines agree on the contact
+  feature.
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+from rbps_b200 import abi, scenes
+
+import narrow_cases as NC
+
+pytestmark = pytest.mark.gpu
+
+
+def _world_with_hulls():
+    """An empty world holding the fixture hulls (ids 0 = tet, 1 = cube)."""
+    b = np.zeros(1, abi.BODY_DT)
+    b[0] = abi.body_default()
+    b[0]["type"] = abi.BODY_STATIC
+    c = np.zeros(1, abi.COLLIDER_DT)
+    c[0] = abi.collider_default()
+    c[0]["shape"] = abi.SHAPE_PLANE
+    c[0]["params"] = (0, 1, 0, 0)
+    c[0]["is_static"] = 1
+    hulls = [NC.HULLS["tet"], NC.HULLS["cube"]]
+    return scenes.WorldSpec(b, np.zeros((1, 3)), c, np.zeros(0, abi.JOINT_DT), hulls)
+
+
+@pytest.fixture(scope="module")
+def engines(rbps, ref):
+    spec = _world_with_hulls()
+    out = {}
+    for prec in (abi.PRECISION_FP64, abi.PRECISION_FP32):
+        bt = rbps.Batch(1, 1.0 / 60.0, 1, precision=prec)
+        bt.add_world(0, spec)
+        bt.commit()
+        out[prec] = bt
+    rw = ref.RefWorld(spec, 1.0 / 60.0, 1)
+    yield out, rw
+    for bt in out.values():
+        bt.close()
+
+
+def _run(engines, prec, sa, ta, sb, tb):
+    batches, rw = engines
+    return batches[prec].collide(sa, ta, sb, tb), rw.collide(sa, ta, sb, tb)
+
+
+def _same(g, r):
+    """Bit-identical manifolds (status, count, normal, points, depths)."""
+    if int(g["status"]) != int(r["status"]) or int(g["n_points"]) != int(r["n_points"]):
+        return False
+    if int(g["status"]) != abi.COLLIDE_HIT:
+        return True
+    k = int(g["n_points"])
+    return (np.array_equal(g["normal"], r["normal"]) and np.array_equal(g["position"][:k], r["position"][:k])
+            and np.array_equal(g["depth"][:k], r["depth"][:k]))
+
+
+def _check_expectation(m, exp, ta):
+    hit = int(m["status"]) == abi.COLLIDE_HIT
+    assert hit == exp["hit"]
+    if not hit:
+        return
+    k = int(m["n_points"])
+    if "depth" in exp:
+        v, tol = exp["depth"]
+        assert abs(m["depth"][0] - v) <= tol
+    if exp.get("depth_positive"):
+        assert m["depth"][0] > 0
+        assert all(m["depth"][i] > 0 for i in range(k))
+    if "n_points" in exp:
+        assert k == exp["n_points"]
+    if "all_depths" in exp:
+        v, tol = exp["all_depths"]
+        assert all(abs(m["depth"][i] - v) <= tol for i in range(k))
+    if "normal" in exp:
+        ax, v, tol = exp["normal"][:3]
+        got = m["normal"][ax] if len(exp["normal"]) > 3 else abs(m["normal"][ax])
+        assert abs(got - v) <= tol
+    if "max_depth_from_verts" in exp:
+        name, tol = exp["max_depth_from_verts"]
+        verts = NC.HULLS[name][0]
+        q = ta[3:]
+        wy = np.array([NC.rotate(q, v)[1] + ta[1] for v in verts])
+        assert abs(max(m["depth"][:k]) - max(0.0, -wy.min())) <= tol
+    assert abs(np.linalg.norm(m["normal"]) - 1.0) < 1e-9
+
+
+@pytest.mark.parametrize("case", NC.REF_CASES, ids=[c[0] for c in NC.REF_CASES])
+def test_reference_analytic_case(engines, case):
+    name, where, a, ta, b, tb, exp = case
+    sa, sb = NC.descs([a]), NC.descs([b])
+    g, r = _run(engines, abi.PRECISION_FP64, sa, np.array([ta]), sb, np.array([tb]))
+    assert _same(g[0], r[0]), f"{name} ({where}): device {g[0]} vs oracle {r[0]}"
+    _check_expectation(g[0], exp, np.array(ta))
+
+
+@pytest.mark.parametrize("case", NC.SYMMETRY_CASES, ids=[c[0] for c in NC.SYMMETRY_CASES])
+def test_reference_symmetry_case(engines, case):
+    name, where, a, ta, b, tb = case
+    sa, sb = NC.descs([a, b]), NC.descs([b, a])
+    tfa, tfb = np.array([ta, tb]), np.array([tb, ta])
+    g, r = _run(engines, abi.PRECISION_FP64, sa, tfa, sb, tfb)
+    for i in range(2):
+        assert _same(g[i], r[i]), f"{name} ({where}) order {i}"
+    assert abs(g[0]["depth"][0] - g[1]["depth"][0]) <= 1e-3
+    assert np.allclose(g[0]["normal"], -g[1]["normal"], atol=1e-3)
+
+
+PAIRINGS = [(a, b) for i, a in enumerate(NC.ANALYTIC_KINDS) for b in NC.ANALYTIC_KINDS[i:]]
+PAIRINGS += [(b, a) for (a, b) in PAIRINGS if a != b]
+PAIRINGS += [(a, "plane") for a in NC.ANALYTIC_KINDS] + [("hull", "plane")]
+
+
+@pytest.mark.parametrize("pairing", PAIRINGS, ids=[f"{a}-{b}" for a, b in PAIRINGS])
+def test_random_poses_fp64_bit_exact(engines, pairing):
+    ka, kb = pairing
+    sa, ta, sb, tb = NC.random_pairs(zlib.crc32(f"{ka}-{kb}".encode()), ka, kb, 2000)
+    g, r = _run(engines, abi.PRECISION_FP64, sa, ta, sb, tb)
+    hits = int((r["status"] == abi.COLLIDE_HIT).sum())
+    assert hits > 100, "sweep should produce contacts"
+    bad = [i for i in range(len(g)) if not _same(g[i], r[i])]
+    assert not bad, f"{len(bad)} of {len(g)} differ; first {bad[0]}: device {g[bad[0]]} oracle {r[bad[0]]}"
+
+
+@pytest.mark.parametrize("pairing", PAIRINGS, ids=[f"{a}-{b}" for a, b in PAIRINGS])
+def test_random_poses_fp32(engines, pairing):
+    """FP32 device arithmetic: where both engines report a contact with the
+    same point count, depth and points agree to 2e-4 m (absolute, shapes of
+    0.1-0.6 m around the origin) and normals to 2e-3; hit/miss may differ
+    only for grazing contacts (depth < 1e-3 m)."""
+    ka, kb = pairing
+    sa, ta, sb, tb = NC.random_pairs(zlib.crc32(f"{ka}-{kb}".encode()), ka, kb, 2000)
+    g, r = _run(engines, abi.PRECISION_FP32, sa, ta, sb, tb)
+    same_feature = 0
+    for i in range(len(g)):
+        gh, rh = int(g[i]["status"]) == 1, int(r[i]["status"]) == 1
+        if gh != rh:
+            d = (g[i] if gh else r[i])["depth"][0]
+            assert d < 1e-3, f"pair {i}: hit/miss differ at depth {d}"
+            continue
+        if not gh or g[i]["n_points"] != r[i]["n_points"]:
+            continue
+        if np.abs(g[i]["normal"] - r[i]["normal"]).max() > 2e-3:
+            continue  # a different SAT axis / feature was chosen (near-tie)
+        same_feature += 1
+        k = int(g[i]["n_points"])
+        assert np.abs(g[i]["depth"][:k] - r[i]["depth"][:k]).max() < 2e-4
+        # point order can differ inside a face clip: compare as sets
+        gp = np.sort(g[i]["position"][:k], axis=0)
+        rp = np.sort(r[i]["position"][:k], axis=0)
+        assert np.abs(gp - rp).max() < 2e-4
+    assert same_feature > 0.8 * int((r["status"] == 1).sum())
+
+
+def test_hull_pairs_report_unsupported(engines):
+    """Hull against a non-plane shape needs GJK/EPA, which the device does
+    not run: the device reports RBPS_COLLIDE_UNSUPPORTED for it."""
+    sa = NC.descs([NC.hull("cube"), NC.sphere(0.5)])
+    sb = NC.descs([NC.box(0.5, 0.5, 0.5), NC.hull("tet")])
+    ta = np.array([NC.tf(0, 0, 0), NC.tf(0, 0, 0)])
+    tb = np.array([NC.tf(1.2, 0, 0), NC.tf(0.5, 0.5, 0)])
+    g, _ = _run(engines, abi.PRECISION_FP64, sa, ta, sb, tb)
+    assert list(g["status"]) == [abi.COLLIDE_UNSUPPORTED] * 2
