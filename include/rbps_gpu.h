@@ -306,6 +306,19 @@ RBPS_API int rbps_batch_get_sap_state(rbps_batch *batch, uint32_t world, double 
  * buffers; synchronous. */
 RBPS_API int rbps_batch_collide(rbps_batch *batch, uint32_t n, const rbps_collider_desc *a, const double *tf_a,
                                 const rbps_collider_desc *b, const double *tf_b, rbps_manifold *out);
+/* Diagnostics: per-world phase timers.  With profiling enabled every step
+ * adds, per world, the SM cycles of each phase (read by the team leader
+ * after the phase's closing barrier) to RBPS_PROFILE_SLOTS uint64 slots:
+ *   0 broadphase, 1 candidate build, 2 narrowphase, 3 colouring,
+ *   4 integrate, 5 contact position solve (reference order: with joints),
+ *   6 joint position solve, 7 velocity update, 8 velocity solve, 9 stats;
+ *   12 = CTA that stepped the world, 13 / 14 = globaltimer ns at the start
+ *   and end of the world's last step.
+ * Enabling (re)zeroes the counters; it costs a few clock reads per phase. */
+#define RBPS_PROFILE_SLOTS 16
+RBPS_API int rbps_batch_set_profile(rbps_batch *batch, int32_t enable);
+/* Copies RBPS_PROFILE_SLOTS values per world for the first cap_worlds worlds. */
+RBPS_API int rbps_batch_get_profile(rbps_batch *batch, uint64_t *out, uint32_t cap_worlds);
 /* Diagnostics: the broadphase + candidate build of one world (the first
  * phase of a step) on its own, at the current poses; counts[0] = SAP pairs,
  * counts[1] = narrowphase candidates.  It updates the SAP state as a step

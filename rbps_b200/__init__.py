@@ -94,6 +94,8 @@ def lib():
             "rbps_batch_get_sap_state": (i, [_P, C.c_uint32, _D, _U, C.POINTER(C.c_float), _U]),
             "rbps_debug_broadphase": (i, [_P, C.c_uint32, _U]),
             "rbps_batch_collide": (i, [_P, C.c_uint32, _P, _D, _P, _D, _P]),
+            "rbps_batch_set_profile": (i, [_P, C.c_int32]),
+            "rbps_batch_get_profile": (i, [_P, C.POINTER(C.c_uint64), C.c_uint32]),
             "rbps_bp_create": (i, [C.c_double, C.c_double, C.POINTER(_P)]),
             "rbps_bp_destroy": (i, [_P]),
             "rbps_bp_insert": (i, [_P, C.c_uint32, _D, _U]),
@@ -214,6 +216,20 @@ class Batch:
     def commit(self):
         _check(lib().rbps_batch_commit(self.h))
         self.committed = True
+
+    PROFILE_PHASES = ("broadphase", "candidates", "narrowphase", "colouring", "integrate", "contact_pos",
+                      "joint_pos", "vel_update", "vel_solve", "stats")
+
+    def set_profile(self, on=True):
+        """Per-world phase timers (SM cycles); enabling zeroes them."""
+        _check(lib().rbps_batch_set_profile(self.h, 1 if on else 0))
+
+    def profile(self):
+        """(n_worlds, 16) uint64: phase cycles (PROFILE_PHASES order), then
+        slot 12 = CTA, 13 / 14 = start / end globaltimer ns of the last step."""
+        out = np.zeros((self.n_worlds, 16), np.uint64)
+        _check(lib().rbps_batch_get_profile(self.h, out.ctypes.data_as(C.POINTER(C.c_uint64)), self.n_worlds))
+        return out
 
     def collide(self, a, tf_a, b, tf_b):
         """Device narrowphase (rbc::dispatch) of n shape pairs: collider

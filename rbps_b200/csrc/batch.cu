@@ -149,13 +149,14 @@ struct rbps_batch
     int *error_d = nullptr;
     uint32_t *work_counter = nullptr;
     uint32_t *small_list = nullptr;
-    char *scratch_small = nullptr, *scratch_big = nullptr;
+    char *scratch = nullptr; // per-world slices (WorldDev::scr_off)
 
     // host mirrors
     std::vector<WorldDev> wdev;
     std::vector<uint32_t> small_ids, big_ids;
-    ScratchLayout lay_small{}, lay_big{};
-    int grid_small = 0, grid_big = 0;
+    PhaseLaunch phase{};      // grid / block of each phase kernel
+    int grid_big = 0;
+    uint32_t n_counters = 0;  // phase work counters per step
     uint64_t total_bodies = 0, total_dynamic = 0;
     uint32_t n_bodies_all = 0, n_coll_all = 0, n_bp_all = 0, n_joint_all = 0, n_row_all = 0;
     uint64_t steps_done = 0;
@@ -171,6 +172,8 @@ struct rbps_batch
     void *dump_cc = nullptr;
     uint32_t *dump_color = nullptr;
     uint32_t dump_pair_cap = 0, dump_cand_cap = 0;
+    unsigned long long *prof = nullptr; // phase timers (rbps_batch_set_profile)
+    bool prof_off = true;
 
     size_t t_size() const { return desc.precision == RBPS_PRECISION_FP64 ? 8 : 4; }
     size_t p_size() const { return desc.precision == RBPS_PRECISION_FP32 ? 4 : 8; }
@@ -277,7 +280,9 @@ extern "C" int rbps_batch_create(const rbps_batch_desc *desc, rbps_batch **out)
         CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
         b->own_stream = true;
     }
-    b->block = desc->block_threads ? (int)desc->block_threads : (desc->solve_mode == RBPS_SOLVE_COLORED ? 128 : 128);
+    b->block = desc->block_threads ? (int)desc->block_threads : 128;
+    for (int k = 0; k < kNumPhaseKernels; ++k)
+        b->phase.block[k] = b->block;
     *out = b.release();
     return RBPS_OK;
 }
@@ -475,6 +480,7 @@ namespace
         e.solve_mode = b->desc.solve_mode;
         e.use_vel_exp = b->desc.use_velocity_expansion;
         e.work_counter = b->work_counter;
+        e.scratch = b->scratch;
         e.small_worlds = b->small_list;
         e.n_small = (uint32_t)b->small_ids.size();
         e.dump_pairs = b->dump ? b->dump_pairs : nullptr;
@@ -483,46 +489,8 @@ namespace
         e.dump_color = b->dump ? b->dump_color : nullptr;
         e.dump_pair_cap = b->dump_pair_cap;
         e.dump_cand_cap = b->dump_cand_cap;
+        e.prof = b->prof_off ? nullptr : b->prof;
         return e;
-    }
-
-    ScratchLayout make_layout(uint32_t nbp, uint32_t nb, uint32_t pair_cap, uint32_t npc, uint32_t block,
-                              size_t cc_size)
-    {
-        ScratchLayout L{};
-        const size_t nep = 2 * (size_t)nbp + 1;
-        const size_t pc = (size_t)pair_cap + 1;
-        const size_t nc = pc + npc;
-        const size_t nt_max = std::max((nep + block - 1) / block, (pc + block - 1) / block) + 1;
-        const size_t counts = 256 * nt_max;
-        const size_t tsums = std::max((counts + block - 1) / block, nt_max) + 4;
-        size_t off = 0;
-        auto take = [&](size_t &field, size_t bytes) {
-            off = align_up(off, 128);
-            field = off;
-            off += bytes;
-        };
-        take(L.ep_k2, nep * 4);
-        take(L.ep_v2, nep * 4);
-        take(L.counts, counts * 4);
-        take(L.tile_sums, tsums * 4);
-        take(L.cnt, nep * 4);
-        take(L.pr_a, pc * 4);
-        take(L.pr_b, pc * 4);
-        take(L.pk, pc * 4);
-        take(L.pv, pc * 4);
-        take(L.pk2, pc * 4);
-        take(L.pv2, pc * 4);
-        take(L.cflag, pc * 4);
-        take(L.cand, nc * sizeof(Cand));
-        take(L.cc, nc * cc_size);
-        take(L.color, nc * 4);
-        take(L.bmask, (size_t)nb * 8 + 8);
-        take(L.bprio, (size_t)nb * 8 + 8);
-        take(L.corder, nc * 4);
-        take(L.misc, kMiscWords * 4);
-        L.stride = align_up(off, 256);
-        return L;
     }
 
     size_t cc_size_of(int precision)
@@ -921,16 +889,26 @@ static int commit_typed(rbps_batch *b)
         }
     }
     const size_t ccs = cc_size_of(b->desc.precision);
+    // per-world scratch slices
+    size_t scr_total = 0;
+    for (uint32_t w = 0; w < W; ++w)
+    {
+        WorldDev &d = b->wdev[w];
+        d.scr_off = scr_total;
+        scr_total += make_layout(d.n_bp, d.n_bodies, d.pair_cap, d.n_pc, ccs).stride;
+    }
+    if ((rc = b->alloc((void **)&b->scratch, std::max<size_t>(scr_total, 256))))
+        return rc;
     if (!b->small_ids.empty())
     {
-        int per_sm = 0;
-        CU(occupancy_small<T, P>(b->block, &per_sm));
-        if (per_sm < 1)
-            return fail(RBPS_ERR_CUDA, "step kernel cannot be resident with %d threads", b->block);
-        b->grid_small = std::min<int>((int)b->small_ids.size(), per_sm * b->sm_count);
-        b->lay_small = make_layout(s_bp, s_b, s_pc, s_npc, b->block, ccs);
-        if ((rc = b->alloc((void **)&b->scratch_small, b->lay_small.stride * b->grid_small)))
-            return rc;
+        for (int k = 0; k < kNumPhaseKernels; ++k)
+        {
+            int per_sm = 0;
+            CU(occupancy_phase<T, P>(k, b->phase.block[k], &per_sm));
+            if (per_sm < 1)
+                return fail(RBPS_ERR_CUDA, "phase kernel %d cannot be resident with %d threads", k, b->phase.block[k]);
+            b->phase.grid[k] = std::min<int>((int)b->small_ids.size(), per_sm * b->sm_count);
+        }
         if ((rc = b->upload(&b->small_list, b->small_ids)))
             return rc;
     }
@@ -941,11 +919,9 @@ static int commit_typed(rbps_batch *b)
         if (per_sm < 1)
             return fail(RBPS_ERR_CUDA, "cooperative step kernel cannot be resident");
         b->grid_big = per_sm * b->sm_count;
-        b->lay_big = make_layout(g_bp, g_b, g_pc, g_npc, b->block, ccs);
-        if ((rc = b->alloc((void **)&b->scratch_big, b->lay_big.stride)))
-            return rc;
     }
-    if ((rc = b->alloc((void **)&b->work_counter, 64)) || (rc = b->alloc((void **)&b->error_d, 64)) ||
+    b->n_counters = 2 + 4 * (uint32_t)b->desc.substeps;
+    if ((rc = b->alloc((void **)&b->work_counter, std::max<size_t>(64, 4 * (size_t)b->n_counters))) || (rc = b->alloc((void **)&b->error_d, 64)) ||
         (rc = b->alloc((void **)&b->stats_d, sizeof(WorldStats) * W)))
         return rc;
     if ((rc = b->upload(&b->worlds_d, b->wdev)))
@@ -1025,27 +1001,19 @@ template <class T, class P>
 static int step_typed(rbps_batch *b, int n)
 {
     Engine<T, P> e = make_engine<T, P>(b);
-    e.scratch = b->scratch_small;
-    e.lay = b->lay_small;
     uint64_t launches = 0;
     for (int s = 0; s < n; ++s)
     {
         if (!b->small_ids.empty())
         {
-            CU(cudaMemsetAsync(b->work_counter, 0, 4, b->stream));
-            CU(launch_step_small<T, P>(e, b->grid_small, b->block, b->stream));
-            ++launches;
+            CU(cudaMemsetAsync(b->work_counter, 0, 4 * (size_t)b->n_counters, b->stream));
+            CU(launch_step_phases<T, P>(e, b->phase, b->stream));
+            launches += b->n_counters;
         }
-        if (!b->big_ids.empty())
+        for (uint32_t w : b->big_ids)
         {
-            Engine<T, P> eb = e;
-            eb.scratch = b->scratch_big;
-            eb.lay = b->lay_big;
-            for (uint32_t w : b->big_ids)
-            {
-                CU(launch_step_big<T, P>(eb, w, b->grid_big, b->block, b->stream));
-                ++launches;
-            }
+            CU(launch_step_big<T, P>(e, w, b->grid_big, b->block, b->stream));
+            ++launches;
         }
     }
     b->launches_last = launches;
@@ -1438,8 +1406,6 @@ template <class T, class P>
 static int debug_bp_typed(rbps_batch *b, uint32_t world, uint32_t *counts)
 {
     Engine<T, P> e = make_engine<T, P>(b);
-    e.scratch = b->scratch_small;
-    e.lay = b->lay_small;
     uint32_t *d = nullptr;
     CU(cudaMalloc(&d, 16));
     CU(cudaMemset(d, 0, 16));
@@ -1458,6 +1424,39 @@ extern "C" RBPS_API int rbps_debug_broadphase(rbps_batch *b, uint32_t world, uin
     if (world >= b->wdev.size() || b->wdev[world].n_bodies > kSmallWorldBodies)
         return fail(RBPS_ERR_INVALID, "rbps_debug_broadphase: small worlds only");
     return DISPATCH_PREC(b, debug_bp_typed, b, world, counts);
+}
+
+// Phase timers (see rbps_batch_set_profile in rbps_gpu.h).
+static_assert(kProfSlots == RBPS_PROFILE_SLOTS, "profile slot count must match the header");
+
+extern "C" int rbps_batch_set_profile(rbps_batch *b, int32_t enable)
+{
+    int rc = ready(b, "rbps_batch_set_profile");
+    if (rc)
+        return rc;
+    const size_t bytes = b->wdev.size() * kProfSlots * sizeof(unsigned long long);
+    if (enable && !b->prof && (rc = b->alloc((void **)&b->prof, bytes)))
+        return rc;
+    if (enable)
+        CU(cudaMemset(b->prof, 0, bytes));
+    else
+        b->prof_off = true;
+    if (enable)
+        b->prof_off = false;
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_get_profile(rbps_batch *b, uint64_t *out, uint32_t cap_worlds)
+{
+    int rc = ready(b, "rbps_batch_get_profile");
+    if (rc)
+        return rc;
+    if (!b->prof)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_get_profile: profiling was never enabled");
+    const size_t n = std::min<size_t>(cap_worlds, b->wdev.size());
+    if (out && n)
+        CU(cudaMemcpy(out, b->prof, n * kProfSlots * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    return RBPS_OK;
 }
 
 // Device narrowphase of independent shape pairs (see rbps_batch_collide in

@@ -69,7 +69,7 @@ namespace rbps_gpu
         CandContacts<T, P> *cc;
         uint32_t *color;
         unsigned long long *bmask, *bprio;
-        uint32_t *corder, *misc;
+        uint32_t *corder, *misc, *act, *alist;
     };
 
     template <class T, class P>
@@ -95,6 +95,8 @@ namespace rbps_gpu
         s.bprio = (unsigned long long *)(base + L.bprio);
         s.corder = (uint32_t *)(base + L.corder);
         s.misc = (uint32_t *)(base + L.misc);
+        s.act = (uint32_t *)(base + L.act);
+        s.alist = (uint32_t *)(base + L.alist);
         return s;
     }
 
@@ -326,18 +328,21 @@ namespace rbps_gpu
         return n_sap + W.n_pc;
     }
 
-    // Jones-Plassmann colouring: a candidate takes the lowest colour free
-    // on both of its dynamic bodies once it holds the highest priority
-    // among the uncoloured candidates sharing them.  Candidates whose bodies
-    // have used all 64 colours go to the serial colour.  Returns the number
-    // of regular colours; corder / colour offsets are filled.
+    // Jones-Plassmann colouring of the candidates that produced contact rows
+    // in this substep (the others have nothing to relax): a candidate takes
+    // the lowest colour free on both of its dynamic bodies once it holds the
+    // highest priority among the uncoloured candidates sharing them.
+    // Candidates whose bodies have used all 64 colours go to the serial
+    // colour; idle candidates get kColorIdle and are not bucketed.  Returns
+    // the number of regular colours; corder / colour offsets are filled.
     template <class T, class P, class Team>
-    __device__ uint32_t color_candidates(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
-                                         uint32_t n_cand)
+    __device__ uint32_t color_active(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
+                                     uint32_t n_cand, BlockShared &sh)
     {
         uint32_t *misc = S.misc;
+        // compact the active candidates into alist
         for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
-            S.color[c] = 0xffffffffu;
+            S.act[c] = S.cc[c].n > 0 ? 1u : 0u;
         for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
         {
             S.bmask[b] = 0ull;
@@ -346,12 +351,21 @@ namespace rbps_gpu
         for (uint32_t x = tm.rank(); x < kMaxColorRounds + 2 * 66; x += tm.size())
             misc[kMiscCCount + x] = 0u;
         tm.sync();
+        const uint32_t n_act = team_excl_scan(tm, S.act, S.act, n_cand, S.tile_sums, sh);
+        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+        {
+            if (S.cc[c].n > 0)
+                S.alist[S.act[c]] = c;
+            S.color[c] = S.cc[c].n > 0 ? 0xffffffffu : kColorIdle;
+        }
+        tm.sync();
         const uint8_t *type = E.B.type + W.body_off;
         uint32_t round = 1;
-        for (; round <= kMaxColorRounds; ++round)
+        for (; round <= kMaxColorRounds && n_act; ++round)
         {
-            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+            for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
             {
+                const uint32_t c = S.alist[q];
                 if (S.color[c] != 0xffffffffu)
                     continue;
                 const Cand cd = S.cand[c];
@@ -363,8 +377,9 @@ namespace rbps_gpu
                     atomicMax(&S.bprio[cd.bb], val);
             }
             tm.sync();
-            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+            for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
             {
+                const uint32_t c = S.alist[q];
                 if (S.color[c] != 0xffffffffu)
                     continue;
                 const Cand cd = S.cand[c];
@@ -398,14 +413,14 @@ namespace rbps_gpu
         }
         if (round > kMaxColorRounds)
         {
-            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
-                if (S.color[c] == 0xffffffffu)
-                    S.color[c] = kColorSerial;
+            for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
+                if (S.color[S.alist[q]] == 0xffffffffu)
+                    S.color[S.alist[q]] = kColorSerial;
             tm.sync();
         }
-        // bucket by colour
-        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
-            atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
+        // bucket the active candidates by colour
+        for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
+            atomicAdd(&misc[kMiscCCount + S.color[S.alist[q]]], 1u);
         tm.sync();
         if (tm.leader())
         {
@@ -423,8 +438,9 @@ namespace rbps_gpu
             misc[kMiscFlags + 1] = ncol;
         }
         tm.sync();
-        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+        for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
         {
+            const uint32_t c = S.alist[q];
             const uint32_t slot = atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
             S.corder[slot] = c;
         }
@@ -524,66 +540,177 @@ namespace rbps_gpu
         return E.rows + j.row0;
     }
 
-    // ------------------------------------------------------------ the step
+    // Per-world phase timers (diagnostics; off when Engine::prof is null).
+    // The team leader adds the SM cycles of each phase, read after the
+    // phase's closing barrier, into prof[world * kProfSlots + phase].
+    struct PhaseClock
+    {
+        unsigned long long *p;
+        long long t;
+        __device__ PhaseClock(unsigned long long *slots, bool frame_start)
+        {
+            p = slots;
+            t = 0;
+            if (p)
+            {
+                t = clock64();
+                if (frame_start)
+                {
+                    unsigned long long g;
+                    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(g));
+                    p[kProfStartNs] = g;
+                    p[kProfCta] = blockIdx.x;
+                }
+            }
+        }
+        __device__ void mark(int phase)
+        {
+            if (!p)
+                return;
+            const long long now = clock64();
+            p[phase] += (unsigned long long)(now - t);
+            t = now;
+        }
+        __device__ void finish()
+        {
+            if (!p)
+                return;
+            unsigned long long g;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(g));
+            p[kProfEndNs] = g;
+        }
+    };
+
     template <class T, class P, class Team>
-    __device__ void world_step(const Engine<T, P> &E, const Team &tm, uint32_t w, char *scratch_base, BlockShared &sh)
+    __device__ __forceinline__ unsigned long long *prof_slots(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    {
+        return tm.leader() && E.prof ? E.prof + (size_t)w * kProfSlots : nullptr;
+    }
+
+    // The scratch slice of world W (layout from the world's own sizes).
+    template <class T, class P>
+    __device__ __forceinline__ Scr<T, P> world_scratch(const Engine<T, P> &E, const WorldDev &W)
+    {
+        return scratch_ptrs<T, P>(E.scratch + W.scr_off,
+                                  make_layout(W.n_bp, W.n_bodies, W.pair_cap, W.n_pc, sizeof(CandContacts<T, P>)));
+    }
+
+    // ------------------------------------------------------------ the step
+    // World::step (World.hpp:192-212) as phases.  Every phase ends with a
+    // team barrier and keeps its state in the world's scratch slice, so the
+    // phases run either back to back on one team (world_step) or as separate
+    // kernels over all worlds (the batched path: every CTA runs the same
+    // phase's code at a time, and each phase kernel gets its own register
+    // budget).
+
+    // Frame (once per step): SAP object update, sort, sweep; candidate list.
+    template <class T, class P, class Team>
+    __device__ void phase_frame(const Engine<T, P> &E, const Team &tm, uint32_t w, BlockShared &sh)
     {
         const WorldDev W = E.worlds[w];
-        const Scr<T, P> S = scratch_ptrs<T, P>(scratch_base, E.lay);
+        const Scr<T, P> S = world_scratch(E, W);
+        PhaseClock clk(prof_slots(E, tm, w), true);
         if (tm.leader())
-            S.misc[kMiscFlags + 3] = 0u;
-        const uint32_t n_pairs = broadphase(E, tm, W, S, sh);
-        const uint32_t n_cand = build_candidates(E, tm, W, S, n_pairs, sh);
-        const bool colored = E.solve_mode == 1;
-        uint32_t n_colors = 0;
-        if (colored)
-            n_colors = color_candidates(E, tm, W, S, n_cand);
-        const uint32_t *coff = S.misc + kMiscCOff;
-        Bodies<T, P> B = E.B;
-        uint32_t n_gjk = 0;
-
-        for (int sub = 0; sub < E.substeps; ++sub)
         {
-            // narrowphase + contacts.clear() / emit (every substep, World.hpp:205-206)
-            for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
-                narrow_candidate(E, W, S.cand[c], S.cc[c], n_gjk);
-            tm.sync();
-            // integrate (Body.cpp:18-39)
-            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
-                integrate_body(B, W.body_off + b, E.h);
-            tm.sync();
-            // position solve (World.hpp:168-173)
-            if (!colored)
+            S.misc[kMiscNGjk] = 0u;
+            S.misc[kMiscMaxColors] = 0u;
+        }
+        const uint32_t n_pairs = broadphase(E, tm, W, S, sh);
+        clk.mark(kPhBroadphase);
+        const uint32_t n_cand = build_candidates(E, tm, W, S, n_pairs, sh);
+        if (tm.leader())
+        {
+            S.misc[kMiscNPairs] = n_pairs;
+            S.misc[kMiscNCand] = n_cand;
+        }
+        tm.sync();
+        clk.mark(kPhCandidates);
+    }
+
+    // Narrowphase + contacts.clear() / emit (every substep, World.hpp:205-206).
+    template <class T, class P, class Team>
+    __device__ void phase_narrow(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    {
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = world_scratch(E, W);
+        PhaseClock clk(prof_slots(E, tm, w), false);
+        const uint32_t n_cand = S.misc[kMiscNCand];
+        uint32_t n_gjk = 0;
+        for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
+            narrow_candidate(E, W, S.cand[c], S.cc[c], n_gjk);
+        if (n_gjk)
+            atomicAdd(S.misc + kMiscNGjk, n_gjk);
+        tm.sync();
+        clk.mark(kPhNarrow);
+    }
+
+    // Colouring of the contacting candidates (colored mode), then integrate
+    // (Body.cpp:18-39).
+    template <class T, class P, class Team>
+    __device__ void phase_color_integrate(const Engine<T, P> &E, const Team &tm, uint32_t w, BlockShared &sh)
+    {
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = world_scratch(E, W);
+        PhaseClock clk(prof_slots(E, tm, w), false);
+        if (E.solve_mode == 1)
+        {
+            const uint32_t nc = color_active(E, tm, W, S, S.misc[kMiscNCand], sh);
+            if (tm.leader() && nc > S.misc[kMiscMaxColors])
+                S.misc[kMiscMaxColors] = nc;
+        }
+        clk.mark(kPhColor);
+        for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            integrate_body(E.B, W.body_off + b, E.h);
+        tm.sync();
+        clk.mark(kPhIntegrate);
+    }
+
+    // Position solve (World.hpp:168-173): contacts, joint errors, joint rows;
+    // then the velocity update (Body.cpp:41-57).
+    template <class T, class P, class Team>
+    __device__ void phase_position(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    {
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = world_scratch(E, W);
+        PhaseClock clk(prof_slots(E, tm, w), false);
+        const Bodies<T, P> &B = E.B;
+        const uint32_t n_cand = S.misc[kMiscNCand];
+        if (E.solve_mode != 1)
+        {
+            if (tm.leader())
             {
-                if (tm.leader())
+                for (uint32_t c = 0; c < n_cand; ++c)
+                    solve_cand_position(E, W, S.cand[c], S.cc[c]);
+                for (uint32_t j = 0; j < W.n_joints; ++j)
                 {
-                    for (uint32_t c = 0; c < n_cand; ++c)
-                        solve_cand_position(E, W, S.cand[c], S.cc[c]);
-                    for (uint32_t j = 0; j < W.n_joints; ++j)
-                    {
-                        Joint<T> jt = E.joints[W.joint_off + j];
-                        joint_errors(B, jt, joint_rows(E, jt), E.h);
-                        E.joints[W.joint_off + j].target_pos = jt.target_pos;
-                    }
-                    for (uint32_t j = 0; j < W.n_joints; ++j)
-                    {
-                        const Joint<T> &jt = E.joints[W.joint_off + j];
-                        solve_joint_rows(B, jt, joint_rows(E, jt), E.inv_h);
-                    }
+                    Joint<T> jt = E.joints[W.joint_off + j];
+                    joint_errors(B, jt, joint_rows(E, jt), E.h);
+                    E.joints[W.joint_off + j].target_pos = jt.target_pos;
+                }
+                for (uint32_t j = 0; j < W.n_joints; ++j)
+                {
+                    const Joint<T> &jt = E.joints[W.joint_off + j];
+                    solve_joint_rows(B, jt, joint_rows(E, jt), E.inv_h);
+                }
+            }
+            tm.sync();
+            clk.mark(kPhContactPos); // reference order: contacts and joints in one phase
+        }
+        else
+        {
+            const uint32_t *coff = S.misc + kMiscCOff;
+            const uint32_t n_colors = S.misc[kMiscNColors];
+            for (uint32_t col = 0; col < n_colors; ++col)
+            {
+                for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
+                {
+                    const uint32_t c = S.corder[q];
+                    solve_cand_position(E, W, S.cand[c], S.cc[c]);
                 }
                 tm.sync();
             }
-            else
+            if (coff[kColorSerial + 1] > coff[kColorSerial])
             {
-                for (uint32_t col = 0; col < n_colors; ++col)
-                {
-                    for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
-                    {
-                        const uint32_t c = S.corder[q];
-                        solve_cand_position(E, W, S.cand[c], S.cc[c]);
-                    }
-                    tm.sync();
-                }
                 if (tm.leader())
                     for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
                     {
@@ -591,6 +718,10 @@ namespace rbps_gpu
                         solve_cand_position(E, W, S.cand[c], S.cc[c]);
                     }
                 tm.sync();
+            }
+            clk.mark(kPhContactPos);
+            if (W.n_joints)
+            {
                 for (uint32_t j = tm.rank(); j < W.n_joints; j += tm.size())
                 {
                     Joint<T> jt = E.joints[W.joint_off + j];
@@ -609,33 +740,49 @@ namespace rbps_gpu
                     tm.sync();
                 }
             }
-            // velocity update (Body.cpp:41-57)
-            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
-                update_velocity_body(B, W.body_off + b, E.inv_h);
-            tm.sync();
-            // velocity solve (World.hpp:176-180)
-            if (!colored)
+            clk.mark(kPhJointPos);
+        }
+        for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            update_velocity_body(B, W.body_off + b, E.inv_h);
+        tm.sync();
+        clk.mark(kPhVelUpdate);
+    }
+
+    // Velocity solve (World.hpp:176-180): restitution / friction, joint damping.
+    template <class T, class P, class Team>
+    __device__ void phase_velocity(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    {
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = world_scratch(E, W);
+        PhaseClock clk(prof_slots(E, tm, w), false);
+        const Bodies<T, P> &B = E.B;
+        if (E.solve_mode != 1)
+        {
+            if (tm.leader())
             {
-                if (tm.leader())
+                const uint32_t n_cand = S.misc[kMiscNCand];
+                for (uint32_t c = 0; c < n_cand; ++c)
+                    solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
+                for (uint32_t j = 0; j < W.n_joints; ++j)
+                    joint_damping(B, E.joints[W.joint_off + j], E.h);
+            }
+            tm.sync();
+        }
+        else
+        {
+            const uint32_t *coff = S.misc + kMiscCOff;
+            const uint32_t n_colors = S.misc[kMiscNColors];
+            for (uint32_t col = 0; col < n_colors; ++col)
+            {
+                for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
                 {
-                    for (uint32_t c = 0; c < n_cand; ++c)
-                        solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
-                    for (uint32_t j = 0; j < W.n_joints; ++j)
-                        joint_damping(B, E.joints[W.joint_off + j], E.h);
+                    const uint32_t c = S.corder[q];
+                    solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
                 }
                 tm.sync();
             }
-            else
+            if (coff[kColorSerial + 1] > coff[kColorSerial])
             {
-                for (uint32_t col = 0; col < n_colors; ++col)
-                {
-                    for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
-                    {
-                        const uint32_t c = S.corder[q];
-                        solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
-                    }
-                    tm.sync();
-                }
                 if (tm.leader())
                     for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
                     {
@@ -643,18 +790,28 @@ namespace rbps_gpu
                         solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
                     }
                 tm.sync();
-                const uint32_t *jco = E.jcolor_off + W.jc_off;
-                for (uint32_t jc = 0; jc < W.n_jcolors; ++jc)
-                {
-                    for (uint32_t q = jco[jc] + tm.rank(); q < jco[jc + 1]; q += tm.size())
-                        joint_damping(B, E.joints[W.joint_off + E.jorder[q]], E.h);
-                    tm.sync();
-                }
+            }
+            const uint32_t *jco = E.jcolor_off + W.jc_off;
+            for (uint32_t jc = 0; jc < W.n_jcolors; ++jc)
+            {
+                for (uint32_t q = jco[jc] + tm.rank(); q < jco[jc + 1]; q += tm.size())
+                    joint_damping(B, E.joints[W.joint_off + E.jorder[q]], E.h);
+                tm.sync();
             }
         }
+        clk.mark(kPhVelSolve);
+    }
 
-        // statistics and parity dumps of the last substep
-        uint32_t *ncon = S.misc + kMiscFlags + 2;
+    // Statistics and parity dumps of the last substep.
+    template <class T, class P, class Team>
+    __device__ void phase_stats(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    {
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = world_scratch(E, W);
+        PhaseClock clk(prof_slots(E, tm, w), false);
+        const bool colored = E.solve_mode == 1;
+        const uint32_t n_cand = S.misc[kMiscNCand];
+        uint32_t *ncon = S.misc + kMiscNContacts;
         if (tm.leader())
             *ncon = 0;
         tm.sync();
@@ -672,49 +829,105 @@ namespace rbps_gpu
         }
         if (local)
             atomicAdd(ncon, local);
-        if (n_gjk)
-            atomicAdd(S.misc + kMiscFlags + 3, n_gjk);
         tm.sync();
         if (tm.leader())
         {
+            const uint32_t *coff = S.misc + kMiscCOff;
             WorldStats st;
-            st.n_pairs = n_pairs;
+            st.n_pairs = S.misc[kMiscNPairs];
             st.n_cand = n_cand;
             st.n_contacts = *ncon;
-            st.n_colors = n_colors;
+            st.n_colors = S.misc[kMiscMaxColors];
             st.n_serial = colored ? coff[kColorSerial + 1] - coff[kColorSerial] : 0u;
-            st.n_gjk = S.misc[kMiscFlags + 3];
+            st.n_gjk = S.misc[kMiscNGjk];
             st.pad_[0] = st.pad_[1] = 0;
             E.stats[w] = st;
-            S.misc[kMiscFlags + 3] = 0;
         }
         tm.sync();
+        clk.mark(kPhStats);
+        clk.finish();
+    }
+
+    // All phases of one step back to back on one team.
+    template <class T, class P, class Team>
+    __device__ void world_step(const Engine<T, P> &E, const Team &tm, uint32_t w, BlockShared &sh)
+    {
+        phase_frame(E, tm, w, sh);
+        for (int sub = 0; sub < E.substeps; ++sub)
+        {
+            phase_narrow(E, tm, w);
+            phase_color_integrate(E, tm, w, sh);
+            phase_position(E, tm, w);
+            phase_velocity(E, tm, w);
+        }
+        phase_stats(E, tm, w);
     }
 
     // ------------------------------------------------------------ kernels
     constexpr int kMaxBlock = 256;
 
-    // Persistent CTAs pull whole worlds (largest first) from a work counter.
-    template <class T, class P>
-    __global__ void __launch_bounds__(kMaxBlock) k_step_small(const Engine<T, P> E)
+    // Persistent CTAs pull small worlds (largest first) from a work counter
+    // and run one phase on each.
+    template <class F>
+    __device__ __forceinline__ void each_small_world(const uint32_t *list, uint32_t n, uint32_t *counter, F &&f)
     {
-        __shared__ BlockShared sh;
         __shared__ uint32_t next;
-        BlockTeam tm;
-        char *scratch = E.scratch + (size_t)blockIdx.x * E.lay.stride;
-        if (threadIdx.x == 0)
-            scratch_ptrs<T, P>(scratch, E.lay).misc[kMiscFlags + 3] = 0;
         for (;;)
         {
             if (threadIdx.x == 0)
-                next = atomicAdd(E.work_counter, 1u);
+                next = atomicAdd(counter, 1u);
             __syncthreads();
             const uint32_t q = next;
             __syncthreads();
-            if (q >= E.n_small)
+            if (q >= n)
                 break;
-            world_step(E, tm, E.small_worlds[q], scratch, sh);
+            f(list[q]);
         }
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_phase_frame(const Engine<T, P> E, uint32_t ctr)
+    {
+        __shared__ BlockShared sh;
+        BlockTeam tm;
+        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr, [&](uint32_t w) { phase_frame(E, tm, w, sh); });
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_phase_narrow(const Engine<T, P> E, uint32_t ctr)
+    {
+        BlockTeam tm;
+        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr, [&](uint32_t w) { phase_narrow(E, tm, w); });
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_phase_color(const Engine<T, P> E, uint32_t ctr)
+    {
+        __shared__ BlockShared sh;
+        BlockTeam tm;
+        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr,
+                         [&](uint32_t w) { phase_color_integrate(E, tm, w, sh); });
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_phase_position(const Engine<T, P> E, uint32_t ctr)
+    {
+        BlockTeam tm;
+        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr, [&](uint32_t w) { phase_position(E, tm, w); });
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_phase_velocity(const Engine<T, P> E, uint32_t ctr)
+    {
+        BlockTeam tm;
+        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr, [&](uint32_t w) { phase_velocity(E, tm, w); });
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_phase_stats(const Engine<T, P> E, uint32_t ctr)
+    {
+        BlockTeam tm;
+        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr, [&](uint32_t w) { phase_stats(E, tm, w); });
     }
 
     // One large world on the whole cooperative grid.
@@ -723,13 +936,24 @@ namespace rbps_gpu
     {
         __shared__ BlockShared sh;
         GridTeam tm;
-        world_step(E, tm, w, E.scratch, sh);
+        world_step(E, tm, w, sh);
     }
 
+    // Enqueues one step of every small world: 2 + 4 * substeps phase kernels
+    // (work counters ctr_base .. ctr_base + 1 + 4 * substeps must be zero).
     template <class T, class P>
-    cudaError_t launch_step_small(const Engine<T, P> &e, int grid, int block, cudaStream_t stream)
+    cudaError_t launch_step_phases(const Engine<T, P> &e, const PhaseLaunch &pl, cudaStream_t stream)
     {
-        k_step_small<T, P><<<grid, block, 0, stream>>>(e);
+        uint32_t ctr = 0;
+        k_phase_frame<T, P><<<pl.grid[kKFrame], pl.block[kKFrame], 0, stream>>>(e, ctr++);
+        for (int s = 0; s < e.substeps; ++s)
+        {
+            k_phase_narrow<T, P><<<pl.grid[kKNarrow], pl.block[kKNarrow], 0, stream>>>(e, ctr++);
+            k_phase_color<T, P><<<pl.grid[kKColor], pl.block[kKColor], 0, stream>>>(e, ctr++);
+            k_phase_position<T, P><<<pl.grid[kKPosition], pl.block[kKPosition], 0, stream>>>(e, ctr++);
+            k_phase_velocity<T, P><<<pl.grid[kKVelocity], pl.block[kKVelocity], 0, stream>>>(e, ctr++);
+        }
+        k_phase_stats<T, P><<<pl.grid[kKStats], pl.block[kKStats], 0, stream>>>(e, ctr++);
         return cudaGetLastError();
     }
 
@@ -742,9 +966,19 @@ namespace rbps_gpu
     }
 
     template <class T, class P>
-    cudaError_t occupancy_small(int block, int *blocks_per_sm)
+    cudaError_t occupancy_phase(int kernel, int block, int *blocks_per_sm)
     {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_small<T, P>, block, 0);
+        switch (kernel)
+        {
+        case kKFrame: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_phase_frame<T, P>, block, 0);
+        case kKNarrow: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_phase_narrow<T, P>, block, 0);
+        case kKColor: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_phase_color<T, P>, block, 0);
+        case kKPosition:
+            return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_phase_position<T, P>, block, 0);
+        case kKVelocity:
+            return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_phase_velocity<T, P>, block, 0);
+        default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_phase_stats<T, P>, block, 0);
+        }
     }
 
     template <class T, class P>
@@ -755,10 +989,11 @@ namespace rbps_gpu
 } // namespace rbps_gpu
 
 #define RBPS_INSTANTIATE_ENGINE(T, P)                                                                          \
-    template cudaError_t rbps_gpu::launch_step_small<T, P>(const rbps_gpu::Engine<T, P> &, int, int, cudaStream_t); \
+    template cudaError_t rbps_gpu::launch_step_phases<T, P>(const rbps_gpu::Engine<T, P> &,                        \
+                                                            const rbps_gpu::PhaseLaunch &, cudaStream_t);           \
     template cudaError_t rbps_gpu::launch_step_big<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int, int,        \
                                                          cudaStream_t);                                           \
-    template cudaError_t rbps_gpu::occupancy_small<T, P>(int, int *);                                              \
+    template cudaError_t rbps_gpu::occupancy_phase<T, P>(int, int, int *);                                         \
     template cudaError_t rbps_gpu::occupancy_big<T, P>(int, int *);                                               \
     template cudaError_t rbps_gpu::launch_collide<T, P>(const rbps_gpu::ShapeDev *, const double *,               \
                                                        const rbps_gpu::ShapeDev *, const double *,               \
@@ -816,7 +1051,7 @@ namespace rbps_gpu
         __shared__ BlockShared sh;
         BlockTeam tm;
         const WorldDev W = E.worlds[w];
-        const Scr<T, P> S = scratch_ptrs<T, P>(E.scratch, E.lay);
+        const Scr<T, P> S = world_scratch(E, W);
         const uint32_t n_pairs = broadphase(E, tm, W, S, sh);
         const uint32_t n_cand = build_candidates(E, tm, W, S, n_pairs, sh);
         if (threadIdx.x == 0)

@@ -24,6 +24,7 @@ namespace rbps_gpu
         uint32_t jc_off, n_jcolors;  // joint colour offsets: n_jcolors + 1 entries
         uint32_t pair_cap;
         uint32_t dump_slot;          // index of this world's dump slices, ~0u = none
+        uint64_t scr_off;            // byte offset of the world's scratch slice
     };
 
     struct WorldStats
@@ -66,10 +67,21 @@ namespace rbps_gpu
         size_t bprio;            // per-body priority (u64)
         size_t corder;           // candidates sorted by colour
         size_t misc;             // small counters
+        size_t act, alist;       // active-candidate flags / compacted list (colored mode)
         size_t stride;           // bytes per executor
     };
 
+    // Per-world scratch: every world owns a slice of the batch scratch buffer
+    // (WorldDev::scr_off) laid out from the world's own sizes, so a world's
+    // frame data (SAP pairs, candidates, contact manifolds, colours) stays
+    // in place between the phase kernels of a step.  Radix-sort and scan
+    // tiles are sized for the smallest team tile (kTileMin threads).
+    constexpr uint32_t kTileMin = 32;
+
+    RBPS_HD size_t scr_align(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
     constexpr uint32_t kColorSerial = 64;  // overflow colour, solved by one thread
+    constexpr uint32_t kColorIdle = 65;    // candidate without contact rows this substep
     constexpr uint32_t kMaxColorRounds = 96;
     constexpr uint32_t kMiscWords = 64 + 2 * 66 + kMaxColorRounds + 8;
     // misc layout (u32 words)
@@ -77,6 +89,77 @@ namespace rbps_gpu
     constexpr uint32_t kMiscCCount = 8;                 // 66 colour counts
     constexpr uint32_t kMiscCOff = 8 + 66;              // 66 colour offsets (+ fill)
     constexpr uint32_t kMiscLeft = 8 + 2 * 66;          // per-round "uncoloured left"
+    // misc scalars: kMiscFlags + 1 colours of this substep, + 2 contact rows,
+    // + 3 GJK candidates, + 4 unclamped SAP pairs, + 5 SAP pairs, + 6 narrowphase
+    // candidates, + 7 most colours over the step's substeps
+    constexpr uint32_t kMiscNColors = kMiscFlags + 1, kMiscNContacts = kMiscFlags + 2, kMiscNGjk = kMiscFlags + 3,
+                       kMiscPairsRaw = kMiscFlags + 4, kMiscNPairs = kMiscFlags + 5, kMiscNCand = kMiscFlags + 6,
+                       kMiscMaxColors = kMiscFlags + 7;
+
+    RBPS_HD ScratchLayout make_layout(uint32_t nbp, uint32_t nb, uint32_t pair_cap, uint32_t npc, size_t cc_size)
+    {
+        ScratchLayout L{};
+        const size_t nep = 2 * (size_t)nbp + 1;
+        const size_t pc = (size_t)pair_cap + 1;
+        const size_t nc = pc + npc;
+        size_t nt = (nep + kTileMin - 1) / kTileMin;
+        nt = nt > (pc + kTileMin - 1) / kTileMin ? nt : (pc + kTileMin - 1) / kTileMin;
+        nt = nt > (nc + kTileMin - 1) / kTileMin ? nt : (nc + kTileMin - 1) / kTileMin;
+        const size_t nt_max = nt + 1;
+        const size_t counts = 256 * nt_max;
+        const size_t ts0 = (counts + kTileMin - 1) / kTileMin;
+        const size_t tsums = (ts0 > nt_max ? ts0 : nt_max) + 4;
+        size_t off = 0;
+        auto take = [&](size_t &field, size_t bytes) {
+            off = scr_align(off, 128);
+            field = off;
+            off += bytes;
+        };
+        take(L.ep_k2, nep * 4);
+        take(L.ep_v2, nep * 4);
+        take(L.counts, counts * 4);
+        take(L.tile_sums, tsums * 4);
+        take(L.cnt, nep * 4);
+        take(L.pr_a, pc * 4);
+        take(L.pr_b, pc * 4);
+        take(L.pk, pc * 4);
+        take(L.pv, pc * 4);
+        take(L.pk2, pc * 4);
+        take(L.pv2, pc * 4);
+        take(L.cflag, pc * 4);
+        take(L.cand, nc * sizeof(Cand));
+        take(L.cc, nc * cc_size);
+        take(L.color, nc * 4);
+        take(L.bmask, (size_t)nb * 8 + 8);
+        take(L.bprio, (size_t)nb * 8 + 8);
+        take(L.corder, nc * 4);
+        take(L.misc, kMiscWords * 4);
+        take(L.act, nc * 4);
+        take(L.alist, nc * 4);
+        L.stride = scr_align(off, 256);
+        return L;
+    }
+
+    // Phase-timer slots per world (Engine::prof): SM cycles summed over the
+    // steps since profiling was enabled, then the CTA and the globaltimer
+    // bounds (ns) of the world's last step.
+    enum : uint32_t
+    {
+        kPhBroadphase = 0,
+        kPhCandidates = 1,
+        kPhNarrow = 2,
+        kPhColor = 3,
+        kPhIntegrate = 4,
+        kPhContactPos = 5,
+        kPhJointPos = 6,
+        kPhVelUpdate = 7,
+        kPhVelSolve = 8,
+        kPhStats = 9,
+        kProfCta = 12,
+        kProfStartNs = 13,
+        kProfEndNs = 14,
+        kProfSlots = 16
+    };
 
     template <class T, class P>
     struct Engine
@@ -115,8 +198,7 @@ namespace rbps_gpu
         int solve_mode;
         int use_vel_exp;
         // executors
-        char *scratch;
-        ScratchLayout lay;
+        char *scratch;            // per-world slices at WorldDev::scr_off
         uint32_t *work_counter;
         const uint32_t *small_worlds;
         uint32_t n_small;
@@ -126,16 +208,34 @@ namespace rbps_gpu
         CandContacts<T, P> *dump_cc;
         uint32_t *dump_color;
         uint32_t dump_pair_cap, dump_cand_cap;
+        unsigned long long *prof; // phase timers, kProfSlots per world (null = off)
     };
 
     // Host entry points, instantiated per precision in engine_f64.cu /
     // engine_f32.cu.  They only enqueue work on `stream`.
+    // Phase kernels of the batched step (one launch per phase).
+    enum : int
+    {
+        kKFrame = 0,
+        kKNarrow = 1,
+        kKColor = 2,
+        kKPosition = 3,
+        kKVelocity = 4,
+        kKStats = 5,
+        kNumPhaseKernels = 6
+    };
+    struct PhaseLaunch
+    {
+        int grid[kNumPhaseKernels];
+        int block[kNumPhaseKernels];
+    };
+
     template <class T, class P>
-    cudaError_t launch_step_small(const Engine<T, P> &e, int grid, int block, cudaStream_t stream);
+    cudaError_t launch_step_phases(const Engine<T, P> &e, const PhaseLaunch &pl, cudaStream_t stream);
+    template <class T, class P>
+    cudaError_t occupancy_phase(int kernel, int block, int *blocks_per_sm);
     template <class T, class P>
     cudaError_t launch_step_big(const Engine<T, P> &e, uint32_t world, int grid, int block, cudaStream_t stream);
-    template <class T, class P>
-    cudaError_t occupancy_small(int block, int *blocks_per_sm);
     template <class T, class P>
     cudaError_t occupancy_big(int block, int *blocks_per_sm);
     template <class T, class P>

@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 def colour_valid(colors, ba, bb, dynamic):
     seen = {}
     for c, a, b in zip(colors, ba, bb):
-        if c == 64:      # serial overflow colour
+        if c >= 64:      # 64 = serial overflow colour, 65 = no contact rows this substep
             continue
         for x in (a, b):
             if dynamic[x]:
@@ -39,6 +39,11 @@ def test_colouring_is_valid(rbps, precision):
     assert len(col) > 0
     assert colour_valid(col, ba, bb, dyn)
     assert b.stats()["max_colors"] >= 2
+    # only candidates with contact rows are coloured; the rest are idle
+    assert set(np.unique(col).tolist()) <= set(range(66))
+    n_active = int((col < 65).sum())
+    assert 0 < n_active < len(col)
+    assert n_active <= len(b.contacts(0))  # every active candidate has >= 1 row
 
 
 def test_colored_fp32_one_step_close(rbps):
