@@ -136,34 +136,31 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference_run(scene, warmup, steps, max_seconds, threads):
+def cpu_reference_run(scene, preroll, warmup, steps, max_seconds, threads):
     """The reference engine (oracle/_ref, built from the reference's own
-    sources) on the host cores, one World per thread at a time: a prefix of
-    the scene's worlds sized so that `steps` steps take about max_seconds,
-    `warmup` untimed steps, then timed chunks of steps until at least
-    `steps` steps and max_seconds / 2 of wall clock have passed.  Returns
-    (body-substeps/s, description of the sample)."""
+    sources) on the host cores, one World per thread at a time, on a prefix
+    of the scene's worlds sized to about max_seconds: `preroll` + `warmup`
+    untimed steps, then timed chunks of steps until at least `steps` steps
+    and half of max_seconds have passed.  Returns (body-substeps/s,
+    description of the sample)."""
     from oracle import ref
     worlds = scene.worlds
-    # calibrate on a small prefix, then size the sample to the time budget
+    # calibrate on a small prefix (falling bodies); resting piles cost ~3x more
     probe = [ref.RefWorld(w, scene.timestep, scene.substeps) for w in worlds[:256]]
     t = ref.step_worlds(probe, 2, threads)
     dyn_probe = sum(w.n_dynamic for w in worlds[:256])
-    rate = dyn_probe * scene.substeps * 2 / max(t, 1e-9) / 3.0  # contacts make later steps ~3x costlier
-    budget_bs = rate * max_seconds
-    total_bs = 0
-    n = 0
+    rate = dyn_probe * scene.substeps * 2 / max(t, 1e-9)
+    per_dyn = scene.substeps * (2.0 * preroll + 3.0 * (warmup + 2 * steps)) / rate  # seconds per dynamic body
+    total_dyn, n = 0, 0
     for w in worlds:
-        need = w.n_dynamic * scene.substeps * steps
-        if n >= 64 and total_bs + need > budget_bs:
+        if n >= 64 and (total_dyn + w.n_dynamic) * per_dyn > max_seconds:
             break
-        total_bs += need
+        total_dyn += w.n_dynamic
         n += 1
     del probe
     sample = worlds[:n]
     refs = [ref.RefWorld(w, scene.timestep, scene.substeps) for w in sample]
-    if warmup:
-        ref.step_worlds(refs, warmup, threads)
+    t_pre = ref.step_worlds(refs, preroll + warmup, threads) if preroll + warmup else 0.0
     secs, done = 0.0, 0
     chunk = max(1, min(steps, 10))
     while done < steps or (secs < 0.5 * max_seconds and done < 20 * steps):
@@ -171,8 +168,8 @@ def cpu_reference_run(scene, warmup, steps, max_seconds, threads):
         done += chunk
     n_dyn = sum(w.n_dynamic for w in sample)
     value = n_dyn * scene.substeps * done / secs
-    info = (f"{n} of {len(worlds)} worlds ({n_dyn} dynamic bodies), {warmup} untimed + {done} timed steps, "
-            f"{secs:.2f} s on {threads} threads")
+    info = (f"{n} of {len(worlds)} worlds ({n_dyn} dynamic bodies), {preroll} pre-roll + {warmup} untimed steps "
+            f"({t_pre:.1f} s), then {done} timed steps in {secs:.2f} s on {threads} threads")
     return value, info
 
 
@@ -185,7 +182,9 @@ def main():
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=50)
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-seconds", type=float, default=30.0)
+    ap.add_argument("--preroll", type=int, default=240,
+                    help="untimed steps before the warm-up (240 = 2 s simulated: the bodies have landed)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--block", type=int, default=0)
     args = ap.parse_args()
@@ -201,12 +200,13 @@ def main():
             return
         scene = scenes.config3(seed=args.seed, n_worlds=args.worlds)
         budget = float(os.environ.get("RBPS_BENCH_REF_SECONDS", "150"))
-        value, info = cpu_reference_run(scene, args.warmup, args.steps, max_seconds=budget, threads=threads)
+        value, info = cpu_reference_run(scene, args.preroll, args.warmup, args.steps, max_seconds=budget,
+                                        threads=threads)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
                 "config": {"workload": WORKLOAD, "worlds": args.worlds, "substeps": 4, "dt": 1 / 120,
-                           "solver": "reference sequential Gauss-Seidel (CPU)"},
+                           "preroll_steps": args.preroll, "solver": "reference sequential Gauss-Seidel (CPU)"},
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                                  "sample": info},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -226,8 +226,11 @@ def main():
     scene = scenes.config3(seed=rank_seed(args.seed, rank), n_worlds=args.worlds)
     stream = torch.cuda.Stream()  # a real stream: the legacy NULL stream would not order our launches
     torch.cuda.set_stream(stream)
+    free0 = torch.cuda.mem_get_info(local)[0]
     batch = rbps_b200.Batch.from_scene(scene, abi.PRECISION_FP32, abi.SOLVE_COLORED, device=local,
                                        stream=stream.cuda_stream, block_threads=args.block)
+    torch.cuda.synchronize()
+    dev_bytes = int(free0 - torch.cuda.mem_get_info(local)[0])
     n_tot, n_dyn = batch.total_bodies()
     n_coll = sum(len(w.colliders) for w in scene.worlds)
     n_joints = sum(len(w.joints) for w in scene.worlds)
@@ -236,7 +239,9 @@ def main():
         if ws > 1:
             torch.distributed.barrier()
 
-    # warm-up (untimed)
+    # pre-roll to the resting regime, then warm-up (both untimed)
+    if args.preroll:
+        batch.step(args.preroll)
     batch.step(args.warmup)
     batch.synchronize()
 
@@ -271,12 +276,12 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = bmodel / (ms_step / 1e3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "step_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tr = json.load(f)
-        # DRAM bytes per launch from ncu on a smaller batch, scaled by dynamic bodies
-        traffic = tr["dram_bytes_per_launch"] * n_dyn / tr["dynamic_bodies"]
+        # DRAM bytes of one step (all its launches) from ncu on a smaller batch, scaled by dynamic bodies
+        traffic = tr["dram_bytes_per_step"] * n_dyn / tr["dynamic_bodies"]
 
     # end-to-end through the C ABI: forces in, poses out, pinned host buffers
     f_host = torch.empty((n_tot, 3), dtype=torch.float64, pin_memory=True)
@@ -299,7 +304,8 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
-            cv, info = cpu_reference_run(scene, args.warmup, min(args.steps, 40), args.cpu_seconds, threads)
+            cv, info = cpu_reference_run(scene, args.preroll, args.warmup, min(args.steps, 40), args.cpu_seconds,
+                                         threads)
             cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "reference", "sample": info}
         except Exception as e:  # the oracle library is missing
             cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": f"unavailable: {e}"}
@@ -311,17 +317,23 @@ def main():
                 "config": {"workload": WORKLOAD, "worlds_per_gpu": args.worlds, "bodies_per_gpu": n_tot,
                            "dynamic_bodies_per_gpu": n_dyn, "substeps": scene.substeps, "dt": scene.timestep,
                            "precision": "fp32", "solver": "graph-coloured Gauss-Seidel",
-                           "l2": "inputs larger than L2 (world state + per-CTA scratch >> 126 MB)",
+                           "preroll_steps": args.preroll,
+                           "timed_steps": f"{args.preroll + args.warmup + 1}..{args.preroll + args.warmup + args.steps}",
+                           "device_bytes": dev_bytes,
+                           "l2": f"inputs larger than L2: {dev_bytes / 1e6:.0f} MB of world state and scratch "
+                                 "touched every step (L2 126 MB)",
                            "parallelism": f"world-sharded replicas x{ws}", "seed": args.seed,
                            "state_finite": finite},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                             "algorithmic_bytes_per_launch": bmodel, "kernel": "k_step_small"},
+                             "algorithmic_bytes_per_step": bmodel,
+                             "kernel": f"one step = {st['kernel_launches'] // max(args.steps, 1)} phase-kernel launches"},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n_tot_all) * 24,
                         "d2h_bytes_per_step": int(n_tot_all) * 56, "steps": args.e2e_steps},
                 "clocks": clk,
                 "gpu_launches": int(st["kernel_launches"]),
+                "cuda_graph": bool(st["graph"]),
                 "stats_last_step": {"pairs": st["pairs"], "candidates": st["candidates"],
                                     "contacts": st["contacts"], "max_colors": st["max_colors"],
                                     "serial_overflow": st["serial_overflow"]}}

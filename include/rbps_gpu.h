@@ -181,7 +181,7 @@ typedef struct rbps_stats {
     uint32_t max_colors;       /* largest colour count of any world, last step   */
     uint32_t serial_overflow;  /* pairs that needed the serial fallback colour   */
     int32_t device_error;      /* last device error word (RBPS_ERR_* or 0)       */
-    uint32_t pad_;
+    uint32_t graph;            /* 1 when steps replay a captured CUDA graph      */
     uint64_t kernel_launches;  /* kernels launched by the last rbps_batch_step  */
 } rbps_stats;
 

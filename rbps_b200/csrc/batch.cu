@@ -155,6 +155,12 @@ struct rbps_batch
     std::vector<WorldDev> wdev;
     std::vector<uint32_t> small_ids, big_ids;
     PhaseLaunch phase{};      // grid / block of each phase kernel
+    FlatLaunch flat{};        // flat colored pipeline
+    bool use_flat = false;
+    uint32_t *wcoff = nullptr, *gcol = nullptr, *sbodies = nullptr, *sjoints = nullptr, *sjcoff = nullptr;
+    uint2 *nlist = nullptr;
+    void **wcand = nullptr, **wcc = nullptr;
+    uint32_t n_sbodies = 0, n_sjoints = 0, n_sjcolors = 0;
     int grid_big = 0;
     uint32_t n_counters = 0;  // phase work counters per step
     uint64_t total_bodies = 0, total_dynamic = 0;
@@ -197,10 +203,18 @@ struct rbps_batch
             CU(cudaMemcpy(*p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice));
         return RBPS_OK;
     }
+    // one step captured as a CUDA graph (replayed by rbps_batch_step)
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_key = -1;      // dump / profile state the graph was captured with
+    bool graph_ok = true;    // false once capture was refused: launch directly
+    uint64_t graph_launches = 0;
+
     ~rbps_batch()
     {
         if (stream)
             cudaStreamSynchronize(stream);
+        if (graph_exec)
+            cudaGraphExecDestroy(graph_exec);
         for (void *p : allocs)
             cudaFree(p);
         if (own_stream && stream)
@@ -481,6 +495,17 @@ namespace
         e.use_vel_exp = b->desc.use_velocity_expansion;
         e.work_counter = b->work_counter;
         e.scratch = b->scratch;
+        e.wcoff = b->wcoff;
+        e.gcol = b->gcol;
+        e.nlist = b->nlist;
+        e.wcand = (Cand *const *)b->wcand;
+        e.wcc = (CandContacts<T, P> *const *)b->wcc;
+        e.sbodies = b->sbodies;
+        e.n_sbodies = b->n_sbodies;
+        e.sjoints = b->sjoints;
+        e.sjcoff = b->sjcoff;
+        e.n_sjcolors = b->n_sjcolors;
+        e.n_sjoints = b->n_sjoints;
         e.small_worlds = b->small_list;
         e.n_small = (uint32_t)b->small_ids.size();
         e.dump_pairs = b->dump ? b->dump_pairs : nullptr;
@@ -510,6 +535,7 @@ namespace
     }
 
     constexpr uint32_t kSmallWorldBodies = 4096;
+    constexpr int kMaxBlockHost = 256; // block of the flat kernels (their __launch_bounds__)
 } // namespace
 
 template <class T, class P>
@@ -921,6 +947,57 @@ static int commit_typed(rbps_batch *b)
         b->grid_big = per_sm * b->sm_count;
     }
     b->n_counters = 2 + 4 * (uint32_t)b->desc.substeps;
+    // ---- flat colored pipeline over the small worlds
+    if (!b->small_ids.empty() && b->desc.solve_mode == RBPS_SOLVE_COLORED)
+    {
+        const uint32_t ns = (uint32_t)b->small_ids.size();
+        size_t cand_cap = 0;
+        std::vector<void *> wcand(W, nullptr), wcc(W, nullptr);
+        std::vector<uint32_t> sbodies;
+        uint32_t max_jc = 0;
+        for (uint32_t w : b->small_ids)
+        {
+            const WorldDev &d = b->wdev[w];
+            const ScratchLayout L = make_layout(d.n_bp, d.n_bodies, d.pair_cap, d.n_pc, ccs);
+            wcand[w] = b->scratch + d.scr_off + L.cand;
+            wcc[w] = b->scratch + d.scr_off + L.cc;
+            cand_cap += (size_t)d.pair_cap + 1 + d.n_pc;
+            for (uint32_t k = 0; k < d.n_bodies; ++k)
+                sbodies.push_back(d.body_off + k);
+            max_jc = std::max(max_jc, d.n_jcolors);
+        }
+        std::vector<uint32_t> sjoints, sjcoff(1, 0);
+        for (uint32_t jc = 0; jc < max_jc; ++jc)
+        {
+            for (uint32_t w : b->small_ids)
+            {
+                const WorldDev &d = b->wdev[w];
+                if (jc >= d.n_jcolors)
+                    continue;
+                for (uint32_t k = joffs[w][jc]; k < joffs[w][jc + 1]; ++k)
+                    sjoints.push_back(d.joint_off + jorders[w][k]);
+            }
+            sjcoff.push_back((uint32_t)sjoints.size());
+        }
+        b->n_sbodies = (uint32_t)sbodies.size();
+        b->n_sjoints = (uint32_t)sjoints.size();
+        b->n_sjcolors = max_jc;
+        if ((rc = b->alloc((void **)&b->wcoff, 4 * ((size_t)ns + 1))) ||
+            (rc = b->alloc((void **)&b->gcol, 4 * (size_t)kGcolWords)) ||
+            (rc = b->alloc((void **)&b->nlist, sizeof(uint2) * std::max<size_t>(cand_cap, 1))) ||
+            (rc = b->upload(&b->wcand, wcand)) || (rc = b->upload(&b->wcc, wcc)) ||
+            (rc = b->upload(&b->sbodies, sbodies)) || (rc = b->upload(&b->sjoints, sjoints)) ||
+            (rc = b->upload(&b->sjcoff, sjcoff)))
+            return rc;
+        CU(cudaMemset(b->gcol, 0, 4 * (size_t)kGcolWords));
+        int per_sm = 0;
+        CU(occupancy_flat<T, P>(0, kMaxBlockHost, &per_sm));
+        b->flat.grid_narrow = std::max(1, per_sm) * b->sm_count;
+        b->flat.block_solve = 128; // 4 worlds per CTA
+        const int warps_per_cta = b->flat.block_solve / 32;
+        b->flat.grid_solve = (int)((ns + warps_per_cta - 1) / warps_per_cta);
+        b->use_flat = true;
+    }
     if ((rc = b->alloc((void **)&b->work_counter, std::max<size_t>(64, 4 * (size_t)b->n_counters))) || (rc = b->alloc((void **)&b->error_d, 64)) ||
         (rc = b->alloc((void **)&b->stats_d, sizeof(WorldStats) * W)))
         return rc;
@@ -997,23 +1074,92 @@ extern "C" int rbps_batch_set_dump(rbps_batch *b, int32_t enable)
 }
 
 // ------------------------------------------------------------ stepping
+// The launches of one step on b->stream; returns the kernel count, or a
+// negative status.
+template <class T, class P>
+static long enqueue_step(rbps_batch *b, const Engine<T, P> &e)
+{
+    long launches = 0;
+    if (!b->small_ids.empty())
+    {
+        if (cudaMemsetAsync(b->work_counter, 0, 4 * (size_t)b->n_counters, b->stream) != cudaSuccess)
+            return RBPS_ERR_CUDA;
+        if (b->use_flat)
+        {
+            if (launch_step_flat<T, P>(e, b->phase, b->flat, b->stream) != cudaSuccess)
+                return RBPS_ERR_CUDA;
+            launches += 3 + 6 * (long)b->desc.substeps;
+        }
+        else
+        {
+            if (launch_step_phases<T, P>(e, b->phase, b->stream) != cudaSuccess)
+                return RBPS_ERR_CUDA;
+            launches += b->n_counters;
+        }
+    }
+    for (uint32_t w : b->big_ids)
+    {
+        if (launch_step_big<T, P>(e, w, b->grid_big, b->block, b->stream) != cudaSuccess)
+            return RBPS_ERR_CUDA;
+        ++launches;
+    }
+    return launches;
+}
+
+// Captures one step into b->graph_exec; on any refusal the batch falls back
+// to direct launches for good.
+template <class T, class P>
+static void capture_step(rbps_batch *b, const Engine<T, P> &e, int key)
+{
+    if (b->graph_exec)
+    {
+        cudaGraphExecDestroy(b->graph_exec);
+        b->graph_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    {
+        cudaGetLastError();
+        b->graph_ok = false;
+        return;
+    }
+    const long n = enqueue_step<T, P>(b, e);
+    const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
+    cudaGraphExec_t x = nullptr;
+    if (n < 0 || ec != cudaSuccess || !g || cudaGraphInstantiate(&x, g, 0) != cudaSuccess)
+    {
+        cudaGetLastError();
+        b->graph_ok = false;
+        x = nullptr;
+    }
+    if (g)
+        cudaGraphDestroy(g);
+    b->graph_exec = x;
+    b->graph_key = key;
+    b->graph_launches = n > 0 ? (uint64_t)n : 0;
+}
+
 template <class T, class P>
 static int step_typed(rbps_batch *b, int n)
 {
     Engine<T, P> e = make_engine<T, P>(b);
+    const int key = (b->dump ? 1 : 0) | (e.prof ? 2 : 0);
+    if (b->graph_ok && n > 0 && (!b->graph_exec || b->graph_key != key))
+        capture_step<T, P>(b, e, key);
     uint64_t launches = 0;
     for (int s = 0; s < n; ++s)
     {
-        if (!b->small_ids.empty())
+        if (b->graph_exec)
         {
-            CU(cudaMemsetAsync(b->work_counter, 0, 4 * (size_t)b->n_counters, b->stream));
-            CU(launch_step_phases<T, P>(e, b->phase, b->stream));
-            launches += b->n_counters;
+            CU(cudaGraphLaunch(b->graph_exec, b->stream));
+            launches += b->graph_launches;
         }
-        for (uint32_t w : b->big_ids)
+        else
         {
-            CU(launch_step_big<T, P>(e, w, b->grid_big, b->block, b->stream));
-            ++launches;
+            const long k = enqueue_step<T, P>(b, e);
+            if (k < 0)
+                return fail(RBPS_ERR_CUDA, "step launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            launches += (uint64_t)k;
         }
     }
     b->launches_last = launches;
@@ -1355,6 +1501,7 @@ extern "C" int rbps_batch_get_stats(rbps_batch *b, rbps_stats *s)
         s->serial_overflow += x.n_serial;
     }
     s->kernel_launches = b->launches_last;
+    s->graph = b->graph_exec ? 1u : 0u;
     return RBPS_OK;
 }
 

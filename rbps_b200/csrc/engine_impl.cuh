@@ -495,10 +495,10 @@ namespace rbps_gpu
         }
     }
 
-    // All contact rows of one candidate, in list order, with both bodies in
-    // registers (load once, relax, store once).
+    // All contact rows of one candidate pair (global bodies ba, bb), in list
+    // order, with both bodies in registers (load once, relax, store once).
     template <class T, class P>
-    __device__ __forceinline__ void solve_cand_position(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+    __device__ __forceinline__ void solve_pair_position(const Engine<T, P> &E, uint32_t ba, uint32_t bb,
                                                         CandContacts<T, P> &cc)
     {
         const int n = cc.n;
@@ -506,7 +506,6 @@ namespace rbps_gpu
             return;
         const vec3<T> nrm = v3(cc.normal);
         const T sf = cc.mat.y;
-        const uint32_t ba = W.body_off + cd.ba, bb = W.body_off + cd.bb;
         BodyR<T, P> A, Bb;
         load_body(E.B, ba, A, true);
         load_body(E.B, bb, Bb, true);
@@ -517,14 +516,13 @@ namespace rbps_gpu
     }
 
     template <class T, class P>
-    __device__ __forceinline__ void solve_cand_velocity(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+    __device__ __forceinline__ void solve_pair_velocity(const Engine<T, P> &E, uint32_t ba, uint32_t bb,
                                                         const CandContacts<T, P> &cc)
     {
         const int n = cc.n;
         if (n == 0)
             return;
         const vec3<T> nrm = v3(cc.normal);
-        const uint32_t ba = W.body_off + cd.ba, bb = W.body_off + cd.bb;
         BodyR<T, P> A, Bb;
         load_body(E.B, ba, A, false);
         load_body(E.B, bb, Bb, false);
@@ -532,6 +530,20 @@ namespace rbps_gpu
             contact_velocity(A, Bb, nrm, cc.mat.x, cc.mat.z, cc.pt[k], E.h);
         store_vel(E.B, ba, A);
         store_vel(E.B, bb, Bb);
+    }
+
+    template <class T, class P>
+    __device__ __forceinline__ void solve_cand_position(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+                                                        CandContacts<T, P> &cc)
+    {
+        solve_pair_position(E, W.body_off + cd.ba, W.body_off + cd.bb, cc);
+    }
+
+    template <class T, class P>
+    __device__ __forceinline__ void solve_cand_velocity(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+                                                        const CandContacts<T, P> &cc)
+    {
+        solve_pair_velocity(E, W.body_off + cd.ba, W.body_off + cd.bb, cc);
     }
 
     template <class T, class P>
@@ -957,6 +969,332 @@ namespace rbps_gpu
         return cudaGetLastError();
     }
 
+    // ------------------------------------------------- batched colored pipeline
+    // Colored mode over the small worlds, per step:
+    //   k_phase_frame    one CTA per world: SAP update / sort / sweep, candidates
+    //   k_flat_prefix    candidate prefix over the worlds
+    //   k_type_count / k_type_scan / k_type_scatter
+    //                    the candidates of all worlds sorted by shape pair, so a
+    //                    warp of the narrowphase runs one pair routine
+    // and per substep:
+    //   k_flat_narrow    one thread per candidate, in shape-pair order
+    //   k_substep_warp   one warp per world: colouring of the contacting
+    //                    candidates, integrate, position solve (colour by colour,
+    //                    joint errors, joint colours), velocity update,
+    //                    velocity solve -- worlds progress independently, a
+    //                    barrier is a __syncwarp
+    // and last k_phase_stats.
+
+    // Candidate prefix over the small worlds (one CTA).
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_flat_prefix(const Engine<T, P> E)
+    {
+        __shared__ BlockShared sh;
+        uint32_t carry = 0;
+        for (uint32_t base = 0; base < E.n_small; base += blockDim.x)
+        {
+            const uint32_t q = base + threadIdx.x;
+            uint32_t v = 0;
+            if (q < E.n_small)
+            {
+                const WorldDev W = E.worlds[E.small_worlds[q]];
+                v = world_scratch(E, W).misc[kMiscNCand];
+            }
+            uint32_t tot;
+            const uint32_t ex = block_excl_scan(v, sh, &tot);
+            if (q < E.n_small)
+                E.wcoff[q] = carry + ex;
+            carry += tot;
+        }
+        if (threadIdx.x == 0)
+            E.wcoff[E.n_small] = carry;
+    }
+
+    // Shape-pair class of a candidate: index of (kind a, kind b) over the
+    // five shape kinds, 25 classes.
+    __device__ __forceinline__ uint32_t kind_index(int kind)
+    {
+        return kind == kSphere ? 0u : kind == kBox ? 1u : kind == kCapsule ? 2u : kind == kPlane ? 3u : 4u;
+    }
+
+    // The small world holding flat candidate f: last q with wcoff[q] <= f.
+    template <class T, class P>
+    __device__ __forceinline__ uint32_t world_of_flat(const Engine<T, P> &E, uint32_t f)
+    {
+        uint32_t lo = 0, hi = E.n_small;
+        while (hi - lo > 1)
+        {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (E.wcoff[mid] <= f)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        return lo;
+    }
+
+    template <class T, class P>
+    __device__ __forceinline__ uint32_t cand_class(const Engine<T, P> &E, const WorldDev &W, const Cand &cd)
+    {
+        return kind_index(E.shape[W.coll_off + cd.ca].kind) * 5u + kind_index(E.shape[W.coll_off + cd.cb].kind);
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_type_count(const Engine<T, P> E)
+    {
+        __shared__ uint32_t cnt[kPairClasses];
+        for (uint32_t k = threadIdx.x; k < kPairClasses; k += blockDim.x)
+            cnt[k] = 0;
+        __syncthreads();
+        const uint32_t total = E.wcoff[E.n_small];
+        for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x)
+        {
+            const uint32_t q = world_of_flat(E, f);
+            const uint32_t w = E.small_worlds[q];
+            const WorldDev W = E.worlds[w];
+            atomicAdd(&cnt[cand_class(E, W, E.wcand[w][f - E.wcoff[q]])], 1u);
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < kPairClasses; k += blockDim.x)
+            if (cnt[k])
+                atomicAdd(&E.gcol[kGcolCount + k], cnt[k]);
+    }
+
+    // Class offsets; zeroes the counts for the next step and the cursors.
+    template <class T, class P>
+    __global__ void k_type_scan(const Engine<T, P> E)
+    {
+        if (threadIdx.x != 0)
+            return;
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < kPairClasses; ++k)
+        {
+            const uint32_t n = E.gcol[kGcolCount + k];
+            E.gcol[kGcolOff + k] = run;
+            E.gcol[kGcolFill + k] = 0u;
+            E.gcol[kGcolCount + k] = 0u;
+            run += n;
+        }
+        E.gcol[kGcolOff + kPairClasses] = run;
+    }
+
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_type_scatter(const Engine<T, P> E)
+    {
+        const uint32_t total = E.wcoff[E.n_small];
+        for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x)
+        {
+            const uint32_t q = world_of_flat(E, f);
+            const uint32_t w = E.small_worlds[q];
+            const WorldDev W = E.worlds[w];
+            const uint32_t c = f - E.wcoff[q];
+            const uint32_t k = cand_class(E, W, E.wcand[w][c]);
+            const uint32_t slot = E.gcol[kGcolOff + k] + atomicAdd(&E.gcol[kGcolFill + k], 1u);
+            E.nlist[slot] = make_uint2(w, c);
+        }
+    }
+
+    // Narrowphase of every candidate of the small worlds, in class order.
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow(const Engine<T, P> E)
+    {
+        const uint32_t total = E.gcol[kGcolOff + kPairClasses];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+        {
+            const uint2 e = E.nlist[i];
+            const WorldDev W = E.worlds[e.x];
+            uint32_t n_gjk = 0;
+            narrow_candidate(E, W, E.wcand[e.x][e.y], E.wcc[e.x][e.y], n_gjk);
+            if (n_gjk)
+                atomicAdd(world_scratch(E, W).misc + kMiscNGjk, n_gjk);
+        }
+    }
+
+    // Jones-Plassmann colouring of one world's contacting candidates by one
+    // warp (same rule as color_active) and its colour buckets (corder /
+    // colour offsets in misc).
+    template <class T, class P>
+    __device__ void warp_color_world(const Engine<T, P> &E, uint32_t w)
+    {
+        const uint32_t lane = lane_id();
+        const uint32_t full = 0xffffffffu;
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = world_scratch(E, W);
+        uint32_t *misc = S.misc;
+        const uint32_t n_cand = misc[kMiscNCand];
+        for (uint32_t b = lane; b < W.n_bodies; b += 32)
+        {
+            S.bmask[b] = 0ull;
+            S.bprio[b] = 0ull;
+        }
+        for (uint32_t k = lane; k < 66; k += 32)
+            misc[kMiscCCount + k] = 0u;
+        // compact the contacting candidates into alist
+        uint32_t n_act = 0;
+        const uint32_t lt = (1u << lane) - 1u;
+        for (uint32_t base = 0; base < n_cand; base += 32)
+        {
+            const uint32_t c = base + lane;
+            const bool live = c < n_cand;
+            const bool act = live && S.cc[c].n > 0;
+            const uint32_t m = __ballot_sync(full, act);
+            if (act)
+            {
+                S.alist[n_act + __popc(m & lt)] = c;
+                S.color[c] = 0xffffffffu;
+            }
+            else if (live)
+                S.color[c] = kColorIdle;
+            n_act += __popc(m);
+        }
+        __syncwarp();
+        const uint8_t *type = E.B.type + W.body_off;
+        uint32_t round = 1;
+        for (; round <= kMaxColorRounds && n_act; ++round)
+        {
+            for (uint32_t q = lane; q < n_act; q += 32)
+            {
+                const uint32_t c = S.alist[q];
+                if (S.color[c] != 0xffffffffu)
+                    continue;
+                const Cand cd = S.cand[c];
+                const unsigned long long val = ((unsigned long long)round << 56) |
+                                               ((unsigned long long)(hash32(c) & 0xffffffu) << 32) | c;
+                if (type[cd.ba] == kDynamic)
+                    atomicMax(&S.bprio[cd.ba], val);
+                if (type[cd.bb] == kDynamic)
+                    atomicMax(&S.bprio[cd.bb], val);
+            }
+            __syncwarp();
+            uint32_t left = 0;
+            for (uint32_t q = lane; q < n_act; q += 32)
+            {
+                const uint32_t c = S.alist[q];
+                if (S.color[c] != 0xffffffffu)
+                    continue;
+                const Cand cd = S.cand[c];
+                const unsigned long long val = ((unsigned long long)round << 56) |
+                                               ((unsigned long long)(hash32(c) & 0xffffffu) << 32) | c;
+                const bool da = type[cd.ba] == kDynamic, db = type[cd.bb] == kDynamic;
+                const bool won = (!da || S.bprio[cd.ba] == val) && (!db || S.bprio[cd.bb] == val);
+                if (!won)
+                {
+                    ++left;
+                    continue;
+                }
+                const unsigned long long used = (da ? S.bmask[cd.ba] : 0ull) | (db ? S.bmask[cd.bb] : 0ull);
+                uint32_t col;
+                if (used == ~0ull)
+                    col = kColorSerial;
+                else
+                {
+                    col = (uint32_t)(__ffsll((long long)~used) - 1);
+                    const unsigned long long bit = 1ull << col;
+                    if (da)
+                        S.bmask[cd.ba] |= bit;
+                    if (db)
+                        S.bmask[cd.bb] |= bit;
+                }
+                S.color[c] = col;
+            }
+            left = __reduce_add_sync(full, left);
+            __syncwarp();
+            if (left == 0)
+                break;
+        }
+        if (round > kMaxColorRounds)
+        {
+            for (uint32_t q = lane; q < n_act; q += 32)
+                if (S.color[S.alist[q]] == 0xffffffffu)
+                    S.color[S.alist[q]] = kColorSerial;
+            __syncwarp();
+        }
+        for (uint32_t q = lane; q < n_act; q += 32)
+            atomicAdd(&misc[kMiscCCount + S.color[S.alist[q]]], 1u);
+        __syncwarp();
+        if (lane == 0)
+        {
+            uint32_t run = 0, ncol = 0;
+            for (uint32_t k = 0; k <= kColorSerial; ++k)
+            {
+                const uint32_t n = misc[kMiscCCount + k];
+                misc[kMiscCOff + k] = run;
+                misc[kMiscCCount + k] = run; // becomes the fill cursor
+                if (n && k < kColorSerial)
+                    ncol = k + 1;
+                run += n;
+            }
+            misc[kMiscCOff + kColorSerial + 1] = run;
+            misc[kMiscNColors] = ncol;
+            if (ncol > misc[kMiscMaxColors])
+                misc[kMiscMaxColors] = ncol;
+        }
+        __syncwarp();
+        for (uint32_t q = lane; q < n_act; q += 32)
+        {
+            const uint32_t c = S.alist[q];
+            const uint32_t slot = atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
+            S.corder[slot] = c;
+        }
+        __syncwarp();
+    }
+
+    // The rest of a substep for one world per warp: colouring, integrate
+    // (Body.cpp:18-39), position solve + velocity update, velocity solve.
+#ifndef RBPS_SUBSTEP_MIN_BLOCKS
+#define RBPS_SUBSTEP_MIN_BLOCKS 3 // resident 128-thread CTAs (4 worlds each) per SM the registers must allow
+#endif
+    template <class T, class P>
+    __global__ void __launch_bounds__(128, RBPS_SUBSTEP_MIN_BLOCKS) k_substep_warp(const Engine<T, P> E)
+    {
+        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+        WarpTeam tm;
+        for (uint32_t q = warp; q < E.n_small; q += n_warps)
+        {
+            const uint32_t w = E.small_worlds[q];
+            {
+                PhaseClock clk(prof_slots(E, tm, w), false);
+                warp_color_world(E, w);
+                clk.mark(kPhColor);
+                const WorldDev W = E.worlds[w];
+                for (uint32_t b = tm.rank(); b < W.n_bodies; b += 32)
+                    integrate_body(E.B, W.body_off + b, E.h);
+                __syncwarp();
+                clk.mark(kPhIntegrate);
+            }
+            phase_position(E, tm, w);
+            phase_velocity(E, tm, w);
+        }
+    }
+
+    template <class T, class P>
+    cudaError_t launch_step_flat(const Engine<T, P> &e, const PhaseLaunch &pl, const FlatLaunch &fl,
+                                 cudaStream_t stream)
+    {
+        k_phase_frame<T, P><<<pl.grid[kKFrame], pl.block[kKFrame], 0, stream>>>(e, 0);
+        k_flat_prefix<T, P><<<1, kMaxBlock, 0, stream>>>(e);
+        k_type_count<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+        k_type_scan<T, P><<<1, 32, 0, stream>>>(e);
+        k_type_scatter<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+        for (int s = 0; s < e.substeps; ++s)
+        {
+            k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+            k_substep_warp<T, P><<<fl.grid_solve, fl.block_solve, 0, stream>>>(e);
+        }
+        k_phase_stats<T, P><<<pl.grid[kKStats], pl.block[kKStats], 0, stream>>>(e, 1);
+        return cudaGetLastError();
+    }
+
+    // kernel 0: narrowphase, 1: substep (warp per world)
+    template <class T, class P>
+    cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm)
+    {
+        if (kernel == 0)
+            return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_flat_narrow<T, P>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_substep_warp<T, P>, block, 0);
+    }
+
     template <class T, class P>
     cudaError_t launch_step_big(const Engine<T, P> &e, uint32_t world, int grid, int block, cudaStream_t stream)
     {
@@ -994,6 +1332,10 @@ namespace rbps_gpu
     template cudaError_t rbps_gpu::launch_step_big<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int, int,        \
                                                          cudaStream_t);                                           \
     template cudaError_t rbps_gpu::occupancy_phase<T, P>(int, int, int *);                                         \
+    template cudaError_t rbps_gpu::launch_step_flat<T, P>(const rbps_gpu::Engine<T, P> &,                          \
+                                                          const rbps_gpu::PhaseLaunch &,                            \
+                                                          const rbps_gpu::FlatLaunch &, cudaStream_t);              \
+    template cudaError_t rbps_gpu::occupancy_flat<T, P>(int, int, int *);                                          \
     template cudaError_t rbps_gpu::occupancy_big<T, P>(int, int *);                                               \
     template cudaError_t rbps_gpu::launch_collide<T, P>(const rbps_gpu::ShapeDev *, const double *,               \
                                                        const rbps_gpu::ShapeDev *, const double *,               \

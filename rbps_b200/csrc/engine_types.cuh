@@ -209,7 +209,23 @@ namespace rbps_gpu
         uint32_t *dump_color;
         uint32_t dump_pair_cap, dump_cand_cap;
         unsigned long long *prof; // phase timers, kProfSlots per world (null = off)
+        // flat colored pipeline over all small worlds (see engine_impl.cuh)
+        uint32_t *wcoff;               // n_small + 1: candidate prefix over small_worlds
+        uint32_t *gcol;                // global colour bookkeeping, kGcolWords
+        uint2 *nlist;                  // (world, candidate) of all small worlds sorted by shape pair
+        Cand *const *wcand;            // per world: its candidate list
+        CandContacts<T, P> *const *wcc; // per world: its contact manifolds
+        const uint32_t *sbodies;       // bodies of the small worlds
+        uint32_t n_sbodies;
+        const uint32_t *sjoints;       // joints of the small worlds grouped by joint colour
+        const uint32_t *sjcoff;        // n_sjcolors + 1 offsets into sjoints
+        uint32_t n_sjcolors, n_sjoints;
     };
+
+    // gcol layout (u32 words): per shape-pair class [0, 32) counts, [32, 64)
+    // fill cursors, [64, 96) offsets (entry kPairClasses = total)
+    constexpr uint32_t kPairClasses = 25;
+    constexpr uint32_t kGcolCount = 0, kGcolFill = 32, kGcolOff = 64, kGcolWords = 96;
 
     // Host entry points, instantiated per precision in engine_f64.cu /
     // engine_f32.cu.  They only enqueue work on `stream`.
@@ -232,6 +248,17 @@ namespace rbps_gpu
 
     template <class T, class P>
     cudaError_t launch_step_phases(const Engine<T, P> &e, const PhaseLaunch &pl, cudaStream_t stream);
+    // Colored mode: the frame / stats phases per world, the substeps flat
+    // over all small worlds (grids: narrowphase, cooperative solves).
+    struct FlatLaunch
+    {
+        int grid_narrow, grid_solve, block_solve;
+    };
+    template <class T, class P>
+    cudaError_t launch_step_flat(const Engine<T, P> &e, const PhaseLaunch &pl, const FlatLaunch &fl,
+                                 cudaStream_t stream);
+    template <class T, class P>
+    cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm);
     template <class T, class P>
     cudaError_t occupancy_phase(int kernel, int block, int *blocks_per_sm);
     template <class T, class P>

@@ -15,6 +15,16 @@
 #pragma once
 #include "math.cuh"
 
+// How the per-row contact relaxation routines are compiled: inline by
+// default, so the two bodies a pair relaxes stay in registers across its
+// rows; -DRBPS_SOLVER_OUTLINE makes them separate functions (smaller kernel
+// code, bodies passed through the stack).
+#ifdef RBPS_SOLVER_OUTLINE
+#define RBPS_SOLVER_CALL __noinline__
+#else
+#define RBPS_SOLVER_CALL __forceinline__
+#endif
+
 namespace rbps_gpu
 {
     template <class T> struct alignas(4 * sizeof(T)) V4
@@ -262,7 +272,7 @@ namespace rbps_gpu
     // apply_constraint_position_level + solve_normal_constraint +
     // solve_tangent_constraint (Contact.cpp:35-195) for one contact row.
     template <class T, class P>
-    __device__ __noinline__ void contact_position(BodyR<T, P> &A, BodyR<T, P> &Bb, const vec3<T> &n, T static_friction,
+    __device__ RBPS_SOLVER_CALL void contact_position(BodyR<T, P> &A, BodyR<T, P> &Bb, const vec3<T> &n, T static_friction,
                                      ContactPt<T, P> &c, T inv_h)
     {
         const vec3<T> ra_l = v3(c.ra), rb_l = v3(c.rb);
@@ -337,7 +347,7 @@ namespace rbps_gpu
 
     // apply_constraint_velocity_level (Contact.cpp:206-289) for one row.
     template <class T, class P>
-    __device__ __noinline__ void contact_velocity(BodyR<T, P> &A, BodyR<T, P> &Bb, const vec3<T> &n, T restitution,
+    __device__ RBPS_SOLVER_CALL void contact_velocity(BodyR<T, P> &A, BodyR<T, P> &Bb, const vec3<T> &n, T restitution,
                                      T dynamic_friction, const ContactPt<T, P> &c, T h)
     {
         if (!c.coll)

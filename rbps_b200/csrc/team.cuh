@@ -40,6 +40,18 @@ namespace rbps_gpu
         __device__ __forceinline__ void sync() const { cg::this_grid().sync(); }
     };
 
+    // One warp of a CTA as a team (barrier = __syncwarp); the phases that
+    // need only flat loops and barriers run unchanged on it.
+    struct WarpTeam
+    {
+        __device__ __forceinline__ uint32_t cta() const { return 0; }
+        __device__ __forceinline__ uint32_t ncta() const { return 1; }
+        __device__ __forceinline__ uint32_t rank() const { return threadIdx.x & 31u; }
+        __device__ __forceinline__ uint32_t size() const { return 32; }
+        __device__ __forceinline__ bool leader() const { return (threadIdx.x & 31u) == 0; }
+        __device__ __forceinline__ void sync() const { __syncwarp(); }
+    };
+
     constexpr int kMaxWarps = 32;
 
     // Shared scratch of the block primitives (one per CTA).
