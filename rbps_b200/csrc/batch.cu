@@ -160,7 +160,7 @@ struct rbps_batch
     uint32_t *wcoff = nullptr, *gcol = nullptr, *sbodies = nullptr, *sjoints = nullptr, *sjcoff = nullptr;
     uint2 *nlist = nullptr;
     void **wcand = nullptr, **wcc = nullptr;
-    uint32_t n_sbodies = 0, n_sjoints = 0, n_sjcolors = 0;
+    uint32_t n_sbodies = 0, n_sjoints = 0, n_sjcolors = 0, n_block_worlds = 0, mask_words = 0;
     int grid_big = 0;
     uint32_t n_counters = 0;  // phase work counters per step
     uint64_t total_bodies = 0, total_dynamic = 0;
@@ -508,6 +508,8 @@ namespace
         e.n_sjoints = b->n_sjoints;
         e.small_worlds = b->small_list;
         e.n_small = (uint32_t)b->small_ids.size();
+        e.n_block_worlds = b->n_block_worlds;
+        e.mask_words = b->mask_words;
         e.dump_pairs = b->dump ? b->dump_pairs : nullptr;
         e.dump_cand = b->dump ? b->dump_cand : nullptr;
         e.dump_cc = b->dump ? (CandContacts<T, P> *)b->dump_cc : nullptr;
@@ -536,6 +538,8 @@ namespace
 
     constexpr uint32_t kSmallWorldBodies = 4096;
     constexpr int kMaxBlockHost = 256; // block of the flat kernels (their __launch_bounds__)
+    constexpr uint32_t kBlockTeamBodies = 160; // colored batches: worlds this large step on a whole CTA
+    constexpr uint32_t kMaskWordsMax = 2048;    // shared colour-mask words per substep CTA (16 KB)
 } // namespace
 
 template <class T, class P>
@@ -991,11 +995,22 @@ static int commit_typed(rbps_batch *b)
             return rc;
         CU(cudaMemset(b->gcol, 0, 4 * (size_t)kGcolWords));
         int per_sm = 0;
-        CU(occupancy_flat<T, P>(0, kMaxBlockHost, &per_sm));
+        CU(occupancy_flat<T, P>(0, kMaxBlockHost, &per_sm, 0));
         b->flat.grid_narrow = std::max(1, per_sm) * b->sm_count;
-        b->flat.block_solve = 128; // 4 worlds per CTA
-        const int warps_per_cta = b->flat.block_solve / 32;
-        b->flat.grid_solve = (int)((ns + warps_per_cta - 1) / warps_per_cta);
+        b->flat.block_solve = 128;
+        // worlds of kBlockTeamBodies bodies or more step on a whole CTA, the
+        // rest on one warp each (small_ids is sorted by body count)
+        uint32_t nbw = 0;
+        while (nbw < ns && b->wdev[b->small_ids[nbw]].n_bodies >= kBlockTeamBodies)
+            ++nbw;
+        b->n_block_worlds = nbw;
+        b->flat.grid_solve = (int)(nbw + (ns - nbw + 3) / 4);
+        // shared colour masks: the largest CTA world, or four warp worlds
+        // (larger worlds fall back to their global mask array)
+        uint32_t words = 4 * kBlockTeamBodies;
+        if (nbw)
+            words = std::max(words, std::min<uint32_t>(b->wdev[b->small_ids[0]].n_bodies, kMaskWordsMax));
+        b->mask_words = words;
         b->use_flat = true;
     }
     if ((rc = b->alloc((void **)&b->work_counter, std::max<size_t>(64, 4 * (size_t)b->n_counters))) || (rc = b->alloc((void **)&b->error_d, 64)) ||

@@ -978,11 +978,11 @@ namespace rbps_gpu
     //                    warp of the narrowphase runs one pair routine
     // and per substep:
     //   k_flat_narrow    one thread per candidate, in shape-pair order
-    //   k_substep_warp   one warp per world: colouring of the contacting
-    //                    candidates, integrate, position solve (colour by colour,
-    //                    joint errors, joint colours), velocity update,
-    //                    velocity solve -- worlds progress independently, a
-    //                    barrier is a __syncwarp
+    //   k_substep        one CTA per large world, one warp per other world:
+    //                    greedy colouring of the contacting candidates, integrate,
+    //                    position solve (colour by colour, joint errors, joint
+    //                    colours), velocity update, velocity solve -- worlds
+    //                    progress independently on their own team barriers
     // and last k_phase_stats.
 
     // Candidate prefix over the small worlds (one CTA).
@@ -1078,19 +1078,40 @@ namespace rbps_gpu
         E.gcol[kGcolOff + kPairClasses] = run;
     }
 
+    // Each CTA takes a contiguous chunk of flat candidates, counts its
+    // classes in shared memory, reserves its ranges with one global atomic
+    // per class, then places its candidates.
     template <class T, class P>
     __global__ void __launch_bounds__(kMaxBlock) k_type_scatter(const Engine<T, P> E)
     {
+        __shared__ uint32_t cnt[kPairClasses], base[kPairClasses];
         const uint32_t total = E.wcoff[E.n_small];
-        for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x)
+        const uint32_t chunk = (total + gridDim.x - 1) / gridDim.x;
+        const uint32_t f0 = blockIdx.x * chunk;
+        const uint32_t f1 = min(total, f0 + chunk);
+        for (uint32_t k = threadIdx.x; k < kPairClasses; k += blockDim.x)
+            cnt[k] = 0;
+        __syncthreads();
+        for (uint32_t f = f0 + threadIdx.x; f < f1; f += blockDim.x)
         {
             const uint32_t q = world_of_flat(E, f);
             const uint32_t w = E.small_worlds[q];
-            const WorldDev W = E.worlds[w];
+            atomicAdd(&cnt[cand_class(E, E.worlds[w], E.wcand[w][f - E.wcoff[q]])], 1u);
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < kPairClasses; k += blockDim.x)
+        {
+            base[k] = cnt[k] ? E.gcol[kGcolOff + k] + atomicAdd(&E.gcol[kGcolFill + k], cnt[k]) : 0u;
+            cnt[k] = 0;
+        }
+        __syncthreads();
+        for (uint32_t f = f0 + threadIdx.x; f < f1; f += blockDim.x)
+        {
+            const uint32_t q = world_of_flat(E, f);
+            const uint32_t w = E.small_worlds[q];
             const uint32_t c = f - E.wcoff[q];
-            const uint32_t k = cand_class(E, W, E.wcand[w][c]);
-            const uint32_t slot = E.gcol[kGcolOff + k] + atomicAdd(&E.gcol[kGcolFill + k], 1u);
-            E.nlist[slot] = make_uint2(w, c);
+            const uint32_t k = cand_class(E, E.worlds[w], E.wcand[w][c]);
+            E.nlist[base[k] + atomicAdd(&cnt[k], 1u)] = make_uint2(w, c);
         }
     }
 
@@ -1241,31 +1262,182 @@ namespace rbps_gpu
 
     // The rest of a substep for one world per warp: colouring, integrate
     // (Body.cpp:18-39), position solve + velocity update, velocity solve.
-#ifndef RBPS_SUBSTEP_MIN_BLOCKS
-#define RBPS_SUBSTEP_MIN_BLOCKS 3 // resident 128-thread CTAs (4 worlds each) per SM the registers must allow
-#endif
+    // The contacting candidates of world W into S.alist, in candidate
+    // order; returns their count to every thread of the team.
     template <class T, class P>
-    __global__ void __launch_bounds__(128, RBPS_SUBSTEP_MIN_BLOCKS) k_substep_warp(const Engine<T, P> E)
+    __device__ uint32_t compact_active(const WarpTeam &, const Scr<T, P> &S, uint32_t n_cand, BlockShared &)
     {
-        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-        const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
-        WarpTeam tm;
-        for (uint32_t q = warp; q < E.n_small; q += n_warps)
+        const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
+        uint32_t n_act = 0;
+        for (uint32_t base = 0; base < n_cand; base += 32)
         {
-            const uint32_t w = E.small_worlds[q];
+            const uint32_t c = base + lane;
+            const bool live = c < n_cand;
+            const bool act = live && S.cc[c].n > 0;
+            const uint32_t m = __ballot_sync(0xffffffffu, act);
+            if (act)
+                S.alist[n_act + __popc(m & lt)] = c;
+            if (live)
+                S.color[c] = act ? 0xffffffffu : kColorIdle;
+            n_act += __popc(m);
+        }
+        __syncwarp();
+        return n_act;
+    }
+
+    template <class T, class P>
+    __device__ uint32_t compact_active(const BlockTeam &, const Scr<T, P> &S, uint32_t n_cand, BlockShared &sh)
+    {
+        uint32_t n_act = 0;
+        for (uint32_t base = 0; base < n_cand; base += blockDim.x)
+        {
+            const uint32_t c = base + threadIdx.x;
+            const bool live = c < n_cand;
+            const bool act = live && S.cc[c].n > 0;
+            uint32_t tot;
+            const uint32_t ex = block_excl_scan(act ? 1u : 0u, sh, &tot);
+            if (act)
+                S.alist[n_act + ex] = c;
+            if (live)
+                S.color[c] = act ? 0xffffffffu : kColorIdle;
+            n_act += tot;
+        }
+        __syncthreads();
+        return n_act;
+    }
+
+    // Greedy colouring of the world's contacting candidates: in candidate
+    // order, each takes the lowest colour free on both of its dynamic bodies
+    // (kColorSerial once a body has used all 64).  The team leader colours
+    // sequentially with the per-body colour masks in `mask` (shared memory
+    // when the world fits); the team then buckets the candidates by colour
+    // (corder, colour offsets in misc).  Returns the number of regular
+    // colours to every thread.
+    template <class T, class P, class Team>
+    __device__ uint32_t greedy_color_world(const Engine<T, P> &E, const Team &tm, uint32_t w,
+                                           unsigned long long *mask, BlockShared &sh)
+    {
+        const WorldDev W = E.worlds[w];
+        const Scr<T, P> S = world_scratch(E, W);
+        uint32_t *misc = S.misc;
+        const uint32_t n_cand = misc[kMiscNCand];
+        for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            mask[b] = 0ull;
+        for (uint32_t k = tm.rank(); k < 66; k += tm.size())
+            misc[kMiscCCount + k] = 0u;
+        const uint32_t n_act = compact_active(tm, S, n_cand, sh);
+        tm.sync();
+        if (tm.leader())
+        {
+            const uint8_t *type = E.B.type + W.body_off;
+            constexpr uint32_t kAhead = 8; // candidates loaded ahead of the mask updates
+            for (uint32_t q0 = 0; q0 < n_act; q0 += kAhead)
             {
-                PhaseClock clk(prof_slots(E, tm, w), false);
-                warp_color_world(E, w);
-                clk.mark(kPhColor);
-                const WorldDev W = E.worlds[w];
-                for (uint32_t b = tm.rank(); b < W.n_bodies; b += 32)
-                    integrate_body(E.B, W.body_off + b, E.h);
-                __syncwarp();
-                clk.mark(kPhIntegrate);
+                uint32_t cs[kAhead];
+                Cand cd[kAhead];
+                bool da[kAhead], db[kAhead];
+#pragma unroll
+                for (uint32_t k = 0; k < kAhead; ++k)
+                    if (q0 + k < n_act)
+                    {
+                        cs[k] = S.alist[q0 + k];
+                        cd[k] = S.cand[cs[k]];
+                        da[k] = type[cd[k].ba] == kDynamic;
+                        db[k] = type[cd[k].bb] == kDynamic;
+                    }
+#pragma unroll
+                for (uint32_t k = 0; k < kAhead; ++k)
+                    if (q0 + k < n_act)
+                    {
+                        const unsigned long long used = (da[k] ? mask[cd[k].ba] : 0ull) | (db[k] ? mask[cd[k].bb] : 0ull);
+                        uint32_t col = kColorSerial;
+                        if (used != ~0ull)
+                        {
+                            col = (uint32_t)(__ffsll((long long)~used) - 1);
+                            const unsigned long long bit = 1ull << col;
+                            if (da[k])
+                                mask[cd[k].ba] |= bit;
+                            if (db[k])
+                                mask[cd[k].bb] |= bit;
+                        }
+                        S.color[cs[k]] = col;
+                        misc[kMiscCCount + col] += 1u;
+                    }
             }
+            uint32_t run = 0, ncol = 0;
+            for (uint32_t k = 0; k <= kColorSerial; ++k)
+            {
+                const uint32_t n = misc[kMiscCCount + k];
+                misc[kMiscCOff + k] = run;
+                misc[kMiscCCount + k] = run; // becomes the fill cursor
+                if (n && k < kColorSerial)
+                    ncol = k + 1;
+                run += n;
+            }
+            misc[kMiscCOff + kColorSerial + 1] = run;
+            misc[kMiscNColors] = ncol;
+            if (ncol > misc[kMiscMaxColors])
+                misc[kMiscMaxColors] = ncol;
+        }
+        tm.sync();
+        for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
+        {
+            const uint32_t c = S.alist[q];
+            const uint32_t slot = atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
+            S.corder[slot] = c;
+        }
+        tm.sync();
+        return misc[kMiscNColors];
+    }
+
+#ifndef RBPS_SUBSTEP_MIN_BLOCKS
+#define RBPS_SUBSTEP_MIN_BLOCKS 3 // resident 128-thread CTAs per SM the registers must allow
+#endif
+    // The rest of a substep for every small world: colouring, integrate
+    // (Body.cpp:18-39), position solve + velocity update, velocity solve.
+    // The largest worlds (the first n_block_worlds of the list) get a whole
+    // CTA each; the others one warp each, four per CTA.  Worlds progress
+    // independently: a barrier is the team's own.
+    template <class T, class P>
+    __global__ void __launch_bounds__(128, RBPS_SUBSTEP_MIN_BLOCKS) k_substep(const Engine<T, P> E)
+    {
+        __shared__ BlockShared sh;
+        extern __shared__ unsigned long long smask[]; // E.mask_words colour masks
+        if (blockIdx.x < E.n_block_worlds)
+        {
+            BlockTeam tm;
+            const uint32_t w = E.small_worlds[blockIdx.x];
+            const WorldDev W = E.worlds[w];
+            PhaseClock clk(prof_slots(E, tm, w), false);
+            greedy_color_world(E, tm, w, W.n_bodies <= E.mask_words ? smask : world_scratch(E, W).bmask, sh);
+            clk.mark(kPhColor);
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+                integrate_body(E.B, W.body_off + b, E.h);
+            tm.sync();
+            clk.mark(kPhIntegrate);
             phase_position(E, tm, w);
             phase_velocity(E, tm, w);
+            return;
         }
+        const uint32_t q = E.n_block_worlds + (blockIdx.x - E.n_block_worlds) * (blockDim.x >> 5) + warp_id();
+        if (q >= E.n_small)
+            return;
+        WarpTeam tm;
+        const uint32_t w = E.small_worlds[q];
+        const WorldDev W = E.worlds[w];
+        {
+            PhaseClock clk(prof_slots(E, tm, w), false);
+            const uint32_t per_warp = E.mask_words / (blockDim.x >> 5);
+            greedy_color_world(E, tm, w,
+                               W.n_bodies <= per_warp ? smask + warp_id() * per_warp : world_scratch(E, W).bmask, sh);
+            clk.mark(kPhColor);
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += 32)
+                integrate_body(E.B, W.body_off + b, E.h);
+            __syncwarp();
+            clk.mark(kPhIntegrate);
+        }
+        phase_position(E, tm, w);
+        phase_velocity(E, tm, w);
     }
 
     template <class T, class P>
@@ -1280,19 +1452,19 @@ namespace rbps_gpu
         for (int s = 0; s < e.substeps; ++s)
         {
             k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
-            k_substep_warp<T, P><<<fl.grid_solve, fl.block_solve, 0, stream>>>(e);
+            k_substep<T, P><<<fl.grid_solve, 128, e.mask_words * sizeof(unsigned long long), stream>>>(e);
         }
         k_phase_stats<T, P><<<pl.grid[kKStats], pl.block[kKStats], 0, stream>>>(e, 1);
         return cudaGetLastError();
     }
 
-    // kernel 0: narrowphase, 1: substep (warp per world)
+    // kernel 0: narrowphase, 1: substep
     template <class T, class P>
-    cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm)
+    cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm, size_t fl_smem)
     {
         if (kernel == 0)
             return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_flat_narrow<T, P>, block, 0);
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_substep_warp<T, P>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_substep<T, P>, block, fl_smem);
     }
 
     template <class T, class P>
@@ -1335,7 +1507,7 @@ namespace rbps_gpu
     template cudaError_t rbps_gpu::launch_step_flat<T, P>(const rbps_gpu::Engine<T, P> &,                          \
                                                           const rbps_gpu::PhaseLaunch &,                            \
                                                           const rbps_gpu::FlatLaunch &, cudaStream_t);              \
-    template cudaError_t rbps_gpu::occupancy_flat<T, P>(int, int, int *);                                          \
+    template cudaError_t rbps_gpu::occupancy_flat<T, P>(int, int, int *, size_t);                                          \
     template cudaError_t rbps_gpu::occupancy_big<T, P>(int, int *);                                               \
     template cudaError_t rbps_gpu::launch_collide<T, P>(const rbps_gpu::ShapeDev *, const double *,               \
                                                        const rbps_gpu::ShapeDev *, const double *,               \

@@ -202,6 +202,8 @@ namespace rbps_gpu
         uint32_t *work_counter;
         const uint32_t *small_worlds;
         uint32_t n_small;
+        uint32_t n_block_worlds;  // colored batches: the first n of small_worlds step on a whole CTA
+        uint32_t mask_words;      // colour-mask words of shared memory per substep CTA
         // parity dumps (null when disabled)
         uint32_t *dump_pairs;   // 2 * pair_cap per slot
         Cand *dump_cand;        // cand_cap per slot
@@ -258,7 +260,7 @@ namespace rbps_gpu
     cudaError_t launch_step_flat(const Engine<T, P> &e, const PhaseLaunch &pl, const FlatLaunch &fl,
                                  cudaStream_t stream);
     template <class T, class P>
-    cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm);
+    cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm, size_t dynamic_smem);
     template <class T, class P>
     cudaError_t occupancy_phase(int kernel, int block, int *blocks_per_sm);
     template <class T, class P>
