@@ -189,7 +189,7 @@ typedef struct rbps_stats {
 enum {
     RBPS_COLLIDE_MISS = 0,        /* no overlap                                  */
     RBPS_COLLIDE_HIT = 1,         /* overlap; n_points >= 1 points are valid     */
-    RBPS_COLLIDE_UNSUPPORTED = 2  /* pair needs GJK/EPA, not built on the device */
+    RBPS_COLLIDE_UNSUPPORTED = 2  /* reserved: every supported shape pair has a device routine */
 };
 
 typedef struct rbps_manifold {
@@ -219,6 +219,18 @@ RBPS_API int rbps_hull_create(rbps_batch *batch, const double *verts, uint32_t n
 /* Quickhull helper (the reference ships no hull builder, ConvexHull.hpp:29-33):
  * CCW outward triangles of the convex hull of n points.  Writes at most
  * tri_cap triangles; *n_tris receives the count. */
+/* The merged-polygon and adjacency tables the library builds for a hull
+ * (those of convex_hull_data_create, ConvexHull.hpp:149-420), host only:
+ * counts = {polygons, polygon indices, vertex->polygon entries,
+ * vertex->neighbour entries, polygon->polygon entries}; each output array
+ * (any may be NULL) needs at most `cap` entries (poly_normals: 3 per polygon;
+ * the *_offsets arrays: polygons + 1 or vertices + 1).  Returns
+ * RBPS_ERR_CAPACITY with counts filled when cap is too small. */
+RBPS_API int rbps_hull_tables(const double *verts, uint32_t n_verts, const uint32_t *tris, uint32_t n_tris,
+                              uint32_t cap, uint32_t *counts, uint32_t *poly_offsets, uint32_t *poly_indices,
+                              double *poly_normals, uint32_t *v2p_offsets, uint32_t *v2p_indices,
+                              uint32_t *v2n_offsets, uint32_t *v2n_indices, uint32_t *p2p_offsets,
+                              uint32_t *p2p_indices);
 RBPS_API int rbps_quickhull(const double *points, uint32_t n_points,
                             uint32_t *tris, uint32_t tri_cap, uint32_t *n_tris);
 

@@ -45,6 +45,8 @@ def lib():
         L.ref_collide.restype = C.c_int
         L.ref_collide.argtypes = [_P, C.c_uint32, _P, _D, _P, _D, _P]
         L.ref_default_descs.argtypes = [_P, _P, _P, _P, _P, _D]
+        L.ref_hull_tables.restype = C.c_int
+        L.ref_hull_tables.argtypes = [_P, C.c_uint32, C.c_uint32, _U, _U, _U, _D, _U, _U, _U, _U, _U, _U]
         L.ref_step.argtypes = [_P, C.c_int]
         L.ref_body_count.restype = C.c_uint32
         L.ref_body_count.argtypes = [_P]
@@ -168,11 +170,36 @@ class RefWorld:
             raise ValueError("ref_collide: unknown shape or hull")
         return out[:n]
 
+    def hull_tables(self, hull, cap=4096):
+        """The reference's polygon / adjacency tables of this world's hull."""
+        return _tables(lambda *a: lib().ref_hull_tables(self.h, hull, cap, *a), cap)
+
     def collision_groups(self):
         c = self.contacts()
         colors = np.zeros(max(len(c), 1), np.uint32)
         ng = lib().ref_collision_groups(self.h, colors.ctypes.data_as(_U), len(c))
         return colors[:len(c)], ng
+
+
+TABLE_NAMES = ("poly_offsets", "poly_indices", "poly_normals", "v2p_offsets", "v2p_indices", "v2n_offsets",
+               "v2n_indices", "p2p_offsets", "p2p_indices")
+
+
+def _tables(fn, cap):
+    """Calls a table dump with cap-sized buffers; vertex offset tables come
+    back at full length (callers slice vert_count + 1)."""
+    counts = np.zeros(5, np.uint32)
+    arrs = [np.zeros(cap, np.uint32), np.zeros(cap, np.uint32), np.zeros(3 * cap, np.float64)] + \
+        [np.zeros(cap, np.uint32) for _ in range(6)]
+    ptrs = [a.ctypes.data_as(_D) if a.dtype == np.float64 else a.ctypes.data_as(_U) for a in arrs]
+    rc = fn(counts.ctypes.data_as(_U), *ptrs)
+    if rc != 0:
+        raise ValueError(f"hull tables: status {rc}")
+    npoly, nidx, nv2p, nv2n, np2p = (int(x) for x in counts)
+    return {"poly_offsets": arrs[0][:npoly + 1], "poly_indices": arrs[1][:nidx],
+            "poly_normals": arrs[2][:3 * npoly].reshape(-1, 3), "v2p_offsets": arrs[3],
+            "v2p_indices": arrs[4][:nv2p], "v2n_offsets": arrs[5], "v2n_indices": arrs[6][:nv2n],
+            "p2p_offsets": arrs[7][:npoly + 1], "p2p_indices": arrs[8][:np2p]}
 
 
 def default_descs():

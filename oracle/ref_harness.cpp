@@ -278,6 +278,48 @@ extern "C"
         world_cfg[3] = bc.reinsert_threshold;
     }
 
+    // The reference's polygon / adjacency tables of hull `hull` of world h
+    // (ConvexHullData, ConvexHull.hpp:60-98), in the layout of
+    // rbps_hull_tables; returns -1 for an unknown hull, -2 when cap is small.
+    int ref_hull_tables(void *h, uint32_t hull, uint32_t cap, uint32_t *counts, uint32_t *poly_offsets,
+                        uint32_t *poly_indices, double *poly_normals, uint32_t *v2p_offsets, uint32_t *v2p_indices,
+                        uint32_t *v2n_offsets, uint32_t *v2n_indices, uint32_t *p2p_offsets, uint32_t *p2p_indices)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        if (hull >= rw->hulls.size())
+            return -1;
+        const rbc::ConvexHullData *d = rw->hulls[hull]->data;
+        const uint32_t np = d->poly_count, nv = d->vert_count;
+        counts[0] = np;
+        counts[1] = np ? d->poly_offsets[np] : 0;
+        counts[2] = np ? d->vertex_to_polys_offsets[nv] : 0;
+        counts[3] = np ? d->vertex_to_neighbors_offsets[nv] : 0;
+        counts[4] = np ? d->poly_to_polys_offsets[np] : 0;
+        uint32_t need = np + 1;
+        for (int k = 1; k < 5; ++k)
+            need = counts[k] > need ? counts[k] : need;
+        if (np && nv + 1 > need)
+            need = nv + 1;
+        if (need > cap)
+            return -2;
+        if (!np)
+        {
+            poly_offsets[0] = 0;
+            return 0;
+        }
+        std::memcpy(poly_offsets, d->poly_offsets, 4 * (np + 1));
+        std::memcpy(poly_indices, d->poly_indices, 4 * counts[1]);
+        for (uint32_t p = 0; p < np; ++p)
+            put3(poly_normals + 3 * p, d->poly_normals[p]);
+        std::memcpy(v2p_offsets, d->vertex_to_polys_offsets, 4 * (nv + 1));
+        std::memcpy(v2p_indices, d->vertex_to_polys_indices, 4 * counts[2]);
+        std::memcpy(v2n_offsets, d->vertex_to_neighbors_offsets, 4 * (nv + 1));
+        std::memcpy(v2n_indices, d->vertex_to_neighbors_indices, 4 * counts[3]);
+        std::memcpy(p2p_offsets, d->poly_to_polys_offsets, 4 * (np + 1));
+        std::memcpy(p2p_indices, d->poly_to_polys_indices, 4 * counts[4]);
+        return 0;
+    }
+
     void ref_step(void *h, int n)
     {
         auto *rw = static_cast<RefWorld *>(h);

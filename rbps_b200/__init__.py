@@ -20,7 +20,7 @@ import numpy as np
 
 from . import abi
 
-__all__ = ["lib", "Batch", "World", "BroadPhase", "RbpsError", "abi", "quickhull"]
+__all__ = ["lib", "Batch", "World", "BroadPhase", "RbpsError", "abi", "quickhull", "hull_tables"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("RBPS_B200_LIB") or os.path.join(_HERE, "librbps_b200.so")
@@ -69,6 +69,8 @@ def lib():
             "rbps_batch_destroy": (i, [_P]),
             "rbps_hull_create": (i, [_P, _D, C.c_uint32, _U, C.c_uint32, _U]),
             "rbps_quickhull": (i, [_D, C.c_uint32, _U, C.c_uint32, _U]),
+            "rbps_hull_tables": (i, [_D, C.c_uint32, _U, C.c_uint32, C.c_uint32, _U, _U, _U, _D, _U, _U, _U, _U, _U,
+                                     _U]),
             "rbps_world_add_body": (i, [_P, C.c_uint32, _P, _U]),
             "rbps_world_add_bodies": (i, [_P, C.c_uint32, C.c_uint32, _P, _U]),
             "rbps_world_set_body_force": (i, [_P, C.c_uint32, C.c_uint32, _D, _D]),
@@ -141,6 +143,24 @@ def quickhull(points):
     n = C.c_uint32(0)
     _check(lib().rbps_quickhull(_dp(pts), len(pts), tris.ctypes.data_as(_U), cap, C.byref(n)))
     return tris[:n.value].copy()
+
+
+def hull_tables(verts, tris, cap=4096):
+    """The merged-polygon and adjacency tables the library builds for a hull
+    (dict of numpy arrays; vertex offset tables at full cap length)."""
+    v = np.ascontiguousarray(verts, np.float64)
+    t = np.ascontiguousarray(tris, np.uint32)
+    counts = np.zeros(5, np.uint32)
+    arrs = [np.zeros(cap, np.uint32), np.zeros(cap, np.uint32), np.zeros(3 * cap, np.float64)] + \
+        [np.zeros(cap, np.uint32) for _ in range(6)]
+    ptrs = [a.ctypes.data_as(_D) if a.dtype == np.float64 else a.ctypes.data_as(_U) for a in arrs]
+    _check(lib().rbps_hull_tables(_dp(v), len(v), t.ctypes.data_as(_U), len(t), cap, counts.ctypes.data_as(_U),
+                                  *ptrs))
+    npoly, nidx, nv2p, nv2n, np2p = (int(x) for x in counts)
+    return {"poly_offsets": arrs[0][:npoly + 1], "poly_indices": arrs[1][:nidx],
+            "poly_normals": arrs[2][:3 * npoly].reshape(-1, 3), "v2p_offsets": arrs[3],
+            "v2p_indices": arrs[4][:nv2p], "v2n_offsets": arrs[5], "v2n_indices": arrs[6][:nv2n],
+            "p2p_offsets": arrs[7][:npoly + 1], "p2p_indices": arrs[8][:np2p]}
 
 
 class Batch:

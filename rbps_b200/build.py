@@ -4,8 +4,9 @@
 
 Each translation unit is compiled by nvcc with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo``; the FP64 step
-kernels are compiled with ``-fmad=false`` so double arithmetic rounds like
-the reference's x86-64 build (no FMA contraction).  Objects are rebuilt only
+kernels and the GJK kernels (double arithmetic in every precision) are
+compiled with ``-fmad=false`` so double arithmetic rounds like the
+reference's x86-64 build (no FMA contraction).  Objects are rebuilt only
 when a source or header is newer than the library.
 """
 import argparse
@@ -29,6 +30,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 UNITS = {
     "engine_f64.cu": ["-fmad=false"],
     "engine_f32.cu": [],
+    "gjk_f64.cu": ["-fmad=false"],
+    "gjk_f32.cu": ["-fmad=false"],
     "batch.cu": [],
     "bp_api.cu": [],
     "selftest.cu": [],

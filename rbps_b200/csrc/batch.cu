@@ -97,11 +97,192 @@ namespace
         std::vector<rbps_joint_desc> joints;
     };
 
+    // A convex hull as the device needs it: vertices, local AABB, and the
+    // merged-polygon and adjacency tables of convex_hull_data_create
+    // (ConvexHull.hpp:149-420) for the hull-hull contact manifold.
     struct HostHull
     {
         std::vector<double> verts;
         double aabb[6];
+        std::vector<uint32_t> poly_off{0}, poly_idx;
+        std::vector<double> poly_n;                   // 3 per polygon
+        std::vector<uint32_t> v2p_off, v2p_idx;       // polygons of each vertex
+        std::vector<uint32_t> v2n_off, v2n_idx;       // polygon-edge neighbours of each vertex
+        std::vector<uint32_t> p2p_off, p2p_idx;       // polygons sharing an edge with each polygon
     };
+
+    // Restatement of convex_hull_data_create's table building
+    // (ConvexHull.hpp:149-420): triangle normals; union-find over triangle
+    // pairs whose normals have dot > 0.99995; per group, the boundary loop of
+    // directed edges whose reverse is absent, walked from the first boundary
+    // edge; the normalised sum of the group's normals; then the vertex ->
+    // polygons, vertex -> neighbours and polygon -> polygons tables in the
+    // same insertion order.  Groups with an empty boundary, a loop under 3
+    // vertices or a zero normal sum are dropped, as there.
+    void build_hull_tables(HostHull &h, const uint32_t *tris, uint32_t n_tris)
+    {
+        const uint32_t nv = (uint32_t)(h.verts.size() / 3);
+        auto V = [&](uint32_t i) { return vec3<double>(h.verts[3 * i], h.verts[3 * i + 1], h.verts[3 * i + 2]); };
+        h.poly_off.assign(1, 0);
+        h.poly_idx.clear();
+        h.poly_n.clear();
+        h.v2p_off.clear(); h.v2p_idx.clear();
+        h.v2n_off.clear(); h.v2n_idx.clear();
+        h.p2p_off.clear(); h.p2p_idx.clear();
+        if (!tris || n_tris == 0)
+            return;
+        std::vector<vec3<double>> norms(n_tris);
+        for (uint32_t f = 0; f < n_tris; ++f)
+        {
+            const vec3<double> A = V(tris[3 * f]), B = V(tris[3 * f + 1]), C = V(tris[3 * f + 2]);
+            norms[f] = normalize(cross(B - A, C - A));
+        }
+        std::vector<int> parent(n_tris);
+        for (uint32_t i = 0; i < n_tris; ++i)
+            parent[i] = (int)i;
+        auto find = [&parent](int x) {
+            while (parent[x] != x)
+            {
+                parent[x] = parent[parent[x]];
+                x = parent[x];
+            }
+            return x;
+        };
+        for (uint32_t i = 0; i < n_tris; ++i)
+            for (uint32_t j = i + 1; j < n_tris; ++j)
+                if (dot(norms[i], norms[j]) > 0.99995)
+                {
+                    const int ri = find((int)i), rj = find((int)j);
+                    if (ri != rj)
+                        parent[ri] = rj;
+                }
+        std::vector<std::vector<uint32_t>> groups;
+        std::vector<int> root_group(n_tris, -1);
+        for (uint32_t i = 0; i < n_tris; ++i)
+        {
+            const int r = find((int)i);
+            if (root_group[r] < 0)
+            {
+                root_group[r] = (int)groups.size();
+                groups.emplace_back();
+            }
+            groups[root_group[r]].push_back(i);
+        }
+        for (const auto &g : groups)
+        {
+            std::vector<std::pair<uint32_t, uint32_t>> e, bnd;
+            for (uint32_t f : g)
+            {
+                const uint32_t a = tris[3 * f], b = tris[3 * f + 1], c = tris[3 * f + 2];
+                e.push_back({a, b});
+                e.push_back({b, c});
+                e.push_back({c, a});
+            }
+            for (size_t i = 0; i < e.size(); ++i)
+            {
+                bool rev = false;
+                for (size_t j = 0; j < e.size(); ++j)
+                    if (i != j && e[j].first == e[i].second && e[j].second == e[i].first)
+                    {
+                        rev = true;
+                        break;
+                    }
+                if (!rev)
+                    bnd.push_back(e[i]);
+            }
+            if (bnd.empty())
+                continue;
+            std::vector<bool> used(bnd.size(), false);
+            std::vector<uint32_t> loop;
+            used[0] = true;
+            loop.push_back(bnd[0].first);
+            uint32_t cur = bnd[0].second;
+            for (size_t step = 1; step < bnd.size(); ++step)
+            {
+                bool found = false;
+                for (size_t k = 0; k < bnd.size(); ++k)
+                    if (!used[k] && bnd[k].first == cur)
+                    {
+                        used[k] = true;
+                        loop.push_back(bnd[k].first);
+                        cur = bnd[k].second;
+                        found = true;
+                        break;
+                    }
+                if (!found)
+                    break;
+            }
+            if (loop.size() < 3)
+                continue;
+            vec3<double> avg(0.0, 0.0, 0.0);
+            for (uint32_t f : g)
+                avg = avg + norms[f];
+            const double len = length(avg);
+            if (len < kEpsilon)
+                continue;
+            avg = avg / len;
+            h.poly_idx.insert(h.poly_idx.end(), loop.begin(), loop.end());
+            h.poly_off.push_back((uint32_t)h.poly_idx.size());
+            h.poly_n.push_back(avg.x);
+            h.poly_n.push_back(avg.y);
+            h.poly_n.push_back(avg.z);
+        }
+        const uint32_t np = (uint32_t)(h.poly_off.size() - 1);
+        if (np == 0)
+            return;
+        std::vector<std::vector<uint32_t>> v2p(nv), v2n(nv), p2p(np);
+        auto push_unique = [](std::vector<uint32_t> &v, uint32_t x) {
+            if (std::find(v.begin(), v.end(), x) == v.end())
+                v.push_back(x);
+        };
+        for (uint32_t p = 0; p < np; ++p)
+        {
+            const uint32_t s0 = h.poly_off[p], n = h.poly_off[p + 1] - s0;
+            for (uint32_t i = 0; i < n; ++i)
+            {
+                const uint32_t a = h.poly_idx[s0 + i], b = h.poly_idx[s0 + (i + 1) % n];
+                push_unique(v2p[a], p);
+                push_unique(v2n[a], b);
+                push_unique(v2n[b], a);
+            }
+        }
+        for (uint32_t p = 0; p < np; ++p)
+        {
+            const uint32_t sp = h.poly_off[p], n_p = h.poly_off[p + 1] - sp;
+            for (uint32_t q = 0; q < np; ++q)
+            {
+                if (q == p)
+                    continue;
+                const uint32_t sq = h.poly_off[q], n_q = h.poly_off[q + 1] - sq;
+                bool shared = false;
+                for (uint32_t i = 0; i < n_p && !shared; ++i)
+                {
+                    const uint32_t a = h.poly_idx[sp + i], b = h.poly_idx[sp + (i + 1) % n_p];
+                    for (uint32_t j = 0; j < n_q; ++j)
+                        if (a == h.poly_idx[sq + (j + 1) % n_q] && b == h.poly_idx[sq + j])
+                        {
+                            shared = true;
+                            break;
+                        }
+                }
+                if (shared)
+                    p2p[p].push_back(q);
+            }
+        }
+        auto flatten = [](const std::vector<std::vector<uint32_t>> &src, std::vector<uint32_t> &off,
+                          std::vector<uint32_t> &idx) {
+            off.assign(1, 0);
+            idx.clear();
+            for (const auto &v : src)
+            {
+                idx.insert(idx.end(), v.begin(), v.end());
+                off.push_back((uint32_t)idx.size());
+            }
+        };
+        flatten(v2p, h.v2p_off, h.v2p_idx);
+        flatten(v2n, h.v2n_off, h.v2n_idx);
+        flatten(p2p, h.p2p_off, h.p2p_idx);
+    }
 
     struct DevBuf
     {
@@ -138,6 +319,9 @@ struct rbps_batch
     double *hull_verts = nullptr;
     uint32_t *hull_voff = nullptr;
     double *hull_aabb = nullptr;
+    HullDesc *hull_desc = nullptr;
+    uint32_t *hull_u32 = nullptr;
+    double *hull_pn = nullptr;
     uint32_t *bp_coll = nullptr;
     FatBox *fat = nullptr;
     uint32_t *ep_key = nullptr, *ep_id = nullptr, *ep_pos = nullptr;
@@ -154,6 +338,11 @@ struct rbps_batch
     // host mirrors
     std::vector<WorldDev> wdev;
     std::vector<uint32_t> small_ids, big_ids;
+    // GJK pass (hull colliders present): queued pairs and workspaces
+    uint2 *gjk_list = nullptr;
+    uint32_t *gjk_count = nullptr;
+    uint32_t gjk_cap = 0, gjk_slots = 0;
+    void *gjk_ws = nullptr;
     PhaseLaunch phase{};      // grid / block of each phase kernel
     FlatLaunch flat{};        // flat colored pipeline
     bool use_flat = false;
@@ -325,10 +514,12 @@ extern "C" int rbps_hull_create(rbps_batch *b, const double *verts, uint32_t n_v
         return fail(RBPS_ERR_INVALID, "rbps_hull_create: need vertices");
     if (b->committed)
         return fail(RBPS_ERR_INVALID, "rbps_hull_create: batch already committed");
-    (void)tris;
-    (void)n_tris;
+    for (uint32_t t = 0; tris && t < 3 * n_tris; ++t)
+        if (tris[t] >= n_verts)
+            return fail(RBPS_ERR_INVALID, "rbps_hull_create: triangle index out of range");
     HostHull h;
     h.verts.assign(verts, verts + 3 * n_verts);
+    build_hull_tables(h, tris, n_tris);
     // local AABB as convex_hull_data_create computes it (ConvexHull.hpp:401-414)
     double mn[3] = {(double)1e30f, (double)1e30f, (double)1e30f};
     double mx[3] = {(double)-1e30f, (double)-1e30f, (double)-1e30f};
@@ -471,6 +662,9 @@ namespace
         e.hulls.verts = b->hull_verts;
         e.hulls.v_off = b->hull_voff;
         e.hulls.local_aabb = b->hull_aabb;
+        e.hulls.desc = b->hull_desc;
+        e.hulls.u32 = b->hull_u32;
+        e.hulls.poly_n = b->hull_pn;
         e.bp_coll = b->bp_coll;
         e.fat = b->fat;
         e.ep_key = b->ep_key;
@@ -517,6 +711,11 @@ namespace
         e.dump_pair_cap = b->dump_pair_cap;
         e.dump_cand_cap = b->dump_cand_cap;
         e.prof = b->prof_off ? nullptr : b->prof;
+        e.gjk_list = b->gjk_list;
+        e.gjk_count = b->gjk_count;
+        e.gjk_cap = b->gjk_cap;
+        e.gjk_slots = b->gjk_slots;
+        e.gjk_ws = b->gjk_ws;
         return e;
     }
 
@@ -717,8 +916,33 @@ static int commit_typed(rbps_batch *b)
             hoff.push_back((uint32_t)(hv.size() / 3));
             ha.insert(ha.end(), h.aabb, h.aabb + 6);
         }
+        std::vector<HullDesc> hd;
+        std::vector<uint32_t> u32;
+        std::vector<double> pn;
+        for (const auto &h : b->hulls)
+        {
+            HullDesc d{};
+            d.np = (uint32_t)(h.poly_off.size() - 1);
+            auto put = [&u32](const std::vector<uint32_t> &v) {
+                const uint32_t base = (uint32_t)u32.size();
+                u32.insert(u32.end(), v.begin(), v.end());
+                return base;
+            };
+            d.po = put(h.poly_off);
+            d.pi = put(h.poly_idx);
+            d.pn = (uint32_t)(pn.size() / 3);
+            pn.insert(pn.end(), h.poly_n.begin(), h.poly_n.end());
+            d.v2p_o = put(h.v2p_off);
+            d.v2p_i = put(h.v2p_idx);
+            d.v2n_o = put(h.v2n_off);
+            d.v2n_i = put(h.v2n_idx);
+            d.p2p_o = put(h.p2p_off);
+            d.p2p_i = put(h.p2p_idx);
+            hd.push_back(d);
+        }
         if ((rc = b->upload(&b->hull_verts, hv)) || (rc = b->upload(&b->hull_voff, hoff)) ||
-            (rc = b->upload(&b->hull_aabb, ha)))
+            (rc = b->upload(&b->hull_aabb, ha)) || (rc = b->upload(&b->hull_desc, hd)) ||
+            (rc = b->upload(&b->hull_u32, u32)) || (rc = b->upload(&b->hull_pn, pn)))
             return rc;
     }
     HullSetDev hs_host{nullptr, nullptr, nullptr};
@@ -1012,6 +1236,27 @@ static int commit_typed(rbps_batch *b)
             words = std::max(words, std::min<uint32_t>(b->wdev[b->small_ids[0]].n_bodies, kMaskWordsMax));
         b->mask_words = words;
         b->use_flat = true;
+    }
+    // ---- GJK pass: only batches with hull colliders reach it
+    {
+        bool any_hull = false;
+        size_t cap = 0;
+        for (uint32_t w : b->small_ids)
+        {
+            const WorldDev &d = b->wdev[w];
+            cap += (size_t)d.pair_cap + 1 + d.n_pc;
+            for (const auto &c : b->worlds[w].colliders)
+                any_hull = any_hull || c.shape == RBPS_SHAPE_CONVEX_HULL;
+        }
+        if (any_hull && cap)
+        {
+            b->gjk_cap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
+            b->gjk_slots = (uint32_t)(((size_t)b->sm_count * 16 + 127) / 128 * 128);
+            if ((rc = b->alloc((void **)&b->gjk_list, sizeof(uint2) * cap)) ||
+                (rc = b->alloc((void **)&b->gjk_count, 64)) ||
+                (rc = b->alloc(&b->gjk_ws, gjk_work_bytes<T, P>() * b->gjk_slots)))
+                return rc;
+        }
     }
     if ((rc = b->alloc((void **)&b->work_counter, std::max<size_t>(64, 4 * (size_t)b->n_counters))) || (rc = b->alloc((void **)&b->error_d, 64)) ||
         (rc = b->alloc((void **)&b->stats_d, sizeof(WorldStats) * W)))
@@ -1621,6 +1866,47 @@ extern "C" int rbps_batch_get_profile(rbps_batch *b, uint64_t *out, uint32_t cap
     return RBPS_OK;
 }
 
+// Polygon and adjacency tables of a hull (see rbps_hull_tables in rbps_gpu.h).
+extern "C" int rbps_hull_tables(const double *verts, uint32_t n_verts, const uint32_t *tris, uint32_t n_tris,
+                                uint32_t cap, uint32_t *counts, uint32_t *poly_offsets, uint32_t *poly_indices,
+                                double *poly_normals, uint32_t *v2p_offsets, uint32_t *v2p_indices,
+                                uint32_t *v2n_offsets, uint32_t *v2n_indices, uint32_t *p2p_offsets,
+                                uint32_t *p2p_indices)
+{
+    if (!verts || !n_verts || !counts)
+        return fail(RBPS_ERR_INVALID, "rbps_hull_tables: need vertices and counts");
+    for (uint32_t t = 0; tris && t < 3 * n_tris; ++t)
+        if (tris[t] >= n_verts)
+            return fail(RBPS_ERR_INVALID, "rbps_hull_tables: triangle index out of range");
+    HostHull h;
+    h.verts.assign(verts, verts + 3 * n_verts);
+    build_hull_tables(h, tris, n_tris);
+    const uint32_t np = (uint32_t)(h.poly_off.size() - 1);
+    counts[0] = np;
+    counts[1] = (uint32_t)h.poly_idx.size();
+    counts[2] = (uint32_t)h.v2p_idx.size();
+    counts[3] = (uint32_t)h.v2n_idx.size();
+    counts[4] = (uint32_t)h.p2p_idx.size();
+    const uint32_t need = std::max({np + 1, counts[1], counts[2], counts[3], counts[4], n_verts + 1});
+    if (need > cap)
+        return fail(RBPS_ERR_CAPACITY, "rbps_hull_tables: tables need %u entries, cap is %u", need, cap);
+    auto put = [](uint32_t *dst, const std::vector<uint32_t> &v) {
+        if (dst)
+            std::copy(v.begin(), v.end(), dst);
+    };
+    put(poly_offsets, h.poly_off);
+    put(poly_indices, h.poly_idx);
+    if (poly_normals)
+        std::copy(h.poly_n.begin(), h.poly_n.end(), poly_normals);
+    put(v2p_offsets, h.v2p_off);
+    put(v2p_indices, h.v2p_idx);
+    put(v2n_offsets, h.v2n_off);
+    put(v2n_indices, h.v2n_idx);
+    put(p2p_offsets, h.p2p_off);
+    put(p2p_indices, h.p2p_idx);
+    return RBPS_OK;
+}
+
 // Device narrowphase of independent shape pairs (see rbps_batch_collide in
 // rbps_gpu.h).
 static_assert(sizeof(CollideOut) == sizeof(rbps_manifold), "CollideOut must mirror rbps_manifold");
@@ -1629,10 +1915,16 @@ template <class T, class P>
 static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> &sa, const double *tf_a,
                          const std::vector<ShapeDev> &sb, const double *tf_b, rbps_manifold *out)
 {
-    HullSetDev hs{b->hull_verts, b->hull_voff, b->hull_aabb};
+    HullSetDev hs{b->hull_verts, b->hull_voff, b->hull_aabb, b->hull_desc, b->hull_u32, b->hull_pn};
     const size_t shape_bytes = (size_t)n * sizeof(ShapeDev), tf_bytes = (size_t)n * 7 * sizeof(double);
+    bool gjk = false;
+    for (uint32_t i = 0; i < n && !gjk; ++i)
+        gjk = (sa[i].kind == kHull || sb[i].kind == kHull) && sa[i].kind != kPlane && sb[i].kind != kPlane;
+    // GJK pairs need a workspace per thread: fewer threads, each looping
+    const uint32_t threads = (uint32_t)std::min<size_t>(((size_t)n + 127) / 128 * 128, gjk ? 1024 : 65536);
+    const size_t ws_bytes = gjk ? gjk_work_bytes<T, P>() * threads : 0;
     char *d = nullptr;
-    const size_t total = 2 * shape_bytes + 2 * tf_bytes + (size_t)n * sizeof(CollideOut);
+    const size_t total = 2 * shape_bytes + 2 * tf_bytes + (size_t)n * sizeof(CollideOut) + ws_bytes;
     CU(cudaMalloc(&d, total));
     ShapeDev *dsa = (ShapeDev *)d, *dsb = (ShapeDev *)(d + shape_bytes);
     double *dta = (double *)(d + 2 * shape_bytes), *dtb = (double *)(d + 2 * shape_bytes + tf_bytes);
@@ -1644,8 +1936,9 @@ static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> 
         e = cudaMemcpyAsync(dta, tf_a, tf_bytes, cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dtb, tf_b, tf_bytes, cudaMemcpyHostToDevice, b->stream);
+    void *ws = gjk ? (void *)(d + 2 * shape_bytes + 2 * tf_bytes + (size_t)n * sizeof(CollideOut)) : nullptr;
     if (e == cudaSuccess)
-        e = launch_collide<T, P>(dsa, dta, dsb, dtb, hs, n, dout, b->stream);
+        e = launch_collide<T, P>(dsa, dta, dsb, dtb, hs, n, dout, ws, threads, b->error_d, b->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(out, dout, (size_t)n * sizeof(CollideOut), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess)
@@ -1653,7 +1946,7 @@ static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> 
     cudaFree(d);
     if (e != cudaSuccess)
         return fail(RBPS_ERR_CUDA, "rbps_batch_collide: %s", cudaGetErrorString(e));
-    return RBPS_OK;
+    return b->committed ? check_device_error(b) : RBPS_OK;
 }
 
 extern "C" int rbps_batch_collide(rbps_batch *b, uint32_t n, const rbps_collider_desc *a, const double *tf_a,

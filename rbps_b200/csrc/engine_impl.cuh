@@ -21,6 +21,7 @@
 // velocity solve (contacts, joint damping).
 #pragma once
 #include "engine_types.cuh"
+#include "gjk.cuh"
 #include "team.cuh"
 
 namespace rbps_gpu
@@ -448,27 +449,13 @@ namespace rbps_gpu
         return misc[kMiscFlags + 1];
     }
 
-    // Narrowphase of one candidate + emit_contact (CollisionPipeline.cpp:59-104).
+    // emit_contact (CollisionPipeline.cpp:59-104): a pair's manifold into
+    // its contact rows (points on A and B, body-local lever arms, mixed
+    // materials).
     template <class T, class P>
-    __device__ __forceinline__ void narrow_candidate(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
-                                                     CandContacts<T, P> &out, uint32_t &n_gjk)
+    __device__ __forceinline__ void emit_manifold(const Engine<T, P> &E, uint32_t gca, uint32_t gcb, uint32_t gba,
+                                                  uint32_t gbb, const Manifold<T> &m, int n, CandContacts<T, P> &out)
     {
-        if (cd.ca >= W.n_coll || cd.cb >= W.n_coll || cd.ba >= W.n_bodies || cd.bb >= W.n_bodies)
-        {
-            set_error_at(E.error, kErrInternal, 3, cd.ca);
-            out.n = 0;
-            return;
-        }
-        const uint32_t gca = W.coll_off + cd.ca, gcb = W.coll_off + cd.cb;
-        const uint32_t gba = W.body_off + cd.ba, gbb = W.body_off + cd.bb;
-        const tf<T> ta = collider_tf(E, gca, gba);
-        const tf<T> tb = collider_tf(E, gcb, gbb);
-        Manifold<T> m;
-        m.n = 0;
-        const int res = dispatch_pair(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, m);
-        if (res == kNeedsGjk)
-            ++n_gjk;
-        const int n = (res == kHit) ? m.n : 0;
         out.n = n;
         if (n == 0)
             return;
@@ -493,6 +480,81 @@ namespace rbps_gpu
             c.depth = m.depth[k];
             c.coll = 0;
         }
+    }
+
+    // Narrowphase of one candidate (the analytic routines); returns
+    // kNeedsGjk for a pair the GJK pass handles (its rows are left empty).
+    template <class T, class P>
+    __device__ __forceinline__ int narrow_candidate(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+                                                    CandContacts<T, P> &out)
+    {
+        if (cd.ca >= W.n_coll || cd.cb >= W.n_coll || cd.ba >= W.n_bodies || cd.bb >= W.n_bodies)
+        {
+            set_error_at(E.error, kErrInternal, 3, cd.ca);
+            out.n = 0;
+            return kMiss;
+        }
+        const uint32_t gca = W.coll_off + cd.ca, gcb = W.coll_off + cd.cb;
+        const uint32_t gba = W.body_off + cd.ba, gbb = W.body_off + cd.bb;
+        const tf<T> ta = collider_tf(E, gca, gba);
+        const tf<T> tb = collider_tf(E, gcb, gbb);
+        Manifold<T> m;
+        m.n = 0;
+        const int res = dispatch_pair(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, m);
+        emit_manifold(E, gca, gcb, gba, gbb, m, res == kHit ? m.n : 0, out);
+        return res;
+    }
+
+    // A GJK pair found by the narrowphase: queued for k_gjk when the batch
+    // has a GJK workspace, else counted as unsupported.
+    template <class T, class P>
+    __device__ __forceinline__ void queue_gjk(const Engine<T, P> &E, uint32_t w, uint32_t c, uint32_t &n_gjk)
+    {
+        if (E.gjk_list)
+        {
+            const uint32_t slot = atomicAdd(E.gjk_count, 1u);
+            if (slot < E.gjk_cap)
+                E.gjk_list[slot] = make_uint2(w, c);
+            else
+                set_error_at(E.error, -2, 6, slot); // RBPS_ERR_CAPACITY
+        }
+        else
+            ++n_gjk;
+    }
+
+    // GJK / EPA / manifold of one queued pair (world w, candidate c) on the
+    // workspace of the calling thread.
+    // GJK and EPA run in double in every precision: their tolerances
+    // (EPA convergence 1e-6, coplanarity 1e-12) are below float resolution.
+    template <class T>
+    __device__ __forceinline__ Manifold<T> manifold_cast(const Manifold<double> &d)
+    {
+        Manifold<T> m;
+        m.n = d.n;
+        m.normal = vec3<T>(d.normal);
+        for (int k = 0; k < 4; ++k)
+        {
+            m.pos[k] = vec3<T>(d.pos[k]);
+            m.depth[k] = T(d.depth[k]);
+        }
+        return m;
+    }
+
+    template <class T, class P>
+    __device__ void gjk_candidate(const Engine<T, P> &E, uint32_t w, uint32_t c, GjkWork<double> &ws)
+    {
+        const WorldDev W = E.worlds[w];
+        const Cand cd = E.wcand ? E.wcand[w][c] : world_scratch(E, W).cand[c];
+        CandContacts<T, P> &out = E.wcc ? E.wcc[w][c] : world_scratch(E, W).cc[c];
+        const uint32_t gca = W.coll_off + cd.ca, gcb = W.coll_off + cd.cb;
+        const uint32_t gba = W.body_off + cd.ba, gbb = W.body_off + cd.bb;
+        const tf<double> ta = collider_tf_d(E, gca, gba);
+        const tf<double> tb = collider_tf_d(E, gcb, gbb);
+        Manifold<double> m;
+        m.n = 0;
+        const bool hit = gjk_epa_manifold(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, ws, m, E.error);
+        const Manifold<T> mt = manifold_cast<T>(m);
+        emit_manifold(E, gca, gcb, gba, gbb, mt, hit ? mt.n : 0, out);
     }
 
     // All contact rows of one candidate pair (global bodies ba, bb), in list
@@ -649,7 +711,14 @@ namespace rbps_gpu
         const uint32_t n_cand = S.misc[kMiscNCand];
         uint32_t n_gjk = 0;
         for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
-            narrow_candidate(E, W, S.cand[c], S.cc[c], n_gjk);
+            if (narrow_candidate(E, W, S.cand[c], S.cc[c]) == kNeedsGjk)
+            {
+                // a world on the cooperative grid has no GJK pass: count it
+                if (tm.ncta() > 1)
+                    ++n_gjk;
+                else
+                    queue_gjk(E, w, c, n_gjk);
+            }
         if (n_gjk)
             atomicAdd(S.misc + kMiscNGjk, n_gjk);
         tm.sync();
@@ -960,7 +1029,10 @@ namespace rbps_gpu
         k_phase_frame<T, P><<<pl.grid[kKFrame], pl.block[kKFrame], 0, stream>>>(e, ctr++);
         for (int s = 0; s < e.substeps; ++s)
         {
+            if (e.gjk_list)
+                cudaMemsetAsync(e.gjk_count, 0, 4, stream);
             k_phase_narrow<T, P><<<pl.grid[kKNarrow], pl.block[kKNarrow], 0, stream>>>(e, ctr++);
+            launch_gjk(e, stream);
             k_phase_color<T, P><<<pl.grid[kKColor], pl.block[kKColor], 0, stream>>>(e, ctr++);
             k_phase_position<T, P><<<pl.grid[kKPosition], pl.block[kKPosition], 0, stream>>>(e, ctr++);
             k_phase_velocity<T, P><<<pl.grid[kKVelocity], pl.block[kKVelocity], 0, stream>>>(e, ctr++);
@@ -1125,7 +1197,8 @@ namespace rbps_gpu
             const uint2 e = E.nlist[i];
             const WorldDev W = E.worlds[e.x];
             uint32_t n_gjk = 0;
-            narrow_candidate(E, W, E.wcand[e.x][e.y], E.wcc[e.x][e.y], n_gjk);
+            if (narrow_candidate(E, W, E.wcand[e.x][e.y], E.wcc[e.x][e.y]) == kNeedsGjk)
+                queue_gjk(E, e.x, e.y, n_gjk);
             if (n_gjk)
                 atomicAdd(world_scratch(E, W).misc + kMiscNGjk, n_gjk);
         }
@@ -1451,7 +1524,10 @@ namespace rbps_gpu
         k_type_scatter<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
         for (int s = 0; s < e.substeps; ++s)
         {
+            if (e.gjk_list)
+                cudaMemsetAsync(e.gjk_count, 0, 4, stream);
             k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+            launch_gjk(e, stream);
             k_substep<T, P><<<fl.grid_solve, 128, e.mask_words * sizeof(unsigned long long), stream>>>(e);
         }
         k_phase_stats<T, P><<<pl.grid[kKStats], pl.block[kKStats], 0, stream>>>(e, 1);
@@ -1509,10 +1585,6 @@ namespace rbps_gpu
                                                           const rbps_gpu::FlatLaunch &, cudaStream_t);              \
     template cudaError_t rbps_gpu::occupancy_flat<T, P>(int, int, int *, size_t);                                          \
     template cudaError_t rbps_gpu::occupancy_big<T, P>(int, int *);                                               \
-    template cudaError_t rbps_gpu::launch_collide<T, P>(const rbps_gpu::ShapeDev *, const double *,               \
-                                                       const rbps_gpu::ShapeDev *, const double *,               \
-                                                       const rbps_gpu::HullSetDev &, uint32_t,                   \
-                                                       rbps_gpu::CollideOut *, cudaStream_t);                    \
     template cudaError_t rbps_gpu::launch_debug_broadphase<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int,    \
                                                                  uint32_t *, cudaStream_t);                         \
     template cudaError_t rbps_gpu::launch_io<T, P>(const rbps_gpu::Engine<T, P> &, int, double *, double *,       \
@@ -1583,56 +1655,4 @@ namespace rbps_gpu
         return cudaGetLastError();
     }
 
-    // rbc::dispatch (Dispatcher.hpp:208-213) on independent shape pairs, one
-    // thread per pair; transforms are 7 doubles (position, quaternion wxyz).
-    template <class T, class P>
-    __global__ void k_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
-                              const HullSetDev hulls, uint32_t n, CollideOut *out)
-    {
-        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= n)
-            return;
-        auto load_tf = [](const double *p) {
-            tf<T> t;
-            t.pos = vec3<T>(T(p[0]), T(p[1]), T(p[2]));
-            t.rot = quat<T>(T(p[3]), T(p[4]), T(p[5]), T(p[6]));
-            return t;
-        };
-        const tf<T> a = load_tf(ta + 7 * (size_t)i), b = load_tf(tb + 7 * (size_t)i);
-        Manifold<T> m;
-        m.n = 0;
-        const int res = dispatch_pair(sa[i], a, sb[i], b, hulls, m);
-        CollideOut o;
-        o.status = res;
-        o.n_points = res == kHit ? m.n : 0;
-        o.normal[0] = o.normal[1] = o.normal[2] = 0.0;
-        for (int k = 0; k < 4; ++k)
-        {
-            o.depth[k] = 0.0;
-            o.position[k][0] = o.position[k][1] = o.position[k][2] = 0.0;
-        }
-        if (res == kHit)
-        {
-            o.normal[0] = double(m.normal.x);
-            o.normal[1] = double(m.normal.y);
-            o.normal[2] = double(m.normal.z);
-            for (int k = 0; k < m.n && k < 4; ++k)
-            {
-                o.position[k][0] = double(m.pos[k].x);
-                o.position[k][1] = double(m.pos[k].y);
-                o.position[k][2] = double(m.pos[k].z);
-                o.depth[k] = double(m.depth[k]);
-            }
-        }
-        out[i] = o;
-    }
-
-    template <class T, class P>
-    cudaError_t launch_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
-                               const HullSetDev &hulls, uint32_t n, CollideOut *out, cudaStream_t stream)
-    {
-        if (n)
-            k_collide<T, P><<<(n + 127) / 128, 128, 0, stream>>>(sa, ta, sb, tb, hulls, n, out);
-        return cudaGetLastError();
-    }
 } // namespace rbps_gpu

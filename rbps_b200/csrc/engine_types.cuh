@@ -211,6 +211,12 @@ namespace rbps_gpu
         uint32_t *dump_color;
         uint32_t dump_pair_cap, dump_cand_cap;
         unsigned long long *prof; // phase timers, kProfSlots per world (null = off)
+        // GJK pass (batches with hull colliders): queued (world, candidate)
+        // pairs of the current substep and one workspace per k_gjk thread
+        uint2 *gjk_list;
+        uint32_t *gjk_count;
+        uint32_t gjk_cap, gjk_slots;
+        void *gjk_ws;
         // flat colored pipeline over all small worlds (see engine_impl.cuh)
         uint32_t *wcoff;               // n_small + 1: candidate prefix over small_worlds
         uint32_t *gcol;                // global colour bookkeeping, kGcolWords
@@ -280,7 +286,14 @@ namespace rbps_gpu
     };
     template <class T, class P>
     cudaError_t launch_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
-                               const HullSetDev &hulls, uint32_t n, CollideOut *out, cudaStream_t stream);
+                               const HullSetDev &hulls, uint32_t n, CollideOut *out, void *gjk_ws, uint32_t threads,
+                               int *err, cudaStream_t stream);
+    // bytes of one GJK / EPA / manifold workspace in precision T
+    template <class T, class P>
+    size_t gjk_work_bytes();
+    // the GJK pass over the pairs the narrowphase queued (no-op without hulls)
+    template <class T, class P>
+    cudaError_t launch_gjk(const Engine<T, P> &e, cudaStream_t stream);
     template <class T, class P>
     cudaError_t launch_debug_broadphase(const Engine<T, P> &e, uint32_t world, int block, uint32_t *out,
                                         cudaStream_t stream);

@@ -28,11 +28,26 @@ namespace rbps_gpu
     };
 
     // Hull geometry of one batch: vertices (double, local frame) per hull.
+    // Bases of one hull's polygon / adjacency tables (ConvexHullData,
+    // ConvexHull.hpp:60-98) in HullSetDev::u32 and poly_n; np = polygons
+    // (0: no tables, the manifold is one EPA point).
+    struct HullDesc
+    {
+        uint32_t np;
+        uint32_t po, pi, pn;     // polygon offsets (np + 1), indices, first normal
+        uint32_t v2p_o, v2p_i;   // vertex -> polygons (offsets: vertices + 1)
+        uint32_t v2n_o, v2n_i;   // vertex -> neighbours
+        uint32_t p2p_o, p2p_i;   // polygon -> polygons (offsets: np + 1)
+    };
+
     struct HullSetDev
     {
-        const double *verts;     // 3 per vertex
-        const uint32_t *v_off;   // n_hulls + 1
+        const double *verts;      // 3 per vertex
+        const uint32_t *v_off;    // n_hulls + 1
         const double *local_aabb; // 6 per hull
+        const HullDesc *desc;     // per hull
+        const uint32_t *u32;      // all index tables
+        const double *poly_n;     // 3 per polygon
     };
 
     struct ShapeDev

@@ -364,3 +364,42 @@ def capsule_world(seed=0, n=48, friction=0.5, restitution=0.0):
         forces.append(f)
         colliders.append(c)
     return _finish(bodies, forces, colliders, [])
+
+
+def hull_world(seed=0, n=24, n_shapes=4, friction=0.5, restitution=0.0):
+    """Ground plane + convex hulls, boxes and spheres dropped close to the
+    ground (exercises GJK / EPA and the hull manifolds).  Hull shapes are the
+    quickhull of 16-32 points on ellipsoids with semi-axes U[0.2, 0.6]; hull
+    mass and inertia from the closed mesh about the vertex origin."""
+    import rbps_b200
+    rng = np.random.Generator(np.random.PCG64(seed))
+    hulls = []
+    for k in range(n_shapes):
+        m = int(rng.integers(16, 33))
+        d = rng.standard_normal((m, 3))
+        pts = d / np.linalg.norm(d, axis=1, keepdims=True) * rng.uniform(0.2, 0.6, 3)
+        hulls.append((pts, rbps_b200.quickhull(pts)))
+    bodies, forces, colliders = [], [], []
+    _ground(bodies, colliders, forces, friction, restitution)
+    kind = rng.integers(0, 4, n)
+    quats = random_quats(rng, n)
+    pos = rng.uniform((-2.0, 0.6, -2.0), (2.0, 3.0, 2.0), (n, 3))
+    for i in range(n):
+        bid = len(bodies)
+        if kind[i] <= 1:
+            h = int(rng.integers(0, n_shapes))
+            m, inertia = hull_mass(hulls[h][0], hulls[h][1])
+            c = _collider(abi.SHAPE_CONVEX_HULL, [], bid, friction, restitution, hull=h)
+        elif kind[i] == 2:
+            h = rng.uniform(0.2, 0.4, 3)
+            m, inertia = box_mass(h)
+            c = _collider(abi.SHAPE_BOX, h, bid, friction, restitution)
+        else:
+            r = rng.uniform(0.2, 0.4)
+            m, inertia = sphere_mass(r)
+            c = _collider(abi.SHAPE_SPHERE, [r], bid, friction, restitution)
+        b, f = _dyn_body(pos[i], quats[i], m, inertia)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(c)
+    return _finish(bodies, forces, colliders, [], hulls)

@@ -20,8 +20,30 @@ CUBE_VERTS = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
                        [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], np.float64)
 CUBE_FACES = np.array([[0, 1, 2], [0, 2, 3], [4, 6, 5], [4, 7, 6], [0, 5, 1], [0, 4, 5],
                        [2, 6, 3], [3, 6, 7], [0, 3, 7], [0, 7, 4], [1, 5, 6], [1, 6, 2]], np.uint32)
-HULLS = {"tet": (TET_VERTS, TET_FACES), "cube": (CUBE_VERTS, CUBE_FACES)}
-HULL_IDS = {"tet": 0, "cube": 1}
+
+def _ellipsoid_hull(seed, n, axes):
+    """n points uniform on an ellipsoid surface and their hull triangles
+    (from a fixed point set, so the fixture does not depend on a build)."""
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    return d / np.linalg.norm(d, axis=1, keepdims=True) * np.asarray(axes)
+
+
+ELLIPSOID_A = _ellipsoid_hull(21, 16, (0.5, 0.3, 0.4))
+ELLIPSOID_B = _ellipsoid_hull(22, 24, (0.35, 0.5, 0.3))
+HULLS = {"tet": (TET_VERTS, TET_FACES), "cube": (CUBE_VERTS, CUBE_FACES),
+         "ellA": (ELLIPSOID_A, None), "ellB": (ELLIPSOID_B, None)}
+HULL_IDS = {"tet": 0, "cube": 1, "ellA": 2, "ellB": 3}
+
+
+def hull_list():
+    """[(verts, tris)] in HULL_IDS order; ellipsoid triangles from quickhull."""
+    import rbps_b200
+    out = []
+    for name in sorted(HULL_IDS, key=HULL_IDS.get):
+        v, t = HULLS[name]
+        out.append((v, t if t is not None else rbps_b200.quickhull(v)))
+    return out
 
 
 def sphere(r):
@@ -211,6 +233,8 @@ def random_quats(rng, n):
 
 
 ANALYTIC_KINDS = ("sphere", "box", "capsule")
+HULL_NAMES = ("tet", "cube", "ellA", "ellB")
+# hull scale: the fixture tet / cube span [-1, 1]; the ellipsoids ~0.5
 
 
 def random_shape(rng, kind):
@@ -232,14 +256,14 @@ def random_pairs(seed, kind_a, kind_b, n, spread=1.2):
     qa = random_quats(rng, n)
     qb = random_quats(rng, n)
     for i in range(n):
-        a = random_shape(rng, kind_a) if kind_a != "hull" else hull("cube" if i % 2 else "tet")
+        a = random_shape(rng, kind_a) if kind_a != "hull" else hull(HULL_NAMES[i % 4])
         if kind_b == "plane":
             b = plane(0, 1, 0, 0)
             pa = (rng.uniform(-2, 2), rng.uniform(-0.6, 1.2), rng.uniform(-2, 2))
             pb = (0.0, 0.0, 0.0)
             qbi = (1.0, 0.0, 0.0, 0.0)
         else:
-            b = random_shape(rng, kind_b)
+            b = random_shape(rng, kind_b) if kind_b != "hull" else hull(HULL_NAMES[(i // 4) % 4])
             pa = tuple(rng.uniform(-3, 3, 3))
             d = rng.normal(size=3)
             d /= np.linalg.norm(d)

@@ -259,3 +259,46 @@ def test_random_sequences(ref, seed):
         b.update()
         for h in live:
             b.fat_equal(h)
+
+
+def _hull_cases():
+    import narrow_cases as NC
+    import rbps_b200
+    rng = np.random.default_rng(11)
+    cases = [("tet", NC.TET_VERTS, NC.TET_FACES), ("cube", NC.CUBE_VERTS, NC.CUBE_FACES)]
+    for k, n in enumerate((8, 16, 24, 32)):
+        d = rng.normal(size=(n, 3))
+        pts = d / np.linalg.norm(d, axis=1, keepdims=True) * rng.uniform(0.2, 1.0, 3)
+        cases.append((f"ellipsoid{n}", pts, rbps_b200.quickhull(pts)))
+    # a box as a point cloud: quickhull splits each face into triangles that must merge back
+    corners = np.array([[x, y, z] for x in (-0.3, 0.3) for y in (-0.5, 0.5) for z in (-0.2, 0.2)])
+    cases.append(("box_cloud", corners, rbps_b200.quickhull(corners)))
+    # a hexagonal prism: faces of 6 vertices
+    ang = np.arange(6) * np.pi / 3
+    ring = np.stack([np.cos(ang), np.zeros(6), np.sin(ang)], 1)
+    prism = np.vstack([ring + [0, -0.4, 0], ring + [0, 0.4, 0]])
+    cases.append(("hex_prism", prism, rbps_b200.quickhull(prism)))
+    return cases
+
+
+def test_hull_tables_match_reference(ref):
+    """The library's polygon / adjacency tables (the restatement of
+    convex_hull_data_create, ConvexHull.hpp:149-420) equal the reference's."""
+    import rbps_b200
+    from rbps_b200 import abi, scenes
+    cases = _hull_cases()
+    b = np.zeros(1, abi.BODY_DT)
+    b[0] = abi.body_default()
+    spec = scenes.WorldSpec(b, np.zeros((1, 3)), np.zeros(0, abi.COLLIDER_DT), np.zeros(0, abi.JOINT_DT),
+                            [(v, t) for _, v, t in cases])
+    rw = ref.RefWorld(spec, 1 / 60, 1)
+    for hid, (name, verts, tris) in enumerate(cases):
+        mine = rbps_b200.hull_tables(verts, tris)
+        theirs = rw.hull_tables(hid)
+        nv = len(verts)
+        assert len(theirs["poly_offsets"]) > 1, name
+        for key in ("poly_offsets", "poly_indices", "p2p_offsets", "p2p_indices", "v2p_indices", "v2n_indices"):
+            np.testing.assert_array_equal(mine[key], theirs[key], err_msg=f"{name}.{key}")
+        for key in ("v2p_offsets", "v2n_offsets"):
+            np.testing.assert_array_equal(mine[key][:nv + 1], theirs[key][:nv + 1], err_msg=f"{name}.{key}")
+        np.testing.assert_array_equal(mine["poly_normals"], theirs["poly_normals"], err_msg=f"{name}.normals")
