@@ -349,7 +349,8 @@ struct rbps_batch
     uint32_t *wcoff = nullptr, *gcol = nullptr, *sbodies = nullptr, *sjoints = nullptr, *sjcoff = nullptr;
     uint2 *nlist = nullptr;
     void **wcand = nullptr, **wcc = nullptr;
-    uint32_t n_sbodies = 0, n_sjoints = 0, n_sjcolors = 0, n_block_worlds = 0, mask_words = 0;
+    uint32_t n_sbodies = 0, n_sjoints = 0, n_sjcolors = 0, n_block_worlds = 0;
+    uint32_t smem_cap_block = 0, smem_cap_warp = 0;
     int grid_big = 0;
     uint32_t n_counters = 0;  // phase work counters per step
     uint64_t total_bodies = 0, total_dynamic = 0;
@@ -703,7 +704,8 @@ namespace
         e.small_worlds = b->small_list;
         e.n_small = (uint32_t)b->small_ids.size();
         e.n_block_worlds = b->n_block_worlds;
-        e.mask_words = b->mask_words;
+        e.smem_cap_block = b->smem_cap_block;
+        e.smem_cap_warp = b->smem_cap_warp;
         e.dump_pairs = b->dump ? b->dump_pairs : nullptr;
         e.dump_cand = b->dump ? b->dump_cand : nullptr;
         e.dump_cc = b->dump ? (CandContacts<T, P> *)b->dump_cc : nullptr;
@@ -737,8 +739,8 @@ namespace
 
     constexpr uint32_t kSmallWorldBodies = 4096;
     constexpr int kMaxBlockHost = 256; // block of the flat kernels (their __launch_bounds__)
-    constexpr uint32_t kBlockTeamBodies = 160; // colored batches: worlds this large step on a whole CTA
-    constexpr uint32_t kMaskWordsMax = 2048;    // shared colour-mask words per substep CTA (16 KB)
+    constexpr uint32_t kBlockTeamBodies = 128; // colored batches: worlds this large step on a whole CTA
+    constexpr uint32_t kSmemBodiesMax = 1024;   // bodies a CTA world keeps in shared memory (137 KB in FP32)
 } // namespace
 
 template <class T, class P>
@@ -1229,12 +1231,16 @@ static int commit_typed(rbps_batch *b)
             ++nbw;
         b->n_block_worlds = nbw;
         b->flat.grid_solve = (int)(nbw + (ns - nbw + 3) / 4);
-        // shared colour masks: the largest CTA world, or four warp worlds
-        // (larger worlds fall back to their global mask array)
-        uint32_t words = 4 * kBlockTeamBodies;
+        // shared-memory world copies: the largest CTA world, or four warp
+        // worlds (a world beyond its cap runs on the batch arrays)
+        auto round16 = [](uint32_t x) { return (x + 15u) / 16u * 16u; };
+        b->smem_cap_warp = round16(kBlockTeamBodies);
+        b->smem_cap_block = 0;
         if (nbw)
-            words = std::max(words, std::min<uint32_t>(b->wdev[b->small_ids[0]].n_bodies, kMaskWordsMax));
-        b->mask_words = words;
+            b->smem_cap_block = round16(std::min<uint32_t>(b->wdev[b->small_ids[0]].n_bodies, kSmemBodiesMax));
+        b->flat.substep_smem = std::max(4 * smem_world_bytes<T, P>(b->smem_cap_warp),
+                                        smem_world_bytes<T, P>(b->smem_cap_block));
+        CU(prepare_substep<T, P>(b->flat.substep_smem));
         b->use_flat = true;
     }
     // ---- GJK pass: only batches with hull colliders reach it

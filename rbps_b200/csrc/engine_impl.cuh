@@ -560,7 +560,7 @@ namespace rbps_gpu
     // All contact rows of one candidate pair (global bodies ba, bb), in list
     // order, with both bodies in registers (load once, relax, store once).
     template <class T, class P>
-    __device__ __forceinline__ void solve_pair_position(const Engine<T, P> &E, uint32_t ba, uint32_t bb,
+    __device__ __forceinline__ void solve_pair_position(const Bodies<T, P> &B, T inv_h, uint32_t ba, uint32_t bb,
                                                         CandContacts<T, P> &cc)
     {
         const int n = cc.n;
@@ -569,16 +569,16 @@ namespace rbps_gpu
         const vec3<T> nrm = v3(cc.normal);
         const T sf = cc.mat.y;
         BodyR<T, P> A, Bb;
-        load_body(E.B, ba, A, true);
-        load_body(E.B, bb, Bb, true);
+        load_body(B, ba, A, true);
+        load_body(B, bb, Bb, true);
         for (int k = 0; k < n; ++k)
-            contact_position(A, Bb, nrm, sf, cc.pt[k], E.inv_h);
-        store_pose(E.B, ba, A);
-        store_pose(E.B, bb, Bb);
+            contact_position(A, Bb, nrm, sf, cc.pt[k], inv_h);
+        store_pose(B, ba, A);
+        store_pose(B, bb, Bb);
     }
 
     template <class T, class P>
-    __device__ __forceinline__ void solve_pair_velocity(const Engine<T, P> &E, uint32_t ba, uint32_t bb,
+    __device__ __forceinline__ void solve_pair_velocity(const Bodies<T, P> &B, T h, uint32_t ba, uint32_t bb,
                                                         const CandContacts<T, P> &cc)
     {
         const int n = cc.n;
@@ -586,26 +586,26 @@ namespace rbps_gpu
             return;
         const vec3<T> nrm = v3(cc.normal);
         BodyR<T, P> A, Bb;
-        load_body(E.B, ba, A, false);
-        load_body(E.B, bb, Bb, false);
+        load_body(B, ba, A, false);
+        load_body(B, bb, Bb, false);
         for (int k = 0; k < n; ++k)
-            contact_velocity(A, Bb, nrm, cc.mat.x, cc.mat.z, cc.pt[k], E.h);
-        store_vel(E.B, ba, A);
-        store_vel(E.B, bb, Bb);
+            contact_velocity(A, Bb, nrm, cc.mat.x, cc.mat.z, cc.pt[k], h);
+        store_vel(B, ba, A);
+        store_vel(B, bb, Bb);
     }
 
     template <class T, class P>
     __device__ __forceinline__ void solve_cand_position(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
                                                         CandContacts<T, P> &cc)
     {
-        solve_pair_position(E, W.body_off + cd.ba, W.body_off + cd.bb, cc);
+        solve_pair_position(E.B, E.inv_h, W.body_off + cd.ba, W.body_off + cd.bb, cc);
     }
 
     template <class T, class P>
     __device__ __forceinline__ void solve_cand_velocity(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
                                                         const CandContacts<T, P> &cc)
     {
-        solve_pair_velocity(E, W.body_off + cd.ba, W.body_off + cd.bb, cc);
+        solve_pair_velocity(E.B, E.h, W.body_off + cd.ba, W.body_off + cd.bb, cc);
     }
 
     template <class T, class P>
@@ -747,30 +747,40 @@ namespace rbps_gpu
     }
 
     // Position solve (World.hpp:168-173): contacts, joint errors, joint rows;
-    // then the velocity update (Body.cpp:41-57).
+    // then the velocity update (Body.cpp:41-57).  B is the body view the
+    // team works on and boff the view index of the world's body 0
+    // (W.body_off for the batch arrays, 0 for a shared-memory copy).
     template <class T, class P, class Team>
-    __device__ void phase_position(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    __device__ void phase_position_on(const Engine<T, P> &E, const Team &tm, uint32_t w, const Bodies<T, P> &B,
+                                      uint32_t boff, const uint32_t *book = nullptr)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
         PhaseClock clk(prof_slots(E, tm, w), false);
-        const Bodies<T, P> &B = E.B;
+        const uint32_t shift = W.body_off - boff; // joint body ids are batch-global
         const uint32_t n_cand = S.misc[kMiscNCand];
         if (E.solve_mode != 1)
         {
             if (tm.leader())
             {
                 for (uint32_t c = 0; c < n_cand; ++c)
-                    solve_cand_position(E, W, S.cand[c], S.cc[c]);
+                {
+                    const Cand cd = S.cand[c];
+                    solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                }
                 for (uint32_t j = 0; j < W.n_joints; ++j)
                 {
                     Joint<T> jt = E.joints[W.joint_off + j];
+                    jt.b1 -= shift;
+                    jt.b2 -= shift;
                     joint_errors(B, jt, joint_rows(E, jt), E.h);
                     E.joints[W.joint_off + j].target_pos = jt.target_pos;
                 }
                 for (uint32_t j = 0; j < W.n_joints; ++j)
                 {
-                    const Joint<T> &jt = E.joints[W.joint_off + j];
+                    Joint<T> jt = E.joints[W.joint_off + j];
+                    jt.b1 -= shift;
+                    jt.b2 -= shift;
                     solve_joint_rows(B, jt, joint_rows(E, jt), E.inv_h);
                 }
             }
@@ -779,14 +789,15 @@ namespace rbps_gpu
         }
         else
         {
-            const uint32_t *coff = S.misc + kMiscCOff;
-            const uint32_t n_colors = S.misc[kMiscNColors];
+            const uint32_t *coff = book ? book + 66 : S.misc + kMiscCOff;
+            const uint32_t n_colors = book ? book[132] : S.misc[kMiscNColors];
             for (uint32_t col = 0; col < n_colors; ++col)
             {
                 for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
                 {
                     const uint32_t c = S.corder[q];
-                    solve_cand_position(E, W, S.cand[c], S.cc[c]);
+                    const Cand cd = S.cand[c];
+                    solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
                 }
                 tm.sync();
             }
@@ -796,7 +807,8 @@ namespace rbps_gpu
                     for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
                     {
                         const uint32_t c = S.corder[q];
-                        solve_cand_position(E, W, S.cand[c], S.cc[c]);
+                        const Cand cd = S.cand[c];
+                        solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
                     }
                 tm.sync();
             }
@@ -806,6 +818,8 @@ namespace rbps_gpu
                 for (uint32_t j = tm.rank(); j < W.n_joints; j += tm.size())
                 {
                     Joint<T> jt = E.joints[W.joint_off + j];
+                    jt.b1 -= shift;
+                    jt.b2 -= shift;
                     joint_errors(B, jt, joint_rows(E, jt), E.h);
                     E.joints[W.joint_off + j].target_pos = jt.target_pos;
                 }
@@ -815,7 +829,9 @@ namespace rbps_gpu
                 {
                     for (uint32_t q = jco[jc] + tm.rank(); q < jco[jc + 1]; q += tm.size())
                     {
-                        const Joint<T> &jt = E.joints[W.joint_off + E.jorder[q]];
+                        Joint<T> jt = E.joints[W.joint_off + E.jorder[q]];
+                        jt.b1 -= shift;
+                        jt.b2 -= shift;
                         solve_joint_rows(B, jt, joint_rows(E, jt), E.inv_h);
                     }
                     tm.sync();
@@ -824,41 +840,57 @@ namespace rbps_gpu
             clk.mark(kPhJointPos);
         }
         for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
-            update_velocity_body(B, W.body_off + b, E.inv_h);
+            update_velocity_body(B, boff + b, E.inv_h);
         tm.sync();
         clk.mark(kPhVelUpdate);
     }
 
+    template <class T, class P, class Team>
+    __device__ void phase_position(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    {
+        phase_position_on(E, tm, w, E.B, E.worlds[w].body_off);
+    }
+
     // Velocity solve (World.hpp:176-180): restitution / friction, joint damping.
     template <class T, class P, class Team>
-    __device__ void phase_velocity(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    __device__ void phase_velocity_on(const Engine<T, P> &E, const Team &tm, uint32_t w, const Bodies<T, P> &B,
+                                      uint32_t boff, const uint32_t *book = nullptr)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
         PhaseClock clk(prof_slots(E, tm, w), false);
-        const Bodies<T, P> &B = E.B;
+        const uint32_t shift = W.body_off - boff;
         if (E.solve_mode != 1)
         {
             if (tm.leader())
             {
                 const uint32_t n_cand = S.misc[kMiscNCand];
                 for (uint32_t c = 0; c < n_cand; ++c)
-                    solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
+                {
+                    const Cand cd = S.cand[c];
+                    solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                }
                 for (uint32_t j = 0; j < W.n_joints; ++j)
-                    joint_damping(B, E.joints[W.joint_off + j], E.h);
+                {
+                    Joint<T> jt = E.joints[W.joint_off + j];
+                    jt.b1 -= shift;
+                    jt.b2 -= shift;
+                    joint_damping(B, jt, E.h);
+                }
             }
             tm.sync();
         }
         else
         {
-            const uint32_t *coff = S.misc + kMiscCOff;
-            const uint32_t n_colors = S.misc[kMiscNColors];
+            const uint32_t *coff = book ? book + 66 : S.misc + kMiscCOff;
+            const uint32_t n_colors = book ? book[132] : S.misc[kMiscNColors];
             for (uint32_t col = 0; col < n_colors; ++col)
             {
                 for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
                 {
                     const uint32_t c = S.corder[q];
-                    solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
+                    const Cand cd = S.cand[c];
+                    solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
                 }
                 tm.sync();
             }
@@ -868,7 +900,8 @@ namespace rbps_gpu
                     for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
                     {
                         const uint32_t c = S.corder[q];
-                        solve_cand_velocity(E, W, S.cand[c], S.cc[c]);
+                        const Cand cd = S.cand[c];
+                        solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
                     }
                 tm.sync();
             }
@@ -876,11 +909,22 @@ namespace rbps_gpu
             for (uint32_t jc = 0; jc < W.n_jcolors; ++jc)
             {
                 for (uint32_t q = jco[jc] + tm.rank(); q < jco[jc + 1]; q += tm.size())
-                    joint_damping(B, E.joints[W.joint_off + E.jorder[q]], E.h);
+                {
+                    Joint<T> jt = E.joints[W.joint_off + E.jorder[q]];
+                    jt.b1 -= shift;
+                    jt.b2 -= shift;
+                    joint_damping(B, jt, E.h);
+                }
                 tm.sync();
             }
         }
         clk.mark(kPhVelSolve);
+    }
+
+    template <class T, class P, class Team>
+    __device__ void phase_velocity(const Engine<T, P> &E, const Team &tm, uint32_t w)
+    {
+        phase_velocity_on(E, tm, w, E.B, E.worlds[w].body_off);
     }
 
     // Statistics and parity dumps of the last substep.
@@ -1388,16 +1432,20 @@ namespace rbps_gpu
     // colours to every thread.
     template <class T, class P, class Team>
     __device__ uint32_t greedy_color_world(const Engine<T, P> &E, const Team &tm, uint32_t w,
-                                           unsigned long long *mask, BlockShared &sh)
+                                           unsigned long long *mask, BlockShared &sh, uint32_t *book)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
         uint32_t *misc = S.misc;
+        // colour counts / fill cursors and offsets: the team's shared block
+        // when it has one, else the world's misc words
+        uint32_t *cnt = book ? book : misc + kMiscCCount;
+        uint32_t *off = book ? book + 66 : misc + kMiscCOff;
         const uint32_t n_cand = misc[kMiscNCand];
         for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
             mask[b] = 0ull;
         for (uint32_t k = tm.rank(); k < 66; k += tm.size())
-            misc[kMiscCCount + k] = 0u;
+            cnt[k] = 0u;
         const uint32_t n_act = compact_active(tm, S, n_cand, sh);
         tm.sync();
         if (tm.leader())
@@ -1434,33 +1482,38 @@ namespace rbps_gpu
                                 mask[cd[k].bb] |= bit;
                         }
                         S.color[cs[k]] = col;
-                        misc[kMiscCCount + col] += 1u;
+                        cnt[col] += 1u;
                     }
             }
             uint32_t run = 0, ncol = 0;
             for (uint32_t k = 0; k <= kColorSerial; ++k)
             {
-                const uint32_t n = misc[kMiscCCount + k];
-                misc[kMiscCOff + k] = run;
-                misc[kMiscCCount + k] = run; // becomes the fill cursor
+                const uint32_t n = cnt[k];
+                off[k] = run;
+                cnt[k] = run; // becomes the fill cursor
                 if (n && k < kColorSerial)
                     ncol = k + 1;
                 run += n;
             }
-            misc[kMiscCOff + kColorSerial + 1] = run;
+            off[kColorSerial + 1] = run;
             misc[kMiscNColors] = ncol;
             if (ncol > misc[kMiscMaxColors])
                 misc[kMiscMaxColors] = ncol;
+            if (book)
+                book[132] = ncol;
         }
         tm.sync();
         for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
         {
             const uint32_t c = S.alist[q];
-            const uint32_t slot = atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
+            const uint32_t slot = atomicAdd(&cnt[S.color[c]], 1u);
             S.corder[slot] = c;
         }
+        if (book) // the offsets also go to misc for the statistics and dumps
+            for (uint32_t k = tm.rank(); k < 66; k += tm.size())
+                misc[kMiscCOff + k] = off[k];
         tm.sync();
-        return misc[kMiscNColors];
+        return book ? book[132] : misc[kMiscNColors];
     }
 
 #ifndef RBPS_SUBSTEP_MIN_BLOCKS
@@ -1471,46 +1524,151 @@ namespace rbps_gpu
     // The largest worlds (the first n_block_worlds of the list) get a whole
     // CTA each; the others one warp each, four per CTA.  Worlds progress
     // independently: a barrier is the team's own.
+    // A team's copy of its world in shared memory: 136 words of colour
+    // bookkeeping (counts / cursors, offsets, colour count), then per body
+    // the colour mask, pose, previous pose and velocities, and the type;
+    // `cap` bodies per array (cap a multiple of 16 keeps every array 16-byte
+    // aligned).  Force, torque and the inertia tensors are read in place
+    // through the batch arrays offset to the world.
+    template <class T, class P>
+    struct SmemWorld
+    {
+        static constexpr size_t kBook = 136 * sizeof(uint32_t);
+        static constexpr size_t kPerBody =
+            sizeof(unsigned long long) + 2 * sizeof(V4<P>) + 2 * sizeof(Q4<T>) + 2 * sizeof(V4<T>) + 1;
+
+        __host__ __device__ static size_t bytes(uint32_t cap) { return kBook + (size_t)cap * kPerBody; }
+
+        __device__ static Bodies<T, P> view(unsigned char *p, uint32_t cap, const Bodies<T, P> &G, uint32_t body_off,
+                                            unsigned long long **mask, uint32_t **book)
+        {
+            *book = reinterpret_cast<uint32_t *>(p);
+            p += kBook;
+            *mask = reinterpret_cast<unsigned long long *>(p);
+            p += (size_t)cap * sizeof(unsigned long long);
+            Bodies<T, P> V;
+            V.pos = reinterpret_cast<V4<P> *>(p);
+            p += (size_t)cap * sizeof(V4<P>);
+            V.prev_pos = reinterpret_cast<V4<P> *>(p);
+            p += (size_t)cap * sizeof(V4<P>);
+            V.rot = reinterpret_cast<Q4<T> *>(p);
+            p += (size_t)cap * sizeof(Q4<T>);
+            V.prev_rot = reinterpret_cast<Q4<T> *>(p);
+            p += (size_t)cap * sizeof(Q4<T>);
+            V.lin = reinterpret_cast<V4<T> *>(p);
+            p += (size_t)cap * sizeof(V4<T>);
+            V.ang = reinterpret_cast<V4<T> *>(p);
+            p += (size_t)cap * sizeof(V4<T>);
+            V.type = p;
+            V.force = G.force + body_off;
+            V.torque = G.torque + body_off;
+            V.inertia = G.inertia + body_off;
+            V.inv_inertia = G.inv_inertia + body_off;
+            return V;
+        }
+    };
+
+    // The rest of a substep for one world on team tm: colouring of the
+    // contacting candidates, integrate (Body.cpp:18-39), position solve +
+    // velocity update, velocity solve.  With `smem` (room for `cap` bodies)
+    // and a world that fits, the bodies live in shared memory for the whole
+    // substep and are written back once.
+    template <class T, class P, class Team>
+    __device__ void substep_world(const Engine<T, P> &E, const Team &tm, uint32_t w, unsigned char *smem,
+                                  uint32_t cap, BlockShared &sh)
+    {
+        const WorldDev W = E.worlds[w];
+        const bool local = smem && W.n_bodies <= cap;
+        unsigned long long *mask = nullptr;
+        uint32_t *book = nullptr;
+        Bodies<T, P> V = E.B;
+        uint32_t boff = W.body_off;
+        if (local)
+        {
+            V = SmemWorld<T, P>::view(smem, cap, E.B, W.body_off, &mask, &book);
+            boff = 0;
+        }
+        else
+            mask = world_scratch(E, W).bmask;
+        PhaseClock clk(prof_slots(E, tm, w), false);
+        greedy_color_world(E, tm, w, mask, sh, book);
+        clk.mark(kPhColor);
+        if (local)
+        {
+            const Bodies<T, P> &G = E.B;
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            {
+                const uint32_t g = W.body_off + b;
+                V.pos[b] = G.pos[g];
+                V.rot[b] = G.rot[g];
+                V.lin[b] = G.lin[g];
+                V.ang[b] = G.ang[g];
+                V.prev_pos[b] = G.prev_pos[g];
+                V.prev_rot[b] = G.prev_rot[g];
+                V.type[b] = G.type[g];
+            }
+            tm.sync();
+        }
+        for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            integrate_body(V, boff + b, E.h);
+        tm.sync();
+        clk.mark(kPhIntegrate);
+        phase_position_on(E, tm, w, V, boff, book);
+        phase_velocity_on(E, tm, w, V, boff, book);
+        if (local)
+        {
+            const Bodies<T, P> &G = E.B;
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            {
+                if (V.type[b] == kStatic)
+                    continue;
+                const uint32_t g = W.body_off + b;
+                G.pos[g] = V.pos[b];
+                G.rot[g] = V.rot[b];
+                G.lin[g] = V.lin[b];
+                G.ang[g] = V.ang[b];
+                G.prev_pos[g] = V.prev_pos[b];
+                G.prev_rot[g] = V.prev_rot[b];
+            }
+            tm.sync();
+        }
+    }
+
+    // The largest worlds (the first n_block_worlds of the list) get a whole
+    // CTA each; the others one warp each, four per CTA.  Worlds progress
+    // independently: a barrier is the team's own.  Dynamic shared memory:
+    // E.smem_cap_block bodies for a CTA world, or E.smem_cap_warp bodies for
+    // each of the four warp worlds.
     template <class T, class P>
     __global__ void __launch_bounds__(128, RBPS_SUBSTEP_MIN_BLOCKS) k_substep(const Engine<T, P> E)
     {
         __shared__ BlockShared sh;
-        extern __shared__ unsigned long long smask[]; // E.mask_words colour masks
+        extern __shared__ __align__(16) unsigned char smem[];
         if (blockIdx.x < E.n_block_worlds)
         {
             BlockTeam tm;
-            const uint32_t w = E.small_worlds[blockIdx.x];
-            const WorldDev W = E.worlds[w];
-            PhaseClock clk(prof_slots(E, tm, w), false);
-            greedy_color_world(E, tm, w, W.n_bodies <= E.mask_words ? smask : world_scratch(E, W).bmask, sh);
-            clk.mark(kPhColor);
-            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
-                integrate_body(E.B, W.body_off + b, E.h);
-            tm.sync();
-            clk.mark(kPhIntegrate);
-            phase_position(E, tm, w);
-            phase_velocity(E, tm, w);
+            substep_world(E, tm, E.small_worlds[blockIdx.x], smem, E.smem_cap_block, sh);
             return;
         }
         const uint32_t q = E.n_block_worlds + (blockIdx.x - E.n_block_worlds) * (blockDim.x >> 5) + warp_id();
         if (q >= E.n_small)
             return;
         WarpTeam tm;
-        const uint32_t w = E.small_worlds[q];
-        const WorldDev W = E.worlds[w];
-        {
-            PhaseClock clk(prof_slots(E, tm, w), false);
-            const uint32_t per_warp = E.mask_words / (blockDim.x >> 5);
-            greedy_color_world(E, tm, w,
-                               W.n_bodies <= per_warp ? smask + warp_id() * per_warp : world_scratch(E, W).bmask, sh);
-            clk.mark(kPhColor);
-            for (uint32_t b = tm.rank(); b < W.n_bodies; b += 32)
-                integrate_body(E.B, W.body_off + b, E.h);
-            __syncwarp();
-            clk.mark(kPhIntegrate);
-        }
-        phase_position(E, tm, w);
-        phase_velocity(E, tm, w);
+        substep_world(E, tm, E.small_worlds[q], smem + warp_id() * SmemWorld<T, P>::bytes(E.smem_cap_warp),
+                      E.smem_cap_warp, sh);
+    }
+
+    // Opens k_substep to `bytes` of dynamic shared memory.
+    template <class T, class P>
+    cudaError_t prepare_substep(size_t bytes)
+    {
+        return cudaFuncSetAttribute(k_substep<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    }
+
+    template <class T, class P>
+    size_t smem_world_bytes(uint32_t cap)
+    {
+        return SmemWorld<T, P>::bytes(cap);
     }
 
     template <class T, class P>
@@ -1528,7 +1686,7 @@ namespace rbps_gpu
                 cudaMemsetAsync(e.gjk_count, 0, 4, stream);
             k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
             launch_gjk(e, stream);
-            k_substep<T, P><<<fl.grid_solve, 128, e.mask_words * sizeof(unsigned long long), stream>>>(e);
+            k_substep<T, P><<<fl.grid_solve, 128, fl.substep_smem, stream>>>(e);
         }
         k_phase_stats<T, P><<<pl.grid[kKStats], pl.block[kKStats], 0, stream>>>(e, 1);
         return cudaGetLastError();
@@ -1580,6 +1738,8 @@ namespace rbps_gpu
     template cudaError_t rbps_gpu::launch_step_big<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int, int,        \
                                                          cudaStream_t);                                           \
     template cudaError_t rbps_gpu::occupancy_phase<T, P>(int, int, int *);                                         \
+    template cudaError_t rbps_gpu::prepare_substep<T, P>(size_t);                                                  \
+    template size_t rbps_gpu::smem_world_bytes<T, P>(uint32_t);                                                    \
     template cudaError_t rbps_gpu::launch_step_flat<T, P>(const rbps_gpu::Engine<T, P> &,                          \
                                                           const rbps_gpu::PhaseLaunch &,                            \
                                                           const rbps_gpu::FlatLaunch &, cudaStream_t);              \

@@ -203,7 +203,8 @@ namespace rbps_gpu
         const uint32_t *small_worlds;
         uint32_t n_small;
         uint32_t n_block_worlds;  // colored batches: the first n of small_worlds step on a whole CTA
-        uint32_t mask_words;      // colour-mask words of shared memory per substep CTA
+        uint32_t smem_cap_block;  // bodies a CTA world keeps in shared memory (colored substep)
+        uint32_t smem_cap_warp;   // bodies each warp world keeps in shared memory
         // parity dumps (null when disabled)
         uint32_t *dump_pairs;   // 2 * pair_cap per slot
         Cand *dump_cand;        // cand_cap per slot
@@ -261,12 +262,19 @@ namespace rbps_gpu
     struct FlatLaunch
     {
         int grid_narrow, grid_solve, block_solve;
+        size_t substep_smem; // dynamic shared memory of k_substep
     };
     template <class T, class P>
     cudaError_t launch_step_flat(const Engine<T, P> &e, const PhaseLaunch &pl, const FlatLaunch &fl,
                                  cudaStream_t stream);
     template <class T, class P>
     cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm, size_t dynamic_smem);
+    // k_substep's shared-memory world copies: bytes for `cap` bodies, and
+    // opening the kernel to a dynamic shared-memory size
+    template <class T, class P>
+    size_t smem_world_bytes(uint32_t cap);
+    template <class T, class P>
+    cudaError_t prepare_substep(size_t bytes);
     template <class T, class P>
     cudaError_t occupancy_phase(int kernel, int block, int *blocks_per_sm);
     template <class T, class P>
