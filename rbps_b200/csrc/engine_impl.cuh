@@ -151,11 +151,11 @@ namespace rbps_gpu
     template <class Team, class SC>
     __device__ __noinline__ uint32_t sap_sort_sweep(const Team &tm, const FatBox *fat, uint32_t *ep_key, uint32_t *ep_id,
                                        uint32_t *ep_pos, uint32_t nbp, uint32_t id_limit, uint32_t pair_cap,
-                                       int *error, const SC &S, BlockShared &sh)
+                                       int *error, const SC &S, BlockShared &sh, uint32_t *sort_smem = nullptr)
     {
         const uint32_t nep = 2 * nbp;
         // stable sort of the endpoints, previous order as the tie-break
-        team_radix_sort(tm, ep_key, ep_id, S.ep_k2, S.ep_v2, nep, 32, S.counts, S.tile_sums, sh);
+        team_sort_staged(tm, ep_key, ep_id, S.ep_k2, S.ep_v2, nep, 32, S.counts, S.tile_sums, sh, sort_smem);
         // inverse permutation
         for (uint32_t i = tm.rank(); i < nep; i += tm.size())
         {
@@ -221,7 +221,7 @@ namespace rbps_gpu
         tm.sync();
         // reference emission order: stable sort by the later opening position
         const int bits = nep > 1 ? 32 - __clz(nep - 1) : 1;
-        team_radix_sort(tm, S.pk, S.pv, S.pk2, S.pv2, total, bits, S.counts, S.tile_sums, sh);
+        team_sort_staged(tm, S.pk, S.pv, S.pk2, S.pv2, total, bits, S.counts, S.tile_sums, sh, sort_smem);
         for (uint32_t k = tm.rank(); k + 1 < total; k += tm.size())
             if (S.pk[k] > S.pk[k + 1])
                 set_error_at(error, kErrInternal, 5, k); // pair sort must leave the keys ordered
@@ -231,7 +231,7 @@ namespace rbps_gpu
 
     template <class T, class P, class Team>
     __device__ uint32_t broadphase(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
-                                   BlockShared &sh)
+                                   BlockShared &sh, uint32_t *sort_smem = nullptr)
     {
         const uint32_t nbp = W.n_bp;
         const uint32_t eb = 2 * W.bp_off;
@@ -271,7 +271,7 @@ namespace rbps_gpu
             ep_key[ep_pos[2 * o + 1]] = order_key(__double2float_rn(f1.mx.x));
         }
         tm.sync();
-        return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, 2 * nbp, W.pair_cap, E.error, S, sh);
+        return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, 2 * nbp, W.pair_cap, E.error, S, sh, sort_smem);
     }
 
     // Filtered SAP pairs followed by the plane candidates; returns the count.
@@ -679,7 +679,8 @@ namespace rbps_gpu
 
     // Frame (once per step): SAP object update, sort, sweep; candidate list.
     template <class T, class P, class Team>
-    __device__ void phase_frame(const Engine<T, P> &E, const Team &tm, uint32_t w, BlockShared &sh)
+    __device__ void phase_frame(const Engine<T, P> &E, const Team &tm, uint32_t w, BlockShared &sh,
+                                uint32_t *sort_smem = nullptr)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
@@ -689,7 +690,7 @@ namespace rbps_gpu
             S.misc[kMiscNGjk] = 0u;
             S.misc[kMiscMaxColors] = 0u;
         }
-        const uint32_t n_pairs = broadphase(E, tm, W, S, sh);
+        const uint32_t n_pairs = broadphase(E, tm, W, S, sh, sort_smem);
         clk.mark(kPhBroadphase);
         const uint32_t n_cand = build_candidates(E, tm, W, S, n_pairs, sh);
         if (tm.leader())
@@ -1014,8 +1015,10 @@ namespace rbps_gpu
     __global__ void __launch_bounds__(kMaxBlock) k_phase_frame(const Engine<T, P> E, uint32_t ctr)
     {
         __shared__ BlockShared sh;
+        __shared__ uint32_t sort_smem[kSmemSortWords];
         BlockTeam tm;
-        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr, [&](uint32_t w) { phase_frame(E, tm, w, sh); });
+        each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr,
+                         [&](uint32_t w) { phase_frame(E, tm, w, sh, sort_smem); });
     }
 
     template <class T, class P>

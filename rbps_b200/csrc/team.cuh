@@ -245,4 +245,48 @@ namespace rbps_gpu
             tm.sync();
         }
     }
+    // A sort staged in shared memory: a CTA team with `smem` (kSmemSortWords
+    // words) and at least 128 threads copies up to kSmemSortMax (key, value)
+    // pairs in, runs the same stable radix sort on the shared copies and
+    // copies the result back -- the same permutation as sorting in place,
+    // without a global-memory round trip per pass step.  Other teams and
+    // larger inputs sort in place.
+    constexpr uint32_t kSmemSortMax = 1536;
+    constexpr uint32_t kSmemSortCounts = 256 * (kSmemSortMax / 128);
+    constexpr uint32_t kSmemSortWords = 4 * kSmemSortMax + kSmemSortCounts + 64;
+
+    template <class Team>
+    __device__ __forceinline__ void team_sort_staged(const Team &tm, uint32_t *keys, uint32_t *vals, uint32_t *kt,
+                                                     uint32_t *vt, uint32_t n, int bits, uint32_t *counts,
+                                                     uint32_t *tile_sums, BlockShared &sh, uint32_t *)
+    {
+        team_radix_sort(tm, keys, vals, kt, vt, n, bits, counts, tile_sums, sh);
+    }
+
+    __device__ __forceinline__ void team_sort_staged(const BlockTeam &tm, uint32_t *keys, uint32_t *vals, uint32_t *kt,
+                                                     uint32_t *vt, uint32_t n, int bits, uint32_t *counts,
+                                                     uint32_t *tile_sums, BlockShared &sh, uint32_t *smem)
+    {
+        if (!smem || n > kSmemSortMax || blockDim.x < 128 || n <= 1)
+        {
+            team_radix_sort(tm, keys, vals, kt, vt, n, bits, counts, tile_sums, sh);
+            return;
+        }
+        uint32_t *ak = smem, *av = smem + kSmemSortMax;
+        uint32_t *bk = smem + 2 * kSmemSortMax, *bv = smem + 3 * kSmemSortMax;
+        uint32_t *sc = smem + 4 * kSmemSortMax, *st = sc + kSmemSortCounts;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            ak[i] = keys[i];
+            av[i] = vals[i];
+        }
+        __syncthreads();
+        team_radix_sort(tm, ak, av, bk, bv, n, bits, sc, st, sh);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            keys[i] = ak[i];
+            vals[i] = av[i];
+        }
+        __syncthreads();
+    }
 } // namespace rbps_gpu
