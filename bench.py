@@ -17,7 +17,13 @@ copies inside the timed region); `roofline` = the step kernel against the
 measured HBM copy bandwidth with the algorithmic byte model below;
 `cpu_baseline` = the reference engine (oracle/_ref, built from the
 reference's own sources) on a bounded sample of the same worlds, all host
-threads.  `--impl reference` times the reference CPU engine alone.
+threads; `plain_gpu` = the plain per-world GPU path (one batch per world,
+same colored solver) on a sample of the same worlds from the same state.
+`--impl reference` times the reference CPU engine alone.
+
+`--workload collision_stress` runs the single 65,536-body world of spheres,
+boxes, capsules and convex hulls instead (scenes.config1) and adds SAP pairs/s
+and GJK pairs/s to its line.
 """
 import argparse
 import json
@@ -173,6 +179,93 @@ def cpu_reference_run(scene, preroll, warmup, steps, max_seconds, threads):
     return value, info
 
 
+def plain_gpu_run(scene, batch, n_sample, steps, warmup, stream):
+    """The plain per-world GPU path on the same worlds: each world its own
+    batch with the same FP32 colored solver (one world per launch sequence,
+    no batching across worlds), the sample worlds stepped one after another
+    on the same stream.  Each plain world starts from the batched run's
+    current state, so both paths time the same regime.  Returns
+    (body-substeps/s, description)."""
+    import torch
+    import rbps_b200
+    from rbps_b200 import abi
+    idx = list(range(min(n_sample, len(scene.worlds))))
+    plain = []
+    for w in idx:
+        sub = type(scene)(scene.name, scene.timestep, scene.substeps, scene.steps, [scene.worlds[w]])
+        b = rbps_b200.Batch.from_scene(sub, abi.PRECISION_FP32, abi.SOLVE_COLORED, stream=stream.cuda_stream)
+        b.set_state(0, batch.state(w))
+        plain.append(b)
+    for b in plain:
+        b.step(warmup)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        for b in plain:
+            b.step(1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    n_dyn = sum(scene.worlds[w].n_dynamic for w in idx)
+    for b in plain:
+        b.close()
+    value = n_dyn * scene.substeps * steps / (ms / 1e3)
+    return value, (f"{len(idx)} of {len(scene.worlds)} worlds ({n_dyn} dynamic bodies), one batch per world, "
+                   f"FP32 colored, {warmup} untimed + {steps} timed steps from the batched state")
+
+
+def collision_stress(args, ws, rank, local):
+    """One world of 65,536 spheres, boxes, capsules and convex hulls over
+    200^3 m (scenes.config1), FP32 colored: K timed steps, each one SAP
+    frame and 10 substeps of narrowphase (GJK / EPA for the hull pairs) and
+    solve.  Reports body-substeps/s, SAP pairs/s and GJK pairs/s."""
+    import torch
+    import rbps_b200
+    from rbps_b200 import abi, scenes
+    torch.cuda.set_device(local)
+    scene = scenes.config1(seed=rank_seed(args.seed, rank))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    batch = rbps_b200.Batch.from_scene(scene, abi.PRECISION_FP32, abi.SOLVE_COLORED, device=local,
+                                       stream=stream.cuda_stream)
+    batch.step(args.warmup)
+    batch.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pairs = gjk = 0
+    ms = 0.0
+    for _ in range(args.steps):  # one step at a time: the per-step counters are read between steps
+        ev0.record(stream)
+        batch.step(1)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms += ev0.elapsed_time(ev1)
+        st = batch.stats()
+        pairs += st["pairs"]
+        gjk += st["gjk_pairs"]
+    batch.synchronize()
+    n_tot, n_dyn = batch.total_bodies()
+    ms = reduce_over_ranks(ms, "max", ws)
+    n_dyn_all = reduce_over_ranks(n_dyn, "sum", ws)
+    pairs_all = reduce_over_ranks(pairs, "sum", ws)
+    gjk_all = reduce_over_ranks(gjk, "sum", ws)
+    if rank == 0:
+        sec = ms / 1e3
+        line = {"metric": "body-substeps/s (collision stress: 65,536 mixed bodies incl. convex hulls, one world)",
+                "value": n_dyn_all * scene.substeps * args.steps / sec, "unit": UNIT, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "config1_collision_stress", "bodies": n_tot, "substeps": scene.substeps,
+                           "dt": scene.timestep, "seed": args.seed, "team": "cooperative grid, one launch per phase",
+                           "timing": "each step bracketed by CUDA events; counters read between steps"},
+                "sap_pairs_per_s": pairs_all / sec, "gjk_pairs_per_s": gjk_all / sec,
+                "sap_pairs_per_step": pairs_all / args.steps / ws, "gjk_pairs_per_step": gjk_all / args.steps / ws,
+                "gpu_launches": int(batch.stats()["kernel_launches"]) * args.steps}
+        print(json.dumps(line), flush=True)
+    batch.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -187,6 +280,9 @@ def main():
                     help="untimed steps before the warm-up (240 = 2 s simulated: the bodies have landed)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--plain-worlds", type=int, default=64,
+                    help="worlds in the plain per-world GPU sample (0 = skip it)")
+    ap.add_argument("--workload", default="batched", choices=["batched", "collision_stress"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -222,6 +318,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import rbps_b200
+    if args.workload == "collision_stress":
+        collision_stress(args, ws, rank, local)
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
 
     scene = scenes.config3(seed=rank_seed(args.seed, rank), n_worlds=args.worlds)
     stream = torch.cuda.Stream()  # a real stream: the legacy NULL stream would not order our launches
@@ -301,6 +402,12 @@ def main():
     e2e_value = n_dyn_all * scene.substeps * args.e2e_steps / (e2e_ms / 1e3)
     finite = bool(np.isfinite(p_host.numpy()).all())
 
+    plain = None
+    if args.plain_worlds > 0:
+        pv, pinfo = plain_gpu_run(scene, batch, args.plain_worlds, min(args.steps, 20), args.warmup, stream)
+        pv = reduce_over_ranks(pv, "sum", ws)  # every rank samples its own worlds
+        plain = {"value": pv, "unit": UNIT, "sample": pinfo, "batched_over_plain": value / pv}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -329,6 +436,7 @@ def main():
                              "algorithmic_bytes_per_step": bmodel,
                              "kernel": f"one step = {st['kernel_launches'] // max(args.steps, 1)} phase-kernel launches"},
                 "cpu_baseline": cpu,
+                "plain_gpu": plain,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n_tot_all) * 24,
                         "d2h_bytes_per_step": int(n_tot_all) * 56, "steps": args.e2e_steps},
                 "clocks": clk,

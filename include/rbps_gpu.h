@@ -183,6 +183,7 @@ typedef struct rbps_stats {
     int32_t device_error;      /* last device error word (RBPS_ERR_* or 0)       */
     uint32_t graph;            /* 1 when steps replay a captured CUDA graph      */
     uint64_t kernel_launches;  /* kernels launched by the last rbps_batch_step  */
+    uint64_t gjk_pairs;        /* pairs run through GJK / EPA in the last step  */
 } rbps_stats;
 
 /* Result of one shape-pair test (rbc::ContactManifold, Contact.hpp:37-51). */

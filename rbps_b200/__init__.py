@@ -52,7 +52,8 @@ class StateView(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("steps", C.c_uint64), ("pairs", C.c_uint64), ("candidates", C.c_uint64),
                 ("contacts", C.c_uint64), ("max_colors", C.c_uint32), ("serial_overflow", C.c_uint32),
-                ("device_error", C.c_int32), ("graph", C.c_uint32), ("kernel_launches", C.c_uint64)]
+                ("device_error", C.c_int32), ("graph", C.c_uint32), ("kernel_launches", C.c_uint64),
+                ("gjk_pairs", C.c_uint64)]
 
 
 def lib():

@@ -1247,7 +1247,7 @@ static int commit_typed(rbps_batch *b)
     {
         bool any_hull = false;
         size_t cap = 0;
-        for (uint32_t w : b->small_ids)
+        for (uint32_t w = 0; w < (uint32_t)b->wdev.size(); ++w)
         {
             const WorldDev &d = b->wdev[w];
             cap += (size_t)d.pair_cap + 1 + d.n_pc;
@@ -1365,9 +1365,10 @@ static long enqueue_step(rbps_batch *b, const Engine<T, P> &e)
     }
     for (uint32_t w : b->big_ids)
     {
-        if (launch_step_big<T, P>(e, w, b->grid_big, b->block, b->stream) != cudaSuccess)
+        long k = 0;
+        if (launch_step_big<T, P>(e, w, b->grid_big, b->block, b->stream, &k) != cudaSuccess)
             return RBPS_ERR_CUDA;
-        ++launches;
+        launches += k;
     }
     return launches;
 }
@@ -1765,6 +1766,7 @@ extern "C" int rbps_batch_get_stats(rbps_batch *b, rbps_stats *s)
         s->contacts += x.n_contacts;
         s->max_colors = std::max(s->max_colors, x.n_colors);
         s->serial_overflow += x.n_serial;
+        s->gjk_pairs += x.n_gjk;
     }
     s->kernel_launches = b->launches_last;
     s->graph = b->graph_exec ? 1u : 0u;

@@ -505,11 +505,13 @@ namespace rbps_gpu
         return res;
     }
 
-    // A GJK pair found by the narrowphase: queued for k_gjk when the batch
-    // has a GJK workspace, else counted as unsupported.
+    // A GJK pair found by the narrowphase: queued for k_gjk and counted
+    // (WorldStats::n_gjk, summed over the step's substeps).  Every batch
+    // with a hull collider has the queue; only hull pairs need GJK.
     template <class T, class P>
     __device__ __forceinline__ void queue_gjk(const Engine<T, P> &E, uint32_t w, uint32_t c, uint32_t &n_gjk)
     {
+        ++n_gjk;
         if (E.gjk_list)
         {
             const uint32_t slot = atomicAdd(E.gjk_count, 1u);
@@ -518,8 +520,6 @@ namespace rbps_gpu
             else
                 set_error_at(E.error, -2, 6, slot); // RBPS_ERR_CAPACITY
         }
-        else
-            ++n_gjk;
     }
 
     // GJK / EPA / manifold of one queued pair (world w, candidate c) on the
@@ -671,11 +671,10 @@ namespace rbps_gpu
 
     // ------------------------------------------------------------ the step
     // World::step (World.hpp:192-212) as phases.  Every phase ends with a
-    // team barrier and keeps its state in the world's scratch slice, so the
-    // phases run either back to back on one team (world_step) or as separate
-    // kernels over all worlds (the batched path: every CTA runs the same
-    // phase's code at a time, and each phase kernel gets its own register
-    // budget).
+    // team barrier and keeps its state in the world's scratch slice, so each
+    // phase runs as its own kernel: over all small worlds, one CTA per world
+    // (every CTA runs the same phase's code at a time), or for one large
+    // world on the whole cooperative grid.
 
     // Frame (once per step): SAP object update, sort, sweep; candidate list.
     template <class T, class P, class Team>
@@ -713,13 +712,7 @@ namespace rbps_gpu
         uint32_t n_gjk = 0;
         for (uint32_t c = tm.rank(); c < n_cand; c += tm.size())
             if (narrow_candidate(E, W, S.cand[c], S.cc[c]) == kNeedsGjk)
-            {
-                // a world on the cooperative grid has no GJK pass: count it
-                if (tm.ncta() > 1)
-                    ++n_gjk;
-                else
-                    queue_gjk(E, w, c, n_gjk);
-            }
+                queue_gjk(E, w, c, n_gjk);
         if (n_gjk)
             atomicAdd(S.misc + kMiscNGjk, n_gjk);
         tm.sync();
@@ -974,21 +967,6 @@ namespace rbps_gpu
         clk.finish();
     }
 
-    // All phases of one step back to back on one team.
-    template <class T, class P, class Team>
-    __device__ void world_step(const Engine<T, P> &E, const Team &tm, uint32_t w, BlockShared &sh)
-    {
-        phase_frame(E, tm, w, sh);
-        for (int sub = 0; sub < E.substeps; ++sub)
-        {
-            phase_narrow(E, tm, w);
-            phase_color_integrate(E, tm, w, sh);
-            phase_position(E, tm, w);
-            phase_velocity(E, tm, w);
-        }
-        phase_stats(E, tm, w);
-    }
-
     // ------------------------------------------------------------ kernels
     constexpr int kMaxBlock = 256;
 
@@ -1058,13 +1036,23 @@ namespace rbps_gpu
         each_small_world(E.small_worlds, E.n_small, E.work_counter + ctr, [&](uint32_t w) { phase_stats(E, tm, w); });
     }
 
-    // One large world on the whole cooperative grid.
+    // One phase of one large world on the whole cooperative grid; the phases
+    // are separate launches so that the GJK pass can run between the
+    // narrowphase and the colouring, as it does for the small worlds.
     template <class T, class P>
-    __global__ void __launch_bounds__(kMaxBlock) k_step_big(const Engine<T, P> E, uint32_t w)
+    __global__ void __launch_bounds__(kMaxBlock) k_big_phase(const Engine<T, P> E, uint32_t w, int phase)
     {
         __shared__ BlockShared sh;
         GridTeam tm;
-        world_step(E, tm, w, sh);
+        switch (phase)
+        {
+        case kKFrame: phase_frame(E, tm, w, sh); break;
+        case kKNarrow: phase_narrow(E, tm, w); break;
+        case kKColor: phase_color_integrate(E, tm, w, sh); break;
+        case kKPosition: phase_position(E, tm, w); break;
+        case kKVelocity: phase_velocity(E, tm, w); break;
+        default: phase_stats(E, tm, w); break;
+        }
     }
 
     // Enqueues one step of every small world: 2 + 4 * substeps phase kernels
@@ -1704,12 +1692,44 @@ namespace rbps_gpu
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_substep<T, P>, block, fl_smem);
     }
 
+    // Enqueues one step of one large world: 2 + 4 * substeps cooperative
+    // phase launches, plus the GJK pass after each narrowphase when the batch
+    // has one.  *launches receives the number of kernels enqueued.
     template <class T, class P>
-    cudaError_t launch_step_big(const Engine<T, P> &e, uint32_t world, int grid, int block, cudaStream_t stream)
+    cudaError_t launch_step_big(const Engine<T, P> &e, uint32_t world, int grid, int block, cudaStream_t stream,
+                                long *launches)
     {
         Engine<T, P> ec = e;
-        void *args[] = {(void *)&ec, (void *)&world};
-        return cudaLaunchCooperativeKernel((const void *)k_step_big<T, P>, dim3(grid), dim3(block), args, 0, stream);
+        int phase = 0;
+        void *args[] = {(void *)&ec, (void *)&world, (void *)&phase};
+        long n = 0;
+        auto run = [&](int ph) {
+            phase = ph;
+            ++n;
+            return cudaLaunchCooperativeKernel((const void *)k_big_phase<T, P>, dim3(grid), dim3(block), args, 0,
+                                               stream);
+        };
+        cudaError_t rc = run(kKFrame);
+        for (int s = 0; s < e.substeps && rc == cudaSuccess; ++s)
+        {
+            if (e.gjk_list && (rc = cudaMemsetAsync(e.gjk_count, 0, 4, stream)) != cudaSuccess)
+                break;
+            if ((rc = run(kKNarrow)) != cudaSuccess)
+                break;
+            if (e.gjk_list)
+            {
+                if ((rc = launch_gjk(e, stream)) != cudaSuccess)
+                    break;
+                ++n;
+            }
+            if ((rc = run(kKColor)) != cudaSuccess || (rc = run(kKPosition)) != cudaSuccess ||
+                (rc = run(kKVelocity)) != cudaSuccess)
+                break;
+        }
+        if (rc == cudaSuccess)
+            rc = run(kKStats);
+        *launches = n;
+        return rc;
     }
 
     template <class T, class P>
@@ -1731,7 +1751,7 @@ namespace rbps_gpu
     template <class T, class P>
     cudaError_t occupancy_big(int block, int *blocks_per_sm)
     {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_big<T, P>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_big_phase<T, P>, block, 0);
     }
 } // namespace rbps_gpu
 
@@ -1739,7 +1759,7 @@ namespace rbps_gpu
     template cudaError_t rbps_gpu::launch_step_phases<T, P>(const rbps_gpu::Engine<T, P> &,                        \
                                                             const rbps_gpu::PhaseLaunch &, cudaStream_t);           \
     template cudaError_t rbps_gpu::launch_step_big<T, P>(const rbps_gpu::Engine<T, P> &, uint32_t, int, int,        \
-                                                         cudaStream_t);                                           \
+                                                         cudaStream_t, long *);                                   \
     template cudaError_t rbps_gpu::occupancy_phase<T, P>(int, int, int *);                                         \
     template cudaError_t rbps_gpu::prepare_substep<T, P>(size_t);                                                  \
     template size_t rbps_gpu::smem_world_bytes<T, P>(uint32_t);                                                    \
@@ -1793,7 +1813,7 @@ namespace rbps_gpu
     }
 
     // Diagnostics: only the frame's broadphase + candidate build of one
-    // world on one CTA (the first phase of world_step).
+    // world on one CTA (the first phase of a step).
     template <class T, class P>
     __global__ void __launch_bounds__(kMaxBlock) k_debug_broadphase(const Engine<T, P> E, uint32_t w, uint32_t *out)
     {

@@ -34,7 +34,7 @@ namespace rbps_gpu
         uint32_t n_contacts;   // contact rows of the last substep
         uint32_t n_colors;     // colours used (colored mode)
         uint32_t n_serial;     // candidates in the serial overflow colour
-        uint32_t n_gjk;        // candidates that needed GJK/EPA
+        uint32_t n_gjk;        // candidates run through GJK/EPA, summed over the substeps
         uint32_t pad_[2];
     };
 
@@ -278,7 +278,8 @@ namespace rbps_gpu
     template <class T, class P>
     cudaError_t occupancy_phase(int kernel, int block, int *blocks_per_sm);
     template <class T, class P>
-    cudaError_t launch_step_big(const Engine<T, P> &e, uint32_t world, int grid, int block, cudaStream_t stream);
+    cudaError_t launch_step_big(const Engine<T, P> &e, uint32_t world, int grid, int block, cudaStream_t stream,
+                                long *launches);
     template <class T, class P>
     cudaError_t occupancy_big(int block, int *blocks_per_sm);
     template <class T, class P>

@@ -276,6 +276,65 @@ def config0(seed=0, n_bodies=512, steps=600):
                  f"{n_bodies} boxes+spheres over a ground plane, seed {seed}")
 
 
+def config1(seed=0, n_bodies=65536, steps=1, n_hull_shapes=None, extent=200.0):
+    """Collision stress, one world: n_bodies split equally (shuffled) among
+    spheres (r U[0.2,0.5]), boxes (half-extents U[0.2,0.5]^3), capsules
+    (half-height U[0.1,0.5], r U[0.1,0.3]) and convex hulls (quickhull of
+    16-32 points on an ellipsoid with semi-axes U[0.2,1]); random
+    orientation, positions U[0, extent]^3, velocities N(0, 2 m/s) per axis;
+    no ground plane, g=-9.81, dt=1/60, 10 substeps.
+
+    Every hull body gets its own hull shape unless n_hull_shapes caps the
+    number of distinct shapes (then body k uses shape k mod n_hull_shapes).
+    Points are Gaussian directions scaled by the semi-axes."""
+    import rbps_b200
+    rng = np.random.Generator(np.random.PCG64(seed))
+    q = n_bodies // 4
+    types = np.array([0] * (n_bodies - 3 * q) + [1] * q + [2] * q + [3] * q)
+    rng.shuffle(types)
+    n_hull = int(np.count_nonzero(types == 3))
+    n_shapes = n_hull if n_hull_shapes is None else max(1, min(n_hull, n_hull_shapes))
+    hulls = []
+    for _ in range(n_shapes):
+        m = int(rng.integers(16, 33))
+        d = rng.standard_normal((m, 3))
+        pts = d / np.linalg.norm(d, axis=1, keepdims=True) * rng.uniform(0.2, 1.0, 3)
+        hulls.append((pts, rbps_b200.quickhull(pts)))
+    hull_props = [hull_mass(v, t) for v, t in hulls]
+    sph_r = rng.uniform(0.2, 0.5, n_bodies)
+    box_h = rng.uniform(0.2, 0.5, (n_bodies, 3))
+    cap_hh = rng.uniform(0.1, 0.5, n_bodies)
+    cap_r = rng.uniform(0.1, 0.3, n_bodies)
+    quats = random_quats(rng, n_bodies)
+    pos = rng.uniform(0.0, extent, (n_bodies, 3))
+    vel = rng.normal(0.0, 2.0, (n_bodies, 3))
+    bodies, forces, colliders = [], [], []
+    k_hull = 0
+    for i in range(n_bodies):
+        t = types[i]
+        if t == 0:
+            m, inertia = sphere_mass(sph_r[i])
+            c = _collider(abi.SHAPE_SPHERE, [sph_r[i]], i, 0.5, 0.0)
+        elif t == 1:
+            m, inertia = box_mass(box_h[i])
+            c = _collider(abi.SHAPE_BOX, box_h[i], i, 0.5, 0.0)
+        elif t == 2:
+            m, inertia = capsule_mass(cap_hh[i], cap_r[i])
+            c = _collider(abi.SHAPE_CAPSULE, [cap_hh[i], cap_r[i]], i, 0.5, 0.0)
+        else:
+            h = k_hull % n_shapes
+            k_hull += 1
+            m, inertia = hull_props[h]
+            c = _collider(abi.SHAPE_CONVEX_HULL, [], i, 0.5, 0.0, hull=h)
+        b, f = _dyn_body(pos[i], quats[i], m, inertia, vel=vel[i])
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(c)
+    w = _finish(bodies, forces, colliders, [], hulls)
+    return Scene("config1_collision_stress", 1.0 / 60.0, 10, steps, [w],
+                 f"{n_bodies} spheres/boxes/capsules/hulls in {extent:g}^3 m, seed {seed}")
+
+
 def config3(seed=0, n_worlds=4096, steps=1000, lo_bodies=8, hi_bodies=512):
     """Batched uneven worlds: per world n ~ log-uniform[8,512] boxes/spheres
     (as config0) + one 13-link revolute capsule chain + ground plane,

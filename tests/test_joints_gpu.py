@@ -20,9 +20,12 @@ same: the same entries non-finite in the same step, the rest bit-identical.
 Gate: bit-identical state after every step wherever no trigonometric
 function of a moving angle is involved. A speed-driven revolute joint
 evaluates cos / sin of its advancing target on the device, whose last-ulp
-rounding may differ from the host libm; a one-ulp difference in the target
-grows through the compliant drive row to about 4e-11 (relative to
-max(|x|, 1)) after 22 steps, so that case is held to 1e-8 over 40 steps.
+rounding may differ from the host libm.  The drive row's normalize()
+threshold (Constraint.cpp:9-11) turns such a difference into a jump, so
+over many steps the trajectories part (4e-11 after 22 steps, 1.4e-8 after
+23).  That case is therefore checked one step at a time: after every step
+the device takes the reference's state, and each step's result must lie
+within 1e-9 of the reference's.
 """
 import math
 
@@ -35,7 +38,7 @@ from helpers import state_err, bit_equal
 pytestmark = pytest.mark.gpu
 
 DT, SUB, STEPS = 1.0 / 60.0, 10, 40
-TOL = 1e-8
+TOL = 1e-9
 
 
 def _quat(axis, angle):
@@ -178,6 +181,7 @@ def test_joint_world_matches_reference(rbps, ref, name):
         if "speed_drive" in name and "revolute" in name:
             err = state_err(st, rs)
             assert max(err.values()) <= TOL, f"step {step}: {err}"
+            b.set_state(0, rs)  # the next step starts from the reference's state
         else:
             assert bit_equal(st, rs), f"step {step}: {state_err(st, rs)}"
         moved = max(moved, float(np.abs(rs["position"] - x0).max()))
