@@ -75,8 +75,23 @@ enum {
     RBPS_SHAPE_CONVEX_HULL = 9
 };
 
-/* rbps::JointType / JointActuationType (constraints/Joint.hpp). */
-enum { RBPS_JOINT_PRISMATIC = 0, RBPS_JOINT_REVOLUTE = 1, RBPS_JOINT_FIXED = 2 };
+/* rbps::JointType / JointActuationType (constraints/Joint.hpp).
+ * RBPS_JOINT_SPHERICAL has no counterpart in the reference, whose joint
+ * types stop at FIXED (a ball joint is only planned there): a ball joint in
+ * the reference's row framework (Constraint.cpp:5-46) with two rows,
+ *   [0] POSITIONAL  attachment p1 - p2, as the revolute's row 1
+ *                   (Joint.cpp:107-111); carries the joint's compliance
+ *   [1] ROTATIONAL  swing cone: when the angle between the two bodies'
+ *                   `axis` exceeds upper_limit, the correction of
+ *                   compute_angle_limit_correction (Joint.cpp:73-90) about
+ *                   normalize(a1 x a2) with limits [-upper_limit, upper_limit]
+ * `limited` switches the cone on; lower_limit, limit_axis, actuation and
+ * damping are ignored.  Unlike the reference's joint rows, whose lambda is
+ * never reset, both rows restart lambda at 0 every substep (standard XPBD),
+ * so the compliance acts as a fixed-stiffness spring.  Both rows take the direction value / |value|
+ * whenever |value| > 1e-9 (set_value's normalize() would leave a zero
+ * direction for |value| in (1e-9, 3.2e-5)). */
+enum { RBPS_JOINT_PRISMATIC = 0, RBPS_JOINT_REVOLUTE = 1, RBPS_JOINT_FIXED = 2, RBPS_JOINT_SPHERICAL = 3 };
 enum { RBPS_ACTUATION_FREE = 0, RBPS_ACTUATION_POSITION = 1, RBPS_ACTUATION_SPEED = 2 };
 
 /* ---------------------------------------------------------- descriptors */
@@ -128,7 +143,8 @@ typedef struct rbps_collider_desc {
 } rbps_collider_desc;
 
 /* Mirrors Prismatic/Revolute/FixedJointParams (JointAPI.hpp:24-57).
- * axis = moving_axis (prismatic) or aligned_axis (revolute). */
+ * axis = moving_axis (prismatic), aligned_axis (revolute) or the swing
+ * axis in both bodies' frames (spherical). */
 typedef struct rbps_joint_desc {
     int32_t type;
     uint32_t body_1;

@@ -8,7 +8,11 @@
 // it; the product library never links or calls it.
 //
 // It takes the same descriptor structs as the product C ABI (rbps_gpu.h) so a
-// parity test builds the identical scene in both engines.
+// parity test builds the identical scene in both engines.  One addition is
+// the oracle's own: the ball joint with a swing cone (RBPS_JOINT_SPHERICAL),
+// which the reference does not have, restated on the reference's own rows
+// and limit routine (SphJoint below).  Its parity is unpinned by any
+// reference test.
 
 #include "rbps/API/World.hpp"
 #include "rbc/BroadPhase.hpp"
@@ -31,12 +35,126 @@ namespace
         ~HullStore() { rbc::convex_hull_data_destroy(data); }
     };
 
+    // A ball joint with a swing cone (RBPS_JOINT_SPHERICAL).  The reference
+    // has no such joint type; this is the oracle's own restatement in the
+    // reference's row framework: its two rows live in the world's
+    // ConstraintCollection (created in joint order, so solve_constraints
+    // relaxes them in the same order as the other joints' rows), and their
+    // errors are set every substep by sph_joint_errors below.
+    struct SphJoint
+    {
+        uint32_t b1, b2;
+        m3d::vec3 r1, r2, axis;
+        bool limited;
+        double cone;
+        uint32_t row_attach, row_cone; // constraint ids
+    };
+
     struct RefWorld
     {
         rbps::World w;
         std::vector<std::unique_ptr<HullStore>> hulls;
+        std::vector<SphJoint> sph;
         RefWorld(double dt, int substeps) : w(dt, substeps) {}
     };
+
+    // set_value (Constraint.cpp:5-12) for the ball joint's rows, with the
+    // direction value / |value| whenever |value| > EPSILON: normalize()
+    // would return the zero vector for |value| in (1e-9, 3.2e-5), and a
+    // rotational row with compliance 0 then divides by zero.
+    void sph_set_value(rbps::ConstraintCollection &cc, uint32_t i, const m3d::vec3 &value)
+    {
+        const double mag = m3d::magnitude(value);
+        cc.magnitude[i] = mag;
+        cc.direction[i] = mag > m3d::EPSILON ? value * (1.0 / mag) : m3d::vec3{1.0, 0.0, 0.0};
+    }
+
+    // Ball-joint row error, evaluated on the current poses right before the
+    // row is solved: the attachment as the revolute joint's
+    // (Joint.cpp:107-111), the swing cone through the reference's own
+    // compute_angle_limit_correction (Joint.cpp:73-90) with the swing angle
+    // phi = atan2(|a1 x a2|, a1 . a2) about n = normalize(a1 x a2) and limits
+    // [-cone, cone].  Both rows restart lambda every substep (standard XPBD,
+    // Mueller et al. 2020, Alg. 2), so the compliant attachment row is a
+    // spring of fixed stiffness.
+    void sph_row_error(RefWorld *rw, const SphJoint &j, bool cone, uint32_t i)
+    {
+        rbps::BodyCollection &bc = rw->w.bodies;
+        rbps::ConstraintCollection &cc = rw->w.constraints;
+        cc.lambda[i] = 0.0;
+        if (!cone)
+        {
+            const m3d::vec3 r1_wc = m3d::rotate(bc.orientation[j.b1], j.r1);
+            const m3d::vec3 r2_wc = m3d::rotate(bc.orientation[j.b2], j.r2);
+            const m3d::vec3 p1 = bc.position[j.b1] + r1_wc;
+            const m3d::vec3 p2 = bc.position[j.b2] + r2_wc;
+            sph_set_value(cc, i, p1 - p2);
+            return;
+        }
+        m3d::vec3 err{0.0, 0.0, 0.0};
+        if (j.limited)
+        {
+            const m3d::vec3 a1 = m3d::rotate(bc.orientation[j.b1], j.axis);
+            const m3d::vec3 a2 = m3d::rotate(bc.orientation[j.b2], j.axis);
+            const m3d::vec3 c = m3d::cross(a1, a2);
+            double phi = m3d::atan2(m3d::magnitude(c), m3d::dot(a1, a2));
+            err = rbps::compute_angle_limit_correction(phi, m3d::normalize(c), a1, a2, -j.cone, j.cone);
+        }
+        sph_set_value(cc, i, -err);
+    }
+
+    // solve_constraints (Constraint.cpp:90-106): every row in pool order,
+    // with a ball joint's row evaluated right before it is solved.  The
+    // other joints' rows keep the errors compute_joint_errors set before
+    // the loop, as in the reference; on a hanging chain those stale errors
+    // over-correct and the chain diverges within a few steps, which is why
+    // the ball joint evaluates its rows in place.
+    void solve_rows_with_sph(RefWorld *rw, double inv_h)
+    {
+        rbps::BodyCollection &bc = rw->w.bodies;
+        rbps::ConstraintCollection &cc = rw->w.constraints;
+        std::vector<int64_t> tag(cc.count(), -1);
+        for (size_t k = 0; k < rw->sph.size(); ++k)
+        {
+            tag[cc.index_of(rw->sph[k].row_attach)] = (int64_t)(2 * k);
+            tag[cc.index_of(rw->sph[k].row_cone)] = (int64_t)(2 * k + 1);
+        }
+        for (uint32_t i = 0; i < cc.count(); ++i)
+        {
+            if (tag[i] >= 0)
+                sph_row_error(rw, rw->sph[tag[i] / 2], (tag[i] & 1) != 0, i);
+            switch (cc.type[i])
+            {
+            case rbps::ConstraintType::POSITIONAL: rbps::compute_positional_constraint_impulse(bc, cc, i, inv_h); break;
+            case rbps::ConstraintType::ROTATIONAL: rbps::compute_rotational_constraint_impulse(bc, cc, i, inv_h); break;
+            default: break;
+            }
+        }
+    }
+
+    // World::step (World.hpp:192-212) with solve_constraints replaced by
+    // solve_rows_with_sph.
+    void step_with_sph(RefWorld *rw)
+    {
+        rbps::World &w = rw->w;
+        const double h = w.timestep / w.substeps;
+        const double inv_h = 1.0 / h;
+        rbps::update_broad_phase_aabbs(w.colliders, w.broad_phase_state, w.bodies, w.timestep, true);
+        rbc::broad_phase_update(w.broad_phase_state);
+        w.contacts.reserve(w.broad_phase_state.pairs.size() * 4);
+        for (int i = 0; i < w.substeps; ++i)
+        {
+            w.contacts.clear();
+            rbps::run_narrow_phase(w.broad_phase_state, w.colliders, w.bodies, w.contacts);
+            rbps::update_position_and_orientation(w.bodies, h);
+            rbps::solve_contacts_position_level(w.contacts, w.bodies, inv_h);
+            rbps::compute_joint_errors(w.joints, w.bodies, w.constraints, h);
+            solve_rows_with_sph(rw, inv_h);
+            rbps::update_velocities(w.bodies, inv_h);
+            rbps::solve_contacts_velocity_level(w.contacts, w.bodies, h);
+            rbps::apply_joint_damping(w.joints, w.bodies, h);
+        }
+    }
 
     m3d::vec3 v3(const double *p) { return m3d::vec3(p[0], p[1], p[2]); }
     m3d::quat q4(const double *p) { return m3d::quat(p[0], p[1], p[2], p[3]); }
@@ -167,6 +285,23 @@ extern "C"
             p.body_1 = d->body_1; p.body_2 = d->body_2;
             p.r_1 = v3(d->r_1); p.r_2 = v3(d->r_2);
             id = rw->w.create_fixed_joint(p);
+        }
+        else if (d->type == RBPS_JOINT_SPHERICAL)
+        {
+            SphJoint j;
+            j.b1 = d->body_1; j.b2 = d->body_2;
+            j.r1 = v3(d->r_1); j.r2 = v3(d->r_2); j.axis = v3(d->axis);
+            j.limited = d->limited != 0;
+            j.cone = d->upper_limit;
+            auto &cc = rw->w.constraints;
+            j.row_attach = rbps::create_constraint(cc, {.body_1 = d->body_1, .body_2 = d->body_2,
+                                                        .type = rbps::ConstraintType::POSITIONAL,
+                                                        .r_1 = j.r1, .r_2 = j.r2, .compliance = d->compliance});
+            j.row_cone = rbps::create_constraint(cc, {.body_1 = d->body_1, .body_2 = d->body_2,
+                                                      .type = rbps::ConstraintType::ROTATIONAL,
+                                                      .r_1 = j.r1, .r_2 = j.r2, .compliance = 0.0});
+            rw->sph.push_back(j);
+            return 0x80000000u | (uint32_t)(rw->sph.size() - 1);
         }
         if (id != UINT32_MAX)
         {
@@ -324,7 +459,12 @@ extern "C"
     {
         auto *rw = static_cast<RefWorld *>(h);
         for (int i = 0; i < n; ++i)
-            rw->w.step();
+        {
+            if (rw->sph.empty())
+                rw->w.step();
+            else
+                step_with_sph(rw);
+        }
     }
 
     uint32_t ref_body_count(void *h) { return static_cast<RefWorld *>(h)->w.bodies.count(); }

@@ -39,6 +39,7 @@ SHAPE_CONVEX_HULL = 9
 JOINT_PRISMATIC = 0
 JOINT_REVOLUTE = 1
 JOINT_FIXED = 2
+JOINT_SPHERICAL = 3    # ball joint with a swing cone; no reference counterpart
 
 ACTUATION_FREE = 0
 ACTUATION_POSITION = 1
@@ -142,7 +143,8 @@ def collider_default():
 
 
 def joint_default(jtype=JOINT_REVOLUTE):
-    """Revolute/Prismatic/FixedJointParams{} (JointAPI.hpp:24-57)."""
+    """Revolute/Prismatic/FixedJointParams{} (JointAPI.hpp:24-57); a
+    spherical joint defaults like a prismatic one (swing axis +x, no cone)."""
     j = np.zeros(1, JOINT_DT)[0]
     j["type"] = jtype
     if jtype != JOINT_FIXED:

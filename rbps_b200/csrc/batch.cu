@@ -627,7 +627,7 @@ extern "C" int rbps_world_add_joint(rbps_batch *b, uint32_t world, const rbps_jo
     HostWorld &w = b->worlds[world];
     if (!d || d->body_1 >= w.bodies.size() || d->body_2 >= w.bodies.size())
         return fail(RBPS_ERR_INVALID, "joint bodies out of range");
-    if (d->type < RBPS_JOINT_PRISMATIC || d->type > RBPS_JOINT_FIXED)
+    if (d->type < RBPS_JOINT_PRISMATIC || d->type > RBPS_JOINT_SPHERICAL)
         return fail(RBPS_ERR_INVALID, "bad joint type %d", d->type);
     if (id)
         *id = (uint32_t)w.joints.size();
@@ -791,7 +791,7 @@ static int commit_typed(rbps_batch *b)
         d.row_off = nr;
         uint32_t rows = 0;
         for (const auto &j : hw.joints)
-            rows += j.type == RBPS_JOINT_REVOLUTE ? 4 : (j.type == RBPS_JOINT_PRISMATIC ? 3 : 2);
+            rows += j.type == RBPS_JOINT_REVOLUTE ? 4 : (j.type == RBPS_JOINT_PRISMATIC ? 3 : 2); // fixed, spherical: 2
         d.n_rows = rows;
         // greedy joint colouring by shared dynamic bodies
         {
@@ -1042,13 +1042,15 @@ static int commit_typed(rbps_batch *b)
                 J.axis = V4<T>{T(jd.axis[0]), T(jd.axis[1]), T(jd.axis[2]), T(0)};
                 if (jd.type == RBPS_JOINT_REVOLUTE)
                     J.limit_axis = V4<T>{T(jd.limit_axis[0]), T(jd.limit_axis[1]), T(jd.limit_axis[2]), T(0)};
-                J.lower = T(jd.lower_limit);
+                // a spherical joint's cone is symmetric: [-upper, upper]
+                const double lower = jd.type == RBPS_JOINT_SPHERICAL ? -jd.upper_limit : jd.lower_limit;
+                J.lower = T(lower);
                 J.upper = T(jd.upper_limit);
                 J.target_pos = T(jd.target_position);
                 J.target_speed = T(jd.target_speed);
                 J.damping = T(jd.damping);
                 // from_axis_angle of the clamped limit angle (quat.hpp:111-117)
-                const double hl = jd.lower_limit * 0.5, hu = jd.upper_limit * 0.5;
+                const double hl = lower * 0.5, hu = jd.upper_limit * 0.5;
                 J.sin_lo = T(std::sin(hl));
                 J.cos_lo = T(std::cos(hl));
                 J.sin_hi = T(std::sin(hu));
@@ -1057,7 +1059,8 @@ static int commit_typed(rbps_batch *b)
                 J.b2 = d.body_off + jd.body_2;
                 J.row0 = row;
                 J.type = jd.type;
-                J.act = jd.type == RBPS_JOINT_FIXED ? RBPS_ACTUATION_FREE : jd.actuation;
+                J.act = jd.type == RBPS_JOINT_FIXED || jd.type == RBPS_JOINT_SPHERICAL ? RBPS_ACTUATION_FREE
+                                                                                       : jd.actuation;
                 J.limited = jd.type == RBPS_JOINT_FIXED ? 0 : jd.limited;
                 int types[4];
                 double comp[4] = {0, 0, 0, 0};
@@ -1073,6 +1076,12 @@ static int commit_typed(rbps_batch *b)
                     cnt = 3;
                     types[0] = kRowRotational; types[1] = kRowPositional; types[2] = kRowPositional;
                     comp[2] = jd.compliance;
+                }
+                else if (jd.type == RBPS_JOINT_SPHERICAL)
+                {
+                    cnt = 2;
+                    types[0] = kRowPositional; types[1] = kRowRotational;
+                    comp[0] = jd.compliance;
                 }
                 else
                 {

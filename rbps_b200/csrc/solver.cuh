@@ -404,7 +404,8 @@ namespace rbps_gpu
     {
         kPrismatic = 0,
         kRevolute = 1,
-        kFixed = 2
+        kFixed = 2,
+        kSpherical = 3
     };
     enum : int
     {
@@ -458,6 +459,19 @@ namespace rbps_gpu
             else
                 d = value * (T(1) / mag);
         }
+        r.dir = V4<T>{d.x, d.y, d.z, mag};
+    }
+
+    // The ball joint's rows (no reference counterpart) take the direction
+    // value / |value| whenever |value| > EPSILON, in every precision, so they
+    // stay clear of the zero-direction band of set_value above.
+    template <class T>
+    __device__ __forceinline__ void row_set_value_div(Row<T> &r, const vec3<T> &value)
+    {
+        const T mag = length(value);
+        vec3<T> d(T(1.0), T(0.0), T(0.0));
+        if (mag > T(kEpsilon))
+            d = value * (T(1.0) / mag);
         r.dir = V4<T>{d.x, d.y, d.z, mag};
     }
 
@@ -575,6 +589,11 @@ namespace rbps_gpu
             }
             row_set_value(rows[2], err_drive);
         }
+        else if (j.type == kSpherical)
+        {
+            // a ball joint evaluates its rows when they are solved
+            // (solve_joint_rows), not here
+        }
         else
         {
             const quat<T> dq = q1 * conjugate(q2);
@@ -587,6 +606,50 @@ namespace rbps_gpu
         }
     }
 
+    // Ball joint (RBPS_JOINT_SPHERICAL; no reference counterpart), both rows
+    // evaluated on the current poses right before each is solved, as XPBD
+    // does (Mueller et al. 2020, Alg. 2), with lambda restarted every
+    // substep.  The reference instead sets every joint row's error before
+    // solving any (World.hpp:168-173); on a hanging chain those stale errors
+    // over-correct and the chain diverges within a few steps.
+    //   row 0: attachment p1 - p2, as the revolute joint's (Joint.cpp:107-111)
+    //   row 1: swing cone -- the swing angle phi between the bodies' axes
+    //          about n = normalize(a1 x a2), limited to [lower, upper] =
+    //          [-cone, cone] as compute_angle_limit_correction does
+    //          (Joint.cpp:73-90), whose from_axis_angle normalizes n again
+    template <class T, class P>
+    __device__ __forceinline__ void solve_ball_joint(BodyR<T, P> &b1, BodyR<T, P> &b2, const Joint<T> &j,
+                                                     Row<T> *rows, T inv_h)
+    {
+        {
+            const vec3<T> p1 = b1.x + rotate(b1.q, v3(j.r1));
+            const vec3<T> p2 = b2.x + rotate(b2.q, v3(j.r2));
+            rows[0].r2.w = T(0.0);
+            row_set_value_div(rows[0], p1 - p2);
+            solve_row(b1, b2, rows[0], inv_h);
+        }
+        vec3<T> err_limit(T(0.0), T(0.0), T(0.0));
+        if (j.limited)
+        {
+            const vec3<T> a1 = rotate(b1.q, v3(j.axis));
+            const vec3<T> a2 = rotate(b2.q, v3(j.axis));
+            const vec3<T> c = cross(a1, a2);
+            const T phi = atan2(length(c), dot(a1, a2));
+            if (phi < j.lower || phi > j.upper)
+            {
+                const bool lo = phi < j.lower;
+                const T s = lo ? j.sin_lo : j.sin_hi;
+                const T co = lo ? j.cos_lo : j.cos_hi;
+                const vec3<T> nn = normalize(normalize(c));
+                const quat<T> rq(co, nn.x * s, nn.y * s, nn.z * s);
+                err_limit = cross(rotate(rq, a1), a2);
+            }
+        }
+        rows[1].r2.w = T(0.0);
+        row_set_value_div(rows[1], -err_limit);
+        solve_row(b1, b2, rows[1], inv_h);
+    }
+
     // All rows of one joint, in row order, its two bodies held in registers.
     template <class T, class P>
     __device__ __noinline__ void solve_joint_rows(const Bodies<T, P> &B, const Joint<T> &j, Row<T> *rows, T inv_h)
@@ -594,8 +657,11 @@ namespace rbps_gpu
         BodyR<T, P> b1, b2;
         load_body(B, j.b1, b1, false);
         load_body(B, j.b2, b2, false);
-        for (int r = 0; r < j.count; ++r)
-            solve_row(b1, b2, rows[r], inv_h);
+        if (j.type == kSpherical)
+            solve_ball_joint(b1, b2, j, rows, inv_h);
+        else
+            for (int r = 0; r < j.count; ++r)
+                solve_row(b1, b2, rows[r], inv_h);
         store_pose(B, j.b1, b1);
         store_pose(B, j.b2, b2);
     }

@@ -335,6 +335,81 @@ def config1(seed=0, n_bodies=65536, steps=1, n_hull_shapes=None, extent=200.0):
                  f"{n_bodies} spheres/boxes/capsules/hulls in {extent:g}^3 m, seed {seed}")
 
 
+def config2(seed=0, n_chains=1024, n_links=32, steps=300, radius=0.05, half_height=0.15, mass=1.0,
+            spacing=1.0, cone_deg=60.0, compliance=1e-6, max_angle_deg=30.0, gap=0.04, friction=0.5):
+    """Joint-heavy single world: n_chains chains of n_links capsules (radius
+    0.05 m, segment 2 * half_height = 0.3 m, 1 kg each) hanging from static
+    anchors on a square grid `spacing` m apart, joined by ball joints with a
+    60 degree swing cone about the links' axes and compliance 1e-6; every
+    joint starts bent by an angle U[-30, 30] degrees about a random
+    horizontal axis of its parent; no ground, g=-9.81, dt=1/60, 8 substeps.
+
+    A link's local +Y is its capsule axis (identity = hanging straight
+    down, pivot above the centre); pivots sit `gap`/2 beyond the capsule
+    tips, so neighbouring links clear each other anywhere inside the cone."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    side = int(math.ceil(math.sqrt(n_chains)))
+    reach = half_height + radius + 0.5 * gap
+    m0, inertia0 = capsule_mass(half_height, radius)
+    inertia = inertia0 * (mass / m0)
+    cone = cone_deg * PI / 180.0
+    amax = max_angle_deg * PI / 180.0
+    bodies, forces, colliders, joints = [], [], [], []
+
+    def qmul(a, b):
+        return (a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3],
+                a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2],
+                a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1],
+                a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0])
+
+    def qrot(q, v):
+        w, x, y, z = q
+        u = np.array([x, y, z])
+        v = np.asarray(v, np.float64)
+        t = 2.0 * np.cross(u, v)
+        return v + w * t + np.cross(u, t)
+
+    for c in range(n_chains):
+        anchor = np.array([(c % side) * spacing, 0.0, (c // side) * spacing])
+        a = abi.body_default()
+        a["type"] = abi.BODY_STATIC
+        a["mass"] = 0.0
+        a["position"] = anchor
+        parent = len(bodies)
+        bodies.append(a)
+        forces.append((0.0, 0.0, 0.0))
+        q_par = (1.0, 0.0, 0.0, 0.0)
+        pivot = anchor
+        for k in range(n_links):
+            phi = rng.uniform(0.0, 2.0 * PI)
+            ang = rng.uniform(-amax, amax)
+            s = math.sin(0.5 * ang)
+            q = qmul(q_par, (math.cos(0.5 * ang), math.cos(phi) * s, 0.0, math.sin(phi) * s))
+            n = math.sqrt(sum(x * x for x in q))
+            q = tuple(x / n for x in q)
+            pos = pivot - qrot(q, (0.0, reach, 0.0))
+            b, f = _dyn_body(tuple(pos), q, mass, inertia)
+            bid = len(bodies)
+            bodies.append(b)
+            forces.append(f)
+            colliders.append(_collider(abi.SHAPE_CAPSULE, [half_height, radius], bid, friction, 0.0))
+            j = abi.joint_default(abi.JOINT_SPHERICAL)
+            j["body_1"] = parent
+            j["body_2"] = bid
+            j["axis"] = (0.0, 1.0, 0.0)
+            j["r_1"] = (0.0, 0.0, 0.0) if k == 0 else (0.0, -reach, 0.0)
+            j["r_2"] = (0.0, reach, 0.0)
+            j["compliance"] = compliance
+            j["limited"] = 1
+            j["upper_limit"] = cone
+            joints.append(j)
+            parent, q_par = bid, q
+            pivot = pos - qrot(q, (0.0, reach, 0.0))
+    w = _finish(bodies, forces, colliders, joints)
+    return Scene("config2_joint_heavy", 1.0 / 60.0, 8, steps, [w],
+                 f"{n_chains} chains x {n_links} capsules, ball joints with a {cone_deg:g} deg cone, seed {seed}")
+
+
 def config3(seed=0, n_worlds=4096, steps=1000, lo_bodies=8, hi_bodies=512):
     """Batched uneven worlds: per world n ~ log-uniform[8,512] boxes/spheres
     (as config0) + one 13-link revolute capsule chain + ground plane,

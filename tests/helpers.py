@@ -49,3 +49,22 @@ def state_err(st, ref_st):
 
 def bit_equal(st, ref_st):
     return all(np.array_equal(np.asarray(st[k]), np.asarray(ref_st[k])) for k in ("position", "orientation"))
+
+
+def _qrot(q, v):
+    w, u = q[:, :1], q[:, 1:]
+    t = 2.0 * np.cross(u, v)
+    return v + w * t + np.cross(u, t)
+
+
+def joint_gaps(spec, st):
+    """(attachment gap in m, swing angle between the bodies' `axis` in
+    degrees) of every joint of a world spec in state st."""
+    J, q, x = spec.joints, st["orientation"], st["position"]
+    b1, b2 = J["body_1"], J["body_2"]
+    p1 = x[b1] + _qrot(q[b1], J["r_1"])
+    p2 = x[b2] + _qrot(q[b2], J["r_2"])
+    a1 = _qrot(q[b1], J["axis"])
+    a2 = _qrot(q[b2], J["axis"])
+    ang = np.degrees(np.arccos(np.clip((a1 * a2).sum(1), -1.0, 1.0)))
+    return np.linalg.norm(p1 - p2, axis=1), ang
