@@ -25,6 +25,9 @@ same colored solver) on a sample of the same worlds from the same state.
 boxes, capsules and convex hulls instead (scenes.config1), `--workload
 joint_heavy` the single world of 1,024 hanging 32-capsule chains on ball
 joints (scenes.config2); their lines add SAP pairs/s and GJK pairs/s.
+`--workload precision_stress` steps 256 box towers 1e4 m from the origin
+(scenes.config4) in FP32, FP32_POS64 and FP64 and reports drift, penetration
+and energy change per mode.
 """
 import argparse
 import json
@@ -309,6 +312,131 @@ def single_world(args, ws, rank, local):
     batch.close()
 
 
+def tower_energy(scene, st, g=9.81):
+    """Kinetic + potential energy of every dynamic body, summed (the ground
+    plane of each world at its static body's height)."""
+    e = 0.0
+    off = 0
+    for w in scene.worlds:
+        n = len(w.bodies)
+        dyn = w.bodies["type"] == 1  # RBPS_BODY_DYNAMIC
+        x = st["position"][off:off + n]
+        v = st["linear_velocity"][off:off + n]
+        om = st["angular_velocity"][off:off + n]
+        q = st["orientation"][off:off + n]
+        m = w.bodies["mass"]
+        I = w.bodies["inertia"][:, :3]
+        # body-frame angular velocity: conj(q) * omega * q
+        qw, qv = q[:, :1], -q[:, 1:]
+        t = 2.0 * np.cross(qv, om)
+        ob = om + qw * t + np.cross(qv, t)
+        y0 = w.bodies["position"][~dyn][:, 1].min() if (~dyn).any() else 0.0
+        ke = 0.5 * m * (v * v).sum(1) + 0.5 * (I * ob * ob).sum(1)
+        pe = m * g * (x[:, 1] - y0)
+        e += float((ke + pe)[dyn].sum())
+        off += n
+    return e
+
+
+def precision_stress(args, ws, rank, local):
+    """256 worlds, each a 64-box tower (half-extent 0.5 m, masses alternating
+    1:1000) 1e4 m from the origin on its own ground plane, friction 0.8,
+    20 substeps (scenes.config4).  Steps the same scene in FP32 (colored),
+    FP32_POS64 (colored, positions relative to a per-world double origin)
+    and FP64 (reference order: the device engine that matches the oracle
+    bit for bit) and reports, per mode, throughput, the largest body
+    displacement from the initial stack, the deepest contact in the last
+    step and the relative change of total energy (the 1:1000 towers fall in
+    every mode, the reference's FP64 solver included), and the frame error:
+    the largest position difference after 200 steps between the towers
+    where they are and the same towers moved to the origin, in the same
+    mode (FP32_POS64 against FP32 at the origin).  FP32's float spacing at
+    1e4 m is 1 mm, which also freezes small horizontal motions there.
+    """
+    import torch
+    import rbps_b200
+    from rbps_b200 import abi, scenes
+    torch.cuda.set_device(local)
+    steps = args.steps
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+
+    def run(scene):
+        x0 = np.concatenate([w.bodies["position"] for w in scene.worlds])
+        st0 = {"position": x0, "orientation": np.concatenate([w.bodies["orientation"] for w in scene.worlds]),
+               "linear_velocity": np.zeros_like(x0), "angular_velocity": np.zeros_like(x0)}
+        e0 = tower_energy(scene, st0)
+        modes = {}
+        for name, prec, solve in (("fp32", abi.PRECISION_FP32, abi.SOLVE_COLORED),
+                                  ("fp32_pos64", abi.PRECISION_FP32_POS64, abi.SOLVE_COLORED),
+                                  ("fp64", abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER)):
+            batch = rbps_b200.Batch.from_scene(scene, prec, solve, device=local, stream=stream.cuda_stream)
+            n_tot, n_dyn = batch.total_bodies()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            batch.step(steps - 1)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            batch.set_dump(True)
+            batch.step(1)
+            st = batch.state_all(("position", "orientation", "linear_velocity", "angular_velocity"))
+            depth = 0.0
+            for w in range(0, len(scene.worlds), 16):
+                c = batch.contacts(w)
+                if len(c):
+                    depth = max(depth, float(c["penetration_depth"].max()))
+            finite = bool(np.isfinite(st["position"]).all())
+            modes[name] = {"ms_per_step": ms / max(steps - 1, 1),
+                           "body_substeps_per_s": n_dyn * scene.substeps * (steps - 1) / (ms / 1e3),
+                           "max_displacement_m": float(np.abs(st["position"] - x0).max()) if finite else None,
+                           "max_penetration_m": depth,
+                           "energy_drift": (tower_energy(scene, st) - e0) / abs(e0) if finite else None,
+                           "finite": finite}
+            batch.close()
+        return modes
+
+    scene = scenes.config4(seed=rank_seed(args.seed, rank))
+    modes = run(scene)
+
+    # frame error: the same towers moved to the origin, 200 steps each way
+    near_worlds, shift = [], []
+    for w in scene.worlds:
+        p = w.bodies["position"]
+        o = 0.5 * (p.min(0) + p.max(0))
+        b = w.bodies.copy()
+        b["position"] = p - o
+        near_worlds.append(scenes.WorldSpec(b, w.forces, w.colliders, w.joints, w.hulls))
+        shift.append(np.repeat(o[None], len(p), 0))
+    near = scenes.Scene(scene.name, scene.timestep, scene.substeps, scene.steps, near_worlds)
+    shift = np.concatenate(shift)
+    for name, prec, solve in (("fp32", abi.PRECISION_FP32, abi.SOLVE_COLORED),
+                              ("fp32_pos64", abi.PRECISION_FP32_POS64, abi.SOLVE_COLORED),
+                              ("fp64", abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER)):
+        a = rbps_b200.Batch.from_scene(scene, prec, solve, device=local, stream=stream.cuda_stream)
+        b = rbps_b200.Batch.from_scene(near, abi.PRECISION_FP32 if prec == abi.PRECISION_FP32_POS64 else prec, solve,
+                                       device=local, stream=stream.cuda_stream)
+        a.step(200)
+        b.step(200)
+        d = np.abs(a.state_all()["position"] - (b.state_all()["position"] + shift))
+        modes[name]["frame_error_200_steps_m"] = float(d.max())
+        a.close()
+        b.close()
+    if rank == 0:
+        line = {"metric": "body-substeps/s (precision stress: 256 worlds x 64-box towers 1e4 m from the origin, "
+                          "FP32_POS64)",
+                "value": modes["fp32_pos64"]["body_substeps_per_s"], "unit": UNIT, "n_gpus": ws, "steps": steps,
+                "warmup": 0, "ms_per_step": modes["fp32_pos64"]["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "config4_precision_stress", "worlds": len(scene.worlds),
+                           "bodies_per_world": len(scene.worlds[0].bodies), "substeps": scene.substeps,
+                           "dt": scene.timestep, "offset_m": 1.0e4, "seed": args.seed,
+                           "timing": "steps 1..K-1 of a fresh scene per mode; step K with dumps for the depths"},
+                "modes": modes}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -325,7 +453,8 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--plain-worlds", type=int, default=64,
                     help="worlds in the plain per-world GPU sample (0 = skip it)")
-    ap.add_argument("--workload", default="batched", choices=["batched", "collision_stress", "joint_heavy"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "collision_stress", "joint_heavy", "precision_stress"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -361,8 +490,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import rbps_b200
-    if args.workload in SINGLE_WORLD:
-        single_world(args, ws, rank, local)
+    if args.workload in SINGLE_WORLD or args.workload == "precision_stress":
+        (precision_stress if args.workload == "precision_stress" else single_world)(args, ws, rank, local)
         if ws > 1:
             torch.distributed.destroy_process_group()
         return

@@ -53,7 +53,8 @@ enum {
 enum {
     RBPS_PRECISION_FP64 = 0,       /* everything double, reference operation order */
     RBPS_PRECISION_FP32 = 1,       /* everything float                              */
-    RBPS_PRECISION_FP32_POS64 = 2  /* float solver, double body positions           */
+    RBPS_PRECISION_FP32_POS64 = 2  /* float solver; body positions float relative   */
+                                   /* to a per-world double origin (far-from-origin) */
 };
 
 /* Order in which contact and joint rows are relaxed inside a substep. */

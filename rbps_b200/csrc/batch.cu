@@ -360,6 +360,25 @@ struct rbps_batch
 
     // host I/O staging (rbps_batch_step_io)
     double *io_force = nullptr, *io_pos = nullptr, *io_rot = nullptr;
+    // RBPS_PRECISION_FP32_POS64: every world's bodies are stored in float
+    // relative to a per-world origin held in double (3 per world), so a
+    // world far from the global origin keeps float resolution near its own
+    // bodies; body_world maps a body to its world (host and device copies).
+    std::vector<double> origin;
+    std::vector<uint32_t> body_world;
+    double *origin_d = nullptr;
+    uint32_t *body_world_d = nullptr;
+    bool relative() const { return desc.precision == RBPS_PRECISION_FP32_POS64; }
+    const double *origin_of_body(size_t g) const
+    {
+        static const double zero[3] = {0.0, 0.0, 0.0};
+        return relative() ? origin.data() + 3 * (size_t)body_world[g] : zero;
+    }
+    const double *origin_of_world(uint32_t w) const
+    {
+        static const double zero[3] = {0.0, 0.0, 0.0};
+        return relative() ? origin.data() + 3 * (size_t)w : zero;
+    }
 
     // dumps
     bool dump = false;
@@ -372,7 +391,7 @@ struct rbps_batch
     bool prof_off = true;
 
     size_t t_size() const { return desc.precision == RBPS_PRECISION_FP64 ? 8 : 4; }
-    size_t p_size() const { return desc.precision == RBPS_PRECISION_FP32 ? 4 : 8; }
+    size_t p_size() const { return desc.precision == RBPS_PRECISION_FP64 ? 8 : 4; }
 
     int alloc(void **p, size_t bytes)
     {
@@ -718,6 +737,8 @@ namespace
         e.gjk_cap = b->gjk_cap;
         e.gjk_slots = b->gjk_slots;
         e.gjk_ws = b->gjk_ws;
+        e.origin = b->origin_d;
+        e.body_world = b->body_world_d;
         return e;
     }
 
@@ -725,9 +746,7 @@ namespace
     {
         if (precision == RBPS_PRECISION_FP64)
             return sizeof(CandContacts<double, double>);
-        if (precision == RBPS_PRECISION_FP32)
-            return sizeof(CandContacts<float, float>);
-        return sizeof(CandContacts<float, double>);
+        return sizeof(CandContacts<float, float>); // FP32 and FP32_POS64
     }
 
     template <class T>
@@ -852,9 +871,33 @@ static int commit_typed(rbps_batch *b)
     std::vector<uint8_t> btype(nb);
     b->total_bodies = nb;
     b->total_dynamic = 0;
+    b->origin.assign(3 * (size_t)W, 0.0);
+    b->body_world.clear();
+    if (b->relative())
+    {
+        // origin = centre of the box around the world's body positions
+        b->body_world.resize(nb);
+        for (uint32_t w = 0; w < W; ++w)
+        {
+            const HostWorld &hw = b->worlds[w];
+            for (int k = 0; k < 3 && !hw.bodies.empty(); ++k)
+            {
+                double lo = hw.bodies[0].position[k], hi = lo;
+                for (const auto &d : hw.bodies)
+                {
+                    lo = std::min(lo, d.position[k]);
+                    hi = std::max(hi, d.position[k]);
+                }
+                b->origin[3 * (size_t)w + k] = 0.5 * (lo + hi);
+            }
+            for (uint32_t i = 0; i < hw.bodies.size(); ++i)
+                b->body_world[b->wdev[w].body_off + i] = w;
+        }
+    }
     for (uint32_t w = 0; w < W; ++w)
     {
         const HostWorld &hw = b->worlds[w];
+        const double *ow = b->origin_of_world(w);
         for (uint32_t i = 0; i < hw.bodies.size(); ++i)
         {
             const rbps_body_desc &d = hw.bodies[i];
@@ -864,8 +907,8 @@ static int commit_typed(rbps_batch *b)
             double iinv[6] = {0, 0, 0, 0, 0, 0};
             if (!st)
                 smat3_inverse(d.inertia, iinv);
-            put_v4<P>(pos, g, d.position[0], d.position[1], d.position[2], 0);
-            put_v4<P>(ppos, g, d.position[0], d.position[1], d.position[2], 0);
+            put_v4<P>(pos, g, d.position[0] - ow[0], d.position[1] - ow[1], d.position[2] - ow[2], 0);
+            put_v4<P>(ppos, g, d.position[0] - ow[0], d.position[1] - ow[1], d.position[2] - ow[2], 0);
             put_v4<T>(rot, g, d.orientation[0], d.orientation[1], d.orientation[2], d.orientation[3]);
             put_v4<T>(lin, g, d.linear_velocity[0], d.linear_velocity[1], d.linear_velocity[2], inv_mass);
             put_v4<T>(ang, g, d.angular_velocity[0], d.angular_velocity[1], d.angular_velocity[2], 0);
@@ -895,6 +938,12 @@ static int commit_typed(rbps_batch *b)
     };
     up(&b->pos, pos);
     up(&b->prev_pos, ppos);
+    if (b->relative())
+    {
+        int rc2;
+        if ((rc2 = b->upload(&b->origin_d, b->origin)) || (rc2 = b->upload(&b->body_world_d, b->body_world)))
+            return rc2;
+    }
     up(&b->rot, rot);
     up(&b->prev_rot, rot);
     up(&b->lin, lin);
@@ -986,7 +1035,8 @@ static int commit_typed(rbps_batch *b)
             const rbps_body_desc &bd = hw.bodies[cd.body_id];
             bpc[d.bp_off + o] = c;
             tf<double> t;
-            const vec3<double> bp(bd.position[0], bd.position[1], bd.position[2]);
+            const double *ow = b->origin_of_world(w);
+            const vec3<double> bp(bd.position[0] - ow[0], bd.position[1] - ow[1], bd.position[2] - ow[2]);
             const quat<double> br(bd.orientation[0], bd.orientation[1], bd.orientation[2], bd.orientation[3]);
             t.pos = bp + rotate(br, vec3<double>(cd.local_pos[0], cd.local_pos[1], cd.local_pos[2]));
             t.rot = br * quat<double>(cd.local_rot[0], cd.local_rot[1], cd.local_rot[2], cd.local_rot[3]);
@@ -1291,10 +1341,8 @@ extern "C" int rbps_batch_commit(rbps_batch *b)
     int rc;
     if (b->desc.precision == RBPS_PRECISION_FP64)
         rc = commit_typed<double, double>(b);
-    else if (b->desc.precision == RBPS_PRECISION_FP32)
-        rc = commit_typed<float, float>(b);
     else
-        rc = commit_typed<float, double>(b);
+        rc = commit_typed<float, float>(b); // FP32 and FP32_POS64
     if (rc)
         return rc;
     CU(cudaDeviceSynchronize());
@@ -1343,9 +1391,7 @@ extern "C" int rbps_batch_set_dump(rbps_batch *b, int32_t enable)
         return RBPS_OK;
     if (b->desc.precision == RBPS_PRECISION_FP64)
         return alloc_dumps<double, double>(b);
-    if (b->desc.precision == RBPS_PRECISION_FP32)
-        return alloc_dumps<float, float>(b);
-    return alloc_dumps<float, double>(b);
+    return alloc_dumps<float, float>(b);
 }
 
 // ------------------------------------------------------------ stepping
@@ -1453,10 +1499,8 @@ extern "C" int rbps_batch_step(rbps_batch *b, int32_t n_steps)
     // the small-world view needs its scratch / layout
     if (b->desc.precision == RBPS_PRECISION_FP64)
         rc = step_typed<double, double>(b, n_steps);
-    else if (b->desc.precision == RBPS_PRECISION_FP32)
-        rc = step_typed<float, float>(b, n_steps);
     else
-        rc = step_typed<float, double>(b, n_steps);
+        rc = step_typed<float, float>(b, n_steps);
     if (!rc)
         b->steps_done += (uint64_t)n_steps;
     return rc;
@@ -1509,7 +1553,10 @@ static int get_state_typed(rbps_batch *b, uint32_t first, uint32_t n, const rbps
     {
         if (v->position)
         {
-            v->position[3 * i] = pos[i].x; v->position[3 * i + 1] = pos[i].y; v->position[3 * i + 2] = pos[i].z;
+            const double *o = b->origin_of_body(first + i);
+            v->position[3 * i] = o[0] + double(pos[i].x);
+            v->position[3 * i + 1] = o[1] + double(pos[i].y);
+            v->position[3 * i + 2] = o[2] + double(pos[i].z);
         }
         if (v->orientation)
         {
@@ -1543,7 +1590,11 @@ static int set_state_typed(rbps_batch *b, uint32_t first, uint32_t n, const rbps
     for (uint32_t i = 0; i < n; ++i)
     {
         if (v->position)
-            pos[i] = V4<P>{P(v->position[3 * i]), P(v->position[3 * i + 1]), P(v->position[3 * i + 2]), P(0)};
+        {
+            const double *o = b->origin_of_body(first + i);
+            pos[i] = V4<P>{P(v->position[3 * i] - o[0]), P(v->position[3 * i + 1] - o[1]),
+                           P(v->position[3 * i + 2] - o[2]), P(0)};
+        }
         if (v->orientation)
             rot[i] = Q4<T>{T(v->orientation[4 * i]), T(v->orientation[4 * i + 1]), T(v->orientation[4 * i + 2]),
                            T(v->orientation[4 * i + 3])};
@@ -1562,9 +1613,7 @@ static int set_state_typed(rbps_batch *b, uint32_t first, uint32_t n, const rbps
 }
 
 #define DISPATCH_PREC(b, fn, ...)                                        \
-    ((b)->desc.precision == RBPS_PRECISION_FP64   ? fn<double, double>(__VA_ARGS__) \
-     : (b)->desc.precision == RBPS_PRECISION_FP32 ? fn<float, float>(__VA_ARGS__)   \
-                                                  : fn<float, double>(__VA_ARGS__))
+    ((b)->desc.precision == RBPS_PRECISION_FP64 ? fn<double, double>(__VA_ARGS__) : fn<float, float>(__VA_ARGS__))
 
 static int ready(rbps_batch *b, const char *who)
 {
@@ -1698,8 +1747,9 @@ static int get_contacts_typed(rbps_batch *b, uint32_t world, rbps_contact *out, 
             r.normal[0] = cc[c].normal.x; r.normal[1] = cc[c].normal.y; r.normal[2] = cc[c].normal.z;
             r.r_a_local[0] = p.ra.x; r.r_a_local[1] = p.ra.y; r.r_a_local[2] = p.ra.z;
             r.r_b_local[0] = p.rb.x; r.r_b_local[1] = p.rb.y; r.r_b_local[2] = p.rb.z;
-            r.point_on_a[0] = p.pa.x; r.point_on_a[1] = p.pa.y; r.point_on_a[2] = p.pa.z;
-            r.point_on_b[0] = p.pb.x; r.point_on_b[1] = p.pb.y; r.point_on_b[2] = p.pb.z;
+            const double *o = b->origin_of_world(world);
+            r.point_on_a[0] = o[0] + p.pa.x; r.point_on_a[1] = o[1] + p.pa.y; r.point_on_a[2] = o[2] + p.pa.z;
+            r.point_on_b[0] = o[0] + p.pb.x; r.point_on_b[1] = o[1] + p.pb.y; r.point_on_b[2] = o[2] + p.pb.z;
             r.penetration_depth = p.depth;
             r.normal_lambda = p.lam_n;
             r.tangent_lambda = p.lam_t;
@@ -1800,7 +1850,13 @@ extern "C" int rbps_batch_get_sap_state(rbps_batch *b, uint32_t world, double *f
     if (n_objects)
         *n_objects = d.n_bp;
     if (fat && d.n_bp)
+    {
         CU(cudaMemcpy(fat, b->fat + d.bp_off, d.n_bp * sizeof(FatBox), cudaMemcpyDeviceToHost));
+        const double *o = b->origin_of_world(world);
+        for (uint32_t k = 0; k < d.n_bp; ++k)
+            for (int a = 0; a < 6; ++a)
+                fat[6 * k + a] += o[a % 3];
+    }
     if ((ep_ids || ep_values) && d.n_bp)
     {
         std::vector<uint32_t> ids(2 * d.n_bp), keys(2 * d.n_bp);

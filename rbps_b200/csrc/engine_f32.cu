@@ -1,5 +1,5 @@
-// FP32 instantiations of the step kernels: all-float, and float solver with
-// double body positions (far-from-origin scenes).
+// FP32 instantiation of the step kernels (RBPS_PRECISION_FP32, and
+// RBPS_PRECISION_FP32_POS64, whose positions are float relative to a
+// per-world double origin).
 #include "engine_impl.cuh"
 RBPS_INSTANTIATE_ENGINE(float, float)
-RBPS_INSTANTIATE_ENGINE(float, double)

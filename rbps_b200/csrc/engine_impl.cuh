@@ -1791,9 +1791,15 @@ namespace rbps_gpu
         {
             const V4<P> x = E.B.pos[i];
             const Q4<T> q = E.B.rot[i];
-            pos[3 * i] = double(x.x);
-            pos[3 * i + 1] = double(x.y);
-            pos[3 * i + 2] = double(x.z);
+            double o[3] = {0.0, 0.0, 0.0};
+            if (E.origin)
+            {
+                const double *ow = E.origin + 3 * (size_t)E.body_world[i];
+                o[0] = ow[0]; o[1] = ow[1]; o[2] = ow[2];
+            }
+            pos[3 * i] = o[0] + double(x.x);
+            pos[3 * i + 1] = o[1] + double(x.y);
+            pos[3 * i + 2] = o[2] + double(x.z);
             rot[4 * i] = double(q.w);
             rot[4 * i + 1] = double(q.x);
             rot[4 * i + 2] = double(q.y);

@@ -218,6 +218,10 @@ namespace rbps_gpu
         uint32_t *gjk_count;
         uint32_t gjk_cap, gjk_slots;
         void *gjk_ws;
+        // RBPS_PRECISION_FP32_POS64: per-world origin (3 doubles a world) and
+        // the world of every body; body positions are stored relative to it
+        const double *origin;
+        const uint32_t *body_world;
         // flat colored pipeline over all small worlds (see engine_impl.cuh)
         uint32_t *wcoff;               // n_small + 1: candidate prefix over small_worlds
         uint32_t *gcol;                // global colour bookkeeping, kGcolWords

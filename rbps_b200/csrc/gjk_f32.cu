@@ -1,6 +1,5 @@
-// FP32 and FP32-positions instantiations of the GJK kernels (compiled with
+// FP32 instantiation of the GJK kernels (compiled with
 // -fmad=false: their GJK / EPA arithmetic is double).
 #include "gjk_kernels.cuh"
 
 RBPS_INSTANTIATE_GJK(float, float)
-RBPS_INSTANTIATE_GJK(float, double)

@@ -428,11 +428,11 @@ def config3(seed=0, n_worlds=4096, steps=1000, lo_bodies=8, hi_bodies=512):
                  f"{n_worlds} worlds, bodies log-uniform[{lo_bodies},{hi_bodies}] + 13-link chain, seed {seed}")
 
 
-def config4(seed=0, n_worlds=256, steps=2000, height=64, offset=1.0e4):
+def config4(seed=0, n_worlds=256, steps=2000, height=64, offset=1.0e4, mass_ratio=1.0e-3):
     """Precision stress: per world a tower of `height` boxes (half-extent
-    0.5), densities alternating 1:1000, offset `offset` m from the origin
-    plus a uniform horizontal jitter, ground plane at the offset, friction
-    0.8, 20 substeps."""
+    0.5), densities alternating 1:1000 (`mass_ratio`; 1.0 gives a uniform
+    tower), offset `offset` m from the origin plus a uniform horizontal
+    jitter, ground plane at the offset, friction 0.8, 20 substeps."""
     rng = np.random.Generator(np.random.PCG64(seed))
     worlds = []
     for w in range(n_worlds):
@@ -443,7 +443,7 @@ def config4(seed=0, n_worlds=256, steps=2000, height=64, offset=1.0e4):
         h = np.array([0.5, 0.5, 0.5])
         for k in range(height):
             m, inertia = box_mass(h)
-            scale = 1.0 if k % 2 == 0 else 1.0e-3
+            scale = 1.0 if k % 2 == 0 else mass_ratio
             b, f = _dyn_body((ox, 0.5 + k * 1.0, oz), (1.0, 0.0, 0.0, 0.0), m * scale, inertia * scale)
             bid = len(bodies)
             bodies.append(b)
