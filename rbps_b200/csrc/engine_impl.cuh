@@ -168,24 +168,57 @@ namespace rbps_gpu
                 set_error_at(error, kErrInternal, 4, i); // the endpoint sort must leave the keys ordered
         }
         tm.sync();
-        // count the pairs each opening endpoint emits
-        for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+        // count the pairs each opening endpoint emits.  A team spread over
+        // the cooperative grid (one large world) gives each opening endpoint
+        // a warp that tests 32 endpoints of its overlap run at a time: the
+        // runs are long there (hundreds of endpoints) and uneven, so one
+        // thread per endpoint would leave most lanes waiting on a few.
+        const bool by_warp = tm.ncta() > 1;
+        const uint32_t lane = threadIdx.x & 31u;
+        if (by_warp)
         {
-            const uint32_t id = ep_id[i];
-            uint32_t c = 0;
-            if (!(id & 1u) && id < id_limit)
+            for (uint32_t i = tm.rank() >> 5; i < nep; i += tm.size() >> 5)
             {
-                const FatBox fa = fat[id >> 1];
-                const uint32_t end = min(ep_pos[id + 1], nep);
-                for (uint32_t j = i + 1; j < end; ++j)
+                const uint32_t id = ep_id[i]; // the same for the whole warp
+                uint32_t c = 0;
+                if (!(id & 1u) && id < id_limit)
                 {
-                    const uint32_t id2 = ep_id[j];
-                    if (!(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]))
-                        ++c;
+                    const FatBox fa = fat[id >> 1];
+                    const uint32_t end = min(ep_pos[id + 1], nep);
+                    for (uint32_t j0 = i + 1; j0 < end; j0 += 32)
+                    {
+                        const uint32_t j = j0 + lane;
+                        bool hit = false;
+                        if (j < end)
+                        {
+                            const uint32_t id2 = ep_id[j];
+                            hit = !(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]);
+                        }
+                        c += __popc(__ballot_sync(0xffffffffu, hit));
+                    }
                 }
+                if (lane == 0)
+                    S.cnt[i] = c;
             }
-            S.cnt[i] = c;
         }
+        else
+            for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+            {
+                const uint32_t id = ep_id[i];
+                uint32_t c = 0;
+                if (!(id & 1u) && id < id_limit)
+                {
+                    const FatBox fa = fat[id >> 1];
+                    const uint32_t end = min(ep_pos[id + 1], nep);
+                    for (uint32_t j = i + 1; j < end; ++j)
+                    {
+                        const uint32_t id2 = ep_id[j];
+                        if (!(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]))
+                            ++c;
+                    }
+                }
+                S.cnt[i] = c;
+            }
         tm.sync();
         uint32_t total = team_excl_scan(tm, S.cnt, S.cnt, nep, S.tile_sums, sh);
         if (tm.leader())
@@ -197,27 +230,61 @@ namespace rbps_gpu
             total = pair_cap;
         }
         // emit (earlier-opening object, later object, later opening position)
-        for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+        if (by_warp)
         {
-            const uint32_t id = ep_id[i];
-            if ((id & 1u) || id >= id_limit)
-                continue;
-            uint32_t k = S.cnt[i];
-            const FatBox fa = fat[id >> 1];
-            const uint32_t end = min(ep_pos[id + 1], nep);
-            for (uint32_t j = i + 1; j < end && k < total; ++j)
+            for (uint32_t i = tm.rank() >> 5; i < nep; i += tm.size() >> 5)
             {
-                const uint32_t id2 = ep_id[j];
-                if (!(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]))
+                const uint32_t id = ep_id[i];
+                if ((id & 1u) || id >= id_limit)
+                    continue;
+                uint32_t k = S.cnt[i];
+                const FatBox fa = fat[id >> 1];
+                const uint32_t end = min(ep_pos[id + 1], nep);
+                for (uint32_t j0 = i + 1; j0 < end && k < total; j0 += 32)
                 {
-                    S.pr_a[k] = id >> 1;
-                    S.pr_b[k] = id2 >> 1;
-                    S.pk[k] = j;
-                    S.pv[k] = k;
-                    ++k;
+                    const uint32_t j = j0 + lane;
+                    uint32_t id2 = 0;
+                    bool hit = false;
+                    if (j < end)
+                    {
+                        id2 = ep_id[j];
+                        hit = !(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]);
+                    }
+                    const uint32_t m = __ballot_sync(0xffffffffu, hit);
+                    const uint32_t kk = k + __popc(m & ((1u << lane) - 1u));
+                    if (hit && kk < total)
+                    {
+                        S.pr_a[kk] = id >> 1;
+                        S.pr_b[kk] = id2 >> 1;
+                        S.pk[kk] = j;
+                        S.pv[kk] = kk;
+                    }
+                    k += __popc(m);
                 }
             }
         }
+        else
+            for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+            {
+                const uint32_t id = ep_id[i];
+                if ((id & 1u) || id >= id_limit)
+                    continue;
+                uint32_t k = S.cnt[i];
+                const FatBox fa = fat[id >> 1];
+                const uint32_t end = min(ep_pos[id + 1], nep);
+                for (uint32_t j = i + 1; j < end && k < total; ++j)
+                {
+                    const uint32_t id2 = ep_id[j];
+                    if (!(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]))
+                    {
+                        S.pr_a[k] = id >> 1;
+                        S.pr_b[k] = id2 >> 1;
+                        S.pk[k] = j;
+                        S.pv[k] = k;
+                        ++k;
+                    }
+                }
+            }
         tm.sync();
         // reference emission order: stable sort by the later opening position
         const int bits = nep > 1 ? 32 - __clz(nep - 1) : 1;
@@ -1653,6 +1720,15 @@ namespace rbps_gpu
     template <class T, class P>
     cudaError_t prepare_substep(size_t bytes)
     {
+        // the attribute belongs to the kernel on the current device, shared
+        // by every batch there: only ever raise it, or a batch created later
+        // with smaller worlds would make an earlier one's launches fail
+        cudaFuncAttributes fa;
+        cudaError_t rc = cudaFuncGetAttributes(&fa, k_substep<T, P>);
+        if (rc != cudaSuccess)
+            return rc;
+        if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes)
+            return cudaSuccess;
         return cudaFuncSetAttribute(k_substep<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     }
 

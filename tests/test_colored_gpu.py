@@ -63,3 +63,18 @@ def test_colored_batch_settles(rbps):
     assert np.isfinite(st["position"]).all()
     # everything has fallen onto the ground plane (y >= -0.1) and stays low
     assert st["position"][:, 1].min() > -0.2
+
+
+def test_batches_of_different_sizes_coexist(rbps):
+    """Colored batches share the substep kernel's shared-memory limit on a
+    device: a batch created after one with larger worlds must not lower it
+    (the larger batch's steps would then fail to launch)."""
+    big = rbps.Batch.from_scene(scenes.config3(seed=2, n_worlds=8, lo_bodies=300, hi_bodies=512),
+                                abi.PRECISION_FP32, abi.SOLVE_COLORED)
+    small = rbps.Batch.from_scene(scenes.config3(seed=3, n_worlds=8, lo_bodies=8, hi_bodies=16),
+                                  abi.PRECISION_FP32, abi.SOLVE_COLORED)
+    big.step(2)
+    small.step(2)
+    big.step(2)
+    for b in (big, small):
+        assert np.isfinite(b.state_all()["position"]).all()
