@@ -1490,7 +1490,8 @@ namespace rbps_gpu
     // colours to every thread.
     template <class T, class P, class Team>
     __device__ uint32_t greedy_color_world(const Engine<T, P> &E, const Team &tm, uint32_t w,
-                                           unsigned long long *mask, BlockShared &sh, uint32_t *book)
+                                           unsigned long long *mask, BlockShared &sh, uint32_t *book,
+                                           uint32_t *stage = nullptr)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
@@ -1506,11 +1507,55 @@ namespace rbps_gpu
             cnt[k] = 0u;
         const uint32_t n_act = compact_active(tm, S, n_cand, sh);
         tm.sync();
+        const uint8_t *type = E.B.type + W.body_off;
+        if (stage)
+        {
+            // Staged: the team loads a chunk of active candidates into shared
+            // memory at once, as packed (a, b, dynamic a, dynamic b) records
+            // (world-local body indices < 2048), so the leader's greedy pass
+            // -- the same candidates in the same order -- touches shared
+            // memory only.
+            uint8_t *scol = reinterpret_cast<uint8_t *>(stage + kColorStage);
+            for (uint32_t q0 = 0; q0 < n_act; q0 += kColorStage)
+            {
+                const uint32_t m = min(kColorStage, n_act - q0);
+                for (uint32_t k = tm.rank(); k < m; k += tm.size())
+                {
+                    const Cand cd = S.cand[S.alist[q0 + k]];
+                    stage[k] = (cd.ba & 2047u) | ((cd.bb & 2047u) << 11) |
+                               ((type[cd.ba] == kDynamic ? 1u : 0u) << 22) |
+                               ((type[cd.bb] == kDynamic ? 1u : 0u) << 23);
+                }
+                tm.sync();
+                if (tm.leader())
+                    for (uint32_t k = 0; k < m; ++k)
+                    {
+                        const uint32_t r = stage[k];
+                        const uint32_t a = r & 2047u, b = (r >> 11) & 2047u;
+                        const bool da = (r >> 22) & 1u, db = (r >> 23) & 1u;
+                        const unsigned long long used = (da ? mask[a] : 0ull) | (db ? mask[b] : 0ull);
+                        uint32_t col = kColorSerial;
+                        if (used != ~0ull)
+                        {
+                            col = (uint32_t)(__ffsll((long long)~used) - 1);
+                            const unsigned long long bit = 1ull << col;
+                            if (da)
+                                mask[a] |= bit;
+                            if (db)
+                                mask[b] |= bit;
+                        }
+                        scol[k] = (uint8_t)col;
+                        cnt[col] += 1u;
+                    }
+                tm.sync();
+                for (uint32_t k = tm.rank(); k < m; k += tm.size())
+                    S.color[S.alist[q0 + k]] = scol[k];
+            }
+        }
         if (tm.leader())
         {
-            const uint8_t *type = E.B.type + W.body_off;
             constexpr uint32_t kAhead = 8; // candidates loaded ahead of the mask updates
-            for (uint32_t q0 = 0; q0 < n_act; q0 += kAhead)
+            for (uint32_t q0 = 0; q0 < (stage ? 0u : n_act); q0 += kAhead)
             {
                 uint32_t cs[kAhead];
                 Cand cd[kAhead];
@@ -1592,16 +1637,20 @@ namespace rbps_gpu
     struct SmemWorld
     {
         static constexpr size_t kBook = 136 * sizeof(uint32_t);
+        // colouring stage: kColorStage packed candidate records + their colours
+        static constexpr size_t kStage = kColorStage * (sizeof(uint32_t) + 1);
         static constexpr size_t kPerBody =
             sizeof(unsigned long long) + 2 * sizeof(V4<P>) + 2 * sizeof(Q4<T>) + 2 * sizeof(V4<T>) + 1;
 
-        __host__ __device__ static size_t bytes(uint32_t cap) { return kBook + (size_t)cap * kPerBody; }
+        __host__ __device__ static size_t bytes(uint32_t cap) { return kBook + kStage + (size_t)cap * kPerBody; }
 
         __device__ static Bodies<T, P> view(unsigned char *p, uint32_t cap, const Bodies<T, P> &G, uint32_t body_off,
-                                            unsigned long long **mask, uint32_t **book)
+                                            unsigned long long **mask, uint32_t **book, uint32_t **stage)
         {
             *book = reinterpret_cast<uint32_t *>(p);
             p += kBook;
+            *stage = reinterpret_cast<uint32_t *>(p);
+            p += kStage;
             *mask = reinterpret_cast<unsigned long long *>(p);
             p += (size_t)cap * sizeof(unsigned long long);
             Bodies<T, P> V;
@@ -1638,18 +1687,18 @@ namespace rbps_gpu
         const WorldDev W = E.worlds[w];
         const bool local = smem && W.n_bodies <= cap;
         unsigned long long *mask = nullptr;
-        uint32_t *book = nullptr;
+        uint32_t *book = nullptr, *stage = nullptr;
         Bodies<T, P> V = E.B;
         uint32_t boff = W.body_off;
         if (local)
         {
-            V = SmemWorld<T, P>::view(smem, cap, E.B, W.body_off, &mask, &book);
+            V = SmemWorld<T, P>::view(smem, cap, E.B, W.body_off, &mask, &book, &stage);
             boff = 0;
         }
         else
             mask = world_scratch(E, W).bmask;
         PhaseClock clk(prof_slots(E, tm, w), false);
-        greedy_color_world(E, tm, w, mask, sh, book);
+        greedy_color_world(E, tm, w, mask, sh, book, stage);
         clk.mark(kPhColor);
         if (local)
         {

@@ -81,6 +81,7 @@ namespace rbps_gpu
     RBPS_HD size_t scr_align(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
     constexpr uint32_t kColorSerial = 64;  // overflow colour, solved by one thread
+    constexpr uint32_t kColorStage = 256;  // candidates staged in shared memory per colouring chunk
     constexpr uint32_t kColorIdle = 65;    // candidate without contact rows this substep
     constexpr uint32_t kMaxColorRounds = 96;
     constexpr uint32_t kMiscWords = 64 + 2 * 66 + kMaxColorRounds + 8;
