@@ -736,6 +736,14 @@ namespace rbps_gpu
                                   make_layout(W.n_bp, W.n_bodies, W.pair_cap, W.n_pc, sizeof(CandContacts<T, P>)));
     }
 
+    // Asks L2 for every 128-byte line of [p, p + bytes) (prefetch.global.L2).
+    __device__ __forceinline__ void prefetch_l2_range(const void *p, size_t bytes)
+    {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+        for (uintptr_t l = a & ~uintptr_t(127); l < a + bytes; l += 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(l));
+    }
+
     // ------------------------------------------------------------ the step
     // World::step (World.hpp:192-212) as phases.  Every phase ends with a
     // team barrier and keeps its state in the world's scratch slice, so each
@@ -1611,6 +1619,10 @@ namespace rbps_gpu
             const uint32_t c = S.alist[q];
             const uint32_t slot = atomicAdd(&cnt[S.color[c]], 1u);
             S.corder[slot] = c;
+            // the position and velocity solves read this candidate's contact
+            // block colour by colour, each read behind a barrier: start it
+            // on its way to L2 now, while integrate runs
+            prefetch_l2_range(S.cc + c, sizeof(CandContacts<T, P>));
         }
         if (book) // the offsets also go to misc for the statistics and dumps
             for (uint32_t k = tm.rank(); k < 66; k += tm.size())
