@@ -12,8 +12,11 @@ steps its own 4,096 worlds (weak scaling, no collective on the step path).
 
 Prints one JSON line (rank 0).  `value` = whole-job body-substeps/s from CUDA
 events on the step stream (max over ranks); `e2e` = the same metric through
-rbps_batch_step_io with page-locked host buffers (forces in, poses out,
-copies inside the timed region); `roofline` = the step kernel against the
+rbps_batch_step_io_async with page-locked host buffers, over the same steps
+(the batch is rewound to a device snapshot taken after the warm-up): every
+step copies its forces in and its poses out, on copy streams that overlap
+the neighbouring steps' compute, and the timed region ends after the last
+step's poses are on the host; `roofline` = the step kernel against the
 measured HBM copy bandwidth with the algorithmic byte model below;
 `cpu_baseline` = the reference engine (oracle/_ref, built from the
 reference's own sources) on a bounded sample of the same worlds, all host
@@ -445,7 +448,7 @@ def main():
     ap.add_argument("--impl", default="rbps", choices=["rbps", "reference"])
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = as many as --steps")
     ap.add_argument("--cpu-seconds", type=float, default=30.0)
     ap.add_argument("--preroll", type=int, default=240,
                     help="untimed steps before the warm-up (240 = 2 s simulated: the bodies have landed)")
@@ -516,6 +519,8 @@ def main():
     if args.preroll:
         batch.step(args.preroll)
     batch.step(args.warmup)
+    # the e2e leg rewinds here, so that both legs time the same steps
+    snap = batch.snapshot()
     batch.synchronize()
 
     # timed region: K steps, device events on the step stream
@@ -561,18 +566,26 @@ def main():
     f_host.copy_(torch.from_numpy(np.concatenate([w.forces for w in scene.worlds])))
     p_host = torch.empty((n_tot, 3), dtype=torch.float64, pin_memory=True)
     q_host = torch.empty((n_tot, 4), dtype=torch.float64, pin_memory=True)
-    batch.step_io(f_host.data_ptr(), p_host.data_ptr(), q_host.data_ptr())  # stage buffers
+    # two pose buffers, alternating: every step's poses land on the host
+    p_host2 = torch.empty_like(p_host)
+    q_host2 = torch.empty_like(q_host)
+    batch.step_io_async(f_host.data_ptr(), p_host.data_ptr(), q_host.data_ptr())  # stage buffers
+    batch.restore(snap)  # back to the first timed step
+    batch.synchronize()
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_steps):
-        batch.step_io(f_host.data_ptr(), p_host.data_ptr(), q_host.data_ptr())
+    e2e_steps = args.steps if args.e2e_steps <= 0 else args.e2e_steps
+    for k in range(e2e_steps):
+        p_out, q_out = (p_host, q_host) if k % 2 == 0 else (p_host2, q_host2)
+        batch.step_io_async(f_host.data_ptr(), p_out.data_ptr(), q_out.data_ptr())
+    batch.synchronize()  # the last step's poses are on the host
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = reduce_over_ranks(e0.elapsed_time(e1), "max", ws)
-    e2e_value = n_dyn_all * scene.substeps * args.e2e_steps / (e2e_ms / 1e3)
-    finite = bool(np.isfinite(p_host.numpy()).all())
+    e2e_value = n_dyn_all * scene.substeps * e2e_steps / (e2e_ms / 1e3)
+    finite = bool(np.isfinite(p_host.numpy()).all() and np.isfinite(p_host2.numpy()).all())
 
     plain = None
     if args.plain_worlds > 0:
@@ -610,7 +623,8 @@ def main():
                 "cpu_baseline": cpu,
                 "plain_gpu": plain,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n_tot_all) * 24,
-                        "d2h_bytes_per_step": int(n_tot_all) * 56, "steps": args.e2e_steps},
+                        "d2h_bytes_per_step": int(n_tot_all) * 56, "steps": e2e_steps,
+                        "window": "the same steps as value (device snapshot after the warm-up, restored)"},
                 "clocks": clk,
                 "gpu_launches": int(st["kernel_launches"]),
                 "cuda_graph": bool(st["graph"]),

@@ -283,6 +283,7 @@ RBPS_API int rbps_batch_commit(rbps_batch *batch);
  * Asynchronous on the batch stream; device errors surface at the next
  * rbps_batch_synchronize / get_* call. */
 RBPS_API int rbps_batch_step(rbps_batch *batch, int32_t n_steps);
+/* Waits for every step and copy enqueued on the batch (both its streams). */
 RBPS_API int rbps_batch_synchronize(rbps_batch *batch);
 /* One World::step of every world with host I/O, for callers that feed
  * forces and read poses every frame: copies force_in (3 doubles per body,
@@ -293,6 +294,33 @@ RBPS_API int rbps_batch_synchronize(rbps_batch *batch);
  * bandwidth. */
 RBPS_API int rbps_batch_step_io(rbps_batch *batch, const double *force_in, double *position_out,
                                 double *orientation_out);
+/* rbps_batch_step_io without the wait, for a caller that steps frame after
+ * frame: enqueues the force copy, the step and the pose copies and returns.
+ * The copies run on a second stream and overlap the neighbouring steps'
+ * compute (two staging slots on the device alternate between calls).  The
+ * call's host buffers must stay untouched until rbps_batch_synchronize
+ * returns (force_in may be reused after the next call returns).  The same
+ * World::step as rbps_batch_step_io (World.hpp:192-212); no reference
+ * counterpart for the pipelining. */
+RBPS_API int rbps_batch_step_io_async(rbps_batch *batch, const double *force_in, double *position_out,
+                                      double *orientation_out);
+
+/* Device-side snapshot of every world's simulation state -- bodies (poses,
+ * previous poses, velocities, forces), the persistent SAP state (fat AABBs,
+ * endpoint order and keys) and the joints' state (drive targets, rows and
+ * their multipliers) -- for callers that fork rollouts from one state and
+ * rewind (sample-based MPC, determinism replays).  The reference has no
+ * snapshot API; its design note (docs/design/world-snapshot-restore/
+ * world-snapshot-restore.md) asks for a pool of pre-allocated slots and a
+ * bit-exact restore, which this provides on the device.  Each call takes a
+ * new slot (device memory owned by the batch, freed with it), copies
+ * asynchronously on the batch stream and returns its id in *slot_out. */
+RBPS_API int rbps_batch_snapshot(rbps_batch *batch, uint32_t *slot_out);
+/* Copies snapshot `slot` back over the batch state (asynchronous on the
+ * batch stream); stepping on from it repeats the original run bit for bit. */
+RBPS_API int rbps_batch_restore(rbps_batch *batch, uint32_t slot);
+/* Overwrites snapshot `slot` with the current state. */
+RBPS_API int rbps_batch_snapshot_update(rbps_batch *batch, uint32_t slot);
 
 /* Per-world body state, host doubles (converted from the device precision). */
 RBPS_API int rbps_batch_get_state(rbps_batch *batch, uint32_t world, const rbps_state_view *view);

@@ -77,6 +77,10 @@ def lib():
             "rbps_world_set_body_force": (i, [_P, C.c_uint32, C.c_uint32, _D, _D]),
             "rbps_world_set_body_forces": (i, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _D]),
             "rbps_batch_step_io": (i, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+            "rbps_batch_step_io_async": (i, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+            "rbps_batch_snapshot": (i, [_P, C.POINTER(C.c_uint32)]),
+            "rbps_batch_snapshot_update": (i, [_P, C.c_uint32]),
+            "rbps_batch_restore": (i, [_P, C.c_uint32]),
             "rbps_world_add_collider": (i, [_P, C.c_uint32, _P, _U]),
             "rbps_world_add_colliders": (i, [_P, C.c_uint32, C.c_uint32, _P, _U]),
             "rbps_world_add_joint": (i, [_P, C.c_uint32, _P, _U]),
@@ -277,6 +281,24 @@ class Batch:
     def step_io(self, force_ptr, pos_ptr, rot_ptr):
         """One step with host I/O through raw host pointers (ints or None)."""
         _check(lib().rbps_batch_step_io(self.h, force_ptr, pos_ptr, rot_ptr))
+
+    def snapshot(self):
+        """Device-side snapshot of the whole batch state; returns its slot."""
+        slot = C.c_uint32(0)
+        _check(lib().rbps_batch_snapshot(self.h, C.byref(slot)))
+        return slot.value
+
+    def snapshot_update(self, slot):
+        _check(lib().rbps_batch_snapshot_update(self.h, slot))
+
+    def restore(self, slot):
+        """Rewinds every world to snapshot `slot`."""
+        _check(lib().rbps_batch_restore(self.h, slot))
+
+    def step_io_async(self, force_ptr, pos_ptr, rot_ptr):
+        """step_io without the wait: the copies overlap neighbouring steps;
+        the host buffers are final after synchronize()."""
+        _check(lib().rbps_batch_step_io_async(self.h, force_ptr, pos_ptr, rot_ptr))
 
     def set_dump(self, on=True):
         _check(lib().rbps_batch_set_dump(self.h, 1 if on else 0))

@@ -418,10 +418,34 @@ struct rbps_batch
     bool graph_ok = true;    // false once capture was refused: launch directly
     uint64_t graph_launches = 0;
 
+    // pipelined host I/O (rbps_batch_step_io_async): an input and an output
+    // copy stream (so a step's force copy never queues behind the previous
+    // step's pose copy), two device staging slots and their events
+    cudaStream_t io_stream = nullptr, io_out_stream = nullptr;
+    double *io_f2[2] = {nullptr, nullptr}, *io_p2[2] = {nullptr, nullptr}, *io_r2[2] = {nullptr, nullptr};
+    cudaEvent_t ev_force_ready[2] = {}, ev_force_free[2] = {}, ev_pose_ready[2] = {}, ev_out_free[2] = {};
+    uint32_t io_slot = 0;
+    bool io_async_ready = false;
+    // snapshot slots (rbps_batch_snapshot): one device buffer each, holding
+    // the state arrays back to back
+    std::vector<char *> snaps;
+
     ~rbps_batch()
     {
+        if (io_stream)
+            cudaStreamSynchronize(io_stream);
+        if (io_out_stream)
+            cudaStreamSynchronize(io_out_stream);
         if (stream)
             cudaStreamSynchronize(stream);
+        for (int k = 0; k < 2; ++k)
+            for (cudaEvent_t e : {ev_force_ready[k], ev_force_free[k], ev_pose_ready[k], ev_out_free[k]})
+                if (e)
+                    cudaEventDestroy(e);
+        if (io_stream)
+            cudaStreamDestroy(io_stream);
+        if (io_out_stream)
+            cudaStreamDestroy(io_out_stream);
         if (graph_exec)
             cudaGraphExecDestroy(graph_exec);
         for (void *p : allocs)
@@ -506,6 +530,10 @@ extern "C" int rbps_batch_create(const rbps_batch_desc *desc, rbps_batch **out)
     b->block = desc->block_threads ? (int)desc->block_threads : 128;
     for (int k = 0; k < kNumPhaseKernels; ++k)
         b->phase.block[k] = b->block;
+    // the frame kernel's duration is the largest world's SAP on one CTA:
+    // twice the threads for it (8.58 -> 8.26 ms a step on 4,096 uneven worlds)
+    if (!desc->block_threads)
+        b->phase.block[kKFrame] = 256;
     *out = b.release();
     return RBPS_OK;
 }
@@ -1409,13 +1437,15 @@ static long enqueue_step(rbps_batch *b, const Engine<T, P> &e)
         {
             if (launch_step_flat<T, P>(e, b->phase, b->flat, b->stream) != cudaSuccess)
                 return RBPS_ERR_CUDA;
-            launches += 3 + 6 * (long)b->desc.substeps;
+            // frame, prefix, 3 class-sort kernels, stats; per substep the
+            // narrowphase, the GJK pass (batches with hulls) and the substep
+            launches += 6 + (long)b->desc.substeps * (e.gjk_list ? 3 : 2);
         }
         else
         {
             if (launch_step_phases<T, P>(e, b->phase, b->stream) != cudaSuccess)
                 return RBPS_ERR_CUDA;
-            launches += b->n_counters;
+            launches += b->n_counters + (e.gjk_list ? (long)b->desc.substeps : 0); // + the GJK passes
         }
     }
     for (uint32_t w : b->big_ids)
@@ -1531,6 +1561,10 @@ extern "C" int rbps_batch_synchronize(rbps_batch *b)
         return fail(RBPS_ERR_INVALID, "rbps_batch_synchronize: commit first");
     CU(cudaSetDevice(b->desc.device));
     CU(cudaStreamSynchronize(b->stream));
+    if (b->io_stream)
+        CU(cudaStreamSynchronize(b->io_stream));
+    if (b->io_out_stream)
+        CU(cudaStreamSynchronize(b->io_out_stream));
     return check_device_error(b);
 }
 
@@ -2092,6 +2126,154 @@ static int step_io_typed(rbps_batch *b, const double *force_in, double *pos_out,
     }
     CU(cudaStreamSynchronize(b->stream));
     return check_device_error(b);
+}
+
+// Pipelined variant: call k uses staging slot s = k % 2.
+//   input stream:   [wait force_free[s]] H2D force -> io_f2[s], record force_ready[s]
+//   compute stream: [wait force_ready[s]] forces in, record force_free[s], step,
+//                   [wait out_free[s]] poses -> io_p2/io_r2[s], record pose_ready[s]
+//   output stream:  [wait pose_ready[s]] D2H poses, record out_free[s]
+// so the copies of call k overlap the compute of calls k - 1 and k + 1.
+template <class T, class P>
+static int step_io_async_typed(rbps_batch *b, const double *force_in, double *pos_out, double *rot_out)
+{
+    const uint32_t n = b->n_bodies_all;
+    int rc;
+    if (!b->io_async_ready)
+    {
+        CU(cudaStreamCreateWithFlags(&b->io_stream, cudaStreamNonBlocking));
+        CU(cudaStreamCreateWithFlags(&b->io_out_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k)
+        {
+            if ((rc = b->alloc((void **)&b->io_f2[k], (size_t)n * 3 * 8)) ||
+                (rc = b->alloc((void **)&b->io_p2[k], (size_t)n * 3 * 8)) ||
+                (rc = b->alloc((void **)&b->io_r2[k], (size_t)n * 4 * 8)))
+                return rc;
+            for (cudaEvent_t *e : {&b->ev_force_ready[k], &b->ev_force_free[k], &b->ev_pose_ready[k], &b->ev_out_free[k]})
+                CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            // every slot starts free
+            CU(cudaEventRecord(b->ev_force_free[k], b->stream));
+            CU(cudaEventRecord(b->ev_out_free[k], b->io_out_stream));
+        }
+        CU(cudaDeviceSynchronize());
+        b->io_async_ready = true;
+    }
+    const uint32_t s = b->io_slot;
+    b->io_slot ^= 1u;
+    Engine<T, P> e = make_engine<T, P>(b);
+    const int grid = std::max(1, std::min<int>(b->sm_count * 8, (int)((n + 255) / 256)));
+    if (force_in)
+    {
+        CU(cudaStreamWaitEvent(b->io_stream, b->ev_force_free[s], 0));
+        CU(cudaMemcpyAsync(b->io_f2[s], force_in, (size_t)n * 3 * 8, cudaMemcpyHostToDevice, b->io_stream));
+        CU(cudaEventRecord(b->ev_force_ready[s], b->io_stream));
+        CU(cudaStreamWaitEvent(b->stream, b->ev_force_ready[s], 0));
+        CU(launch_io<T, P>(e, 0, b->io_f2[s], nullptr, n, grid, b->stream));
+        CU(cudaEventRecord(b->ev_force_free[s], b->stream));
+    }
+    if ((rc = step_typed<T, P>(b, 1)))
+        return rc;
+    b->steps_done += 1;
+    if (pos_out || rot_out)
+    {
+        CU(cudaStreamWaitEvent(b->stream, b->ev_out_free[s], 0));
+        CU(launch_io<T, P>(e, 1, b->io_p2[s], b->io_r2[s], n, grid, b->stream));
+        CU(cudaEventRecord(b->ev_pose_ready[s], b->stream));
+        CU(cudaStreamWaitEvent(b->io_out_stream, b->ev_pose_ready[s], 0));
+        if (pos_out)
+            CU(cudaMemcpyAsync(pos_out, b->io_p2[s], (size_t)n * 3 * 8, cudaMemcpyDeviceToHost, b->io_out_stream));
+        if (rot_out)
+            CU(cudaMemcpyAsync(rot_out, b->io_r2[s], (size_t)n * 4 * 8, cudaMemcpyDeviceToHost, b->io_out_stream));
+        CU(cudaEventRecord(b->ev_out_free[s], b->io_out_stream));
+    }
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_step_io_async(rbps_batch *b, const double *force_in, double *position_out,
+                                        double *orientation_out)
+{
+    if (!b || !b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_step_io_async: commit first");
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, step_io_async_typed, b, force_in, position_out, orientation_out);
+}
+
+// ------------------------------------------------------------ snapshots
+// The device arrays that carry state from one step to the next.  Everything
+// else on the device is either constant after commit (shapes, inertia,
+// layouts) or rebuilt every frame (candidates, contacts, colours).
+template <class T, class P>
+static std::vector<std::pair<void *, size_t>> state_arrays(rbps_batch *b)
+{
+    const size_t nb = b->n_bodies_all, nbp = b->n_bp_all;
+    std::vector<std::pair<void *, size_t>> v = {
+        {b->pos, nb * sizeof(V4<P>)},      {b->prev_pos, nb * sizeof(V4<P>)},
+        {b->rot, nb * sizeof(Q4<T>)},      {b->prev_rot, nb * sizeof(Q4<T>)},
+        {b->lin, nb * sizeof(V4<T>)},      {b->ang, nb * sizeof(V4<T>)},
+        {b->force, nb * sizeof(V4<T>)},    {b->torque, nb * sizeof(V4<T>)},
+        {b->fat, nbp * sizeof(FatBox)},    {b->ep_key, 2 * nbp * sizeof(uint32_t)},
+        {b->ep_id, 2 * nbp * sizeof(uint32_t)}, {b->ep_pos, 2 * nbp * sizeof(uint32_t)},
+        {b->joints_d, (size_t)b->n_joint_all * sizeof(Joint<T>)},
+        {b->rows_d, (size_t)b->n_row_all * sizeof(Row<T>)}};
+    std::vector<std::pair<void *, size_t>> out;
+    for (auto &a : v)
+        if (a.first && a.second)
+            out.push_back(a);
+    return out;
+}
+
+// dir 0: state -> slot, 1: slot -> state
+template <class T, class P>
+static int snapshot_copy(rbps_batch *b, char *slot, int dir)
+{
+    size_t off = 0;
+    for (auto &a : state_arrays<T, P>(b))
+    {
+        void *dst = dir == 0 ? (void *)(slot + off) : a.first;
+        const void *src = dir == 0 ? a.first : (const void *)(slot + off);
+        CU(cudaMemcpyAsync(dst, src, a.second, cudaMemcpyDeviceToDevice, b->stream));
+        off += (a.second + 255) / 256 * 256;
+    }
+    return RBPS_OK;
+}
+
+template <class T, class P>
+static int snapshot_new(rbps_batch *b, uint32_t *slot_out)
+{
+    size_t bytes = 0;
+    for (auto &a : state_arrays<T, P>(b))
+        bytes += (a.second + 255) / 256 * 256;
+    char *p = nullptr;
+    int rc = b->alloc((void **)&p, std::max<size_t>(bytes, 256));
+    if (rc)
+        return rc;
+    b->snaps.push_back(p);
+    *slot_out = (uint32_t)(b->snaps.size() - 1);
+    return snapshot_copy<T, P>(b, p, 0);
+}
+
+extern "C" int rbps_batch_snapshot(rbps_batch *b, uint32_t *slot_out)
+{
+    if (!b || !b->committed || !slot_out)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_snapshot: commit first, and pass slot_out");
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, snapshot_new, b, slot_out);
+}
+
+extern "C" int rbps_batch_snapshot_update(rbps_batch *b, uint32_t slot)
+{
+    if (!b || !b->committed || slot >= b->snaps.size())
+        return fail(RBPS_ERR_INVALID, "rbps_batch_snapshot_update: no snapshot %u", slot);
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, snapshot_copy, b, b->snaps[slot], 0);
+}
+
+extern "C" int rbps_batch_restore(rbps_batch *b, uint32_t slot)
+{
+    if (!b || !b->committed || slot >= b->snaps.size())
+        return fail(RBPS_ERR_INVALID, "rbps_batch_restore: no snapshot %u", slot);
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, snapshot_copy, b, b->snaps[slot], 1);
 }
 
 extern "C" int rbps_batch_step_io(rbps_batch *b, const double *force_in, double *position_out, double *orientation_out)
