@@ -551,7 +551,7 @@ namespace rbps_gpu
 
     // Narrowphase of one candidate (the analytic routines); returns
     // kNeedsGjk for a pair the GJK pass handles (its rows are left empty).
-    template <class T, class P>
+    template <class T, class P, int Sel = kSelAll>
     __device__ __forceinline__ int narrow_candidate(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
                                                     CandContacts<T, P> &out)
     {
@@ -567,7 +567,7 @@ namespace rbps_gpu
         const tf<T> tb = collider_tf(E, gcb, gbb);
         Manifold<T> m;
         m.n = 0;
-        const int res = dispatch_pair(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, m);
+        const int res = dispatch_pair<T, Sel>(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, m);
         emit_manifold(E, gca, gcb, gba, gbb, m, res == kHit ? m.n : 0, out);
         return res;
     }
@@ -1159,7 +1159,8 @@ namespace rbps_gpu
     //                    the candidates of all worlds sorted by shape pair, so a
     //                    warp of the narrowphase runs one pair routine
     // and per substep:
-    //   k_flat_narrow    one thread per candidate, in shape-pair order
+    //   k_flat_narrow    one thread per candidate, in shape-pair order; the
+    //                    box-box class in k_flat_narrow_boxbox
     //   k_substep        one CTA per large world, one warp per other world:
     //                    greedy colouring of the contacting candidates, integrate,
     //                    position solve (colour by colour, joint errors, joint
@@ -1198,6 +1199,7 @@ namespace rbps_gpu
     {
         return kind == kSphere ? 0u : kind == kBox ? 1u : kind == kCapsule ? 2u : kind == kPlane ? 3u : 4u;
     }
+    constexpr uint32_t kClassBoxBox = 1u * 5u + 1u; // cand_class of a box-box pair
 
     // The small world holding flat candidate f: last q with wcoff[q] <= f.
     template <class T, class P>
@@ -1297,21 +1299,41 @@ namespace rbps_gpu
         }
     }
 
-    // Narrowphase of every candidate of the small worlds, in class order.
+    // Narrowphase of flat entry i of the class-sorted candidate list of the
+    // small worlds.
+    template <class T, class P, int Sel>
+    __device__ __forceinline__ void narrow_flat(const Engine<T, P> &E, uint32_t i)
+    {
+        const uint2 e = E.nlist[i];
+        const WorldDev W = E.worlds[e.x];
+        uint32_t n_gjk = 0;
+        if (narrow_candidate<T, P, Sel>(E, W, E.wcand[e.x][e.y], E.wcc[e.x][e.y]) == kNeedsGjk)
+            queue_gjk(E, e.x, e.y, n_gjk);
+        if (n_gjk)
+            atomicAdd(world_scratch(E, W).misc + kMiscNGjk, n_gjk);
+    }
+
+    // Narrowphase of every candidate of the small worlds but the box-box
+    // ones, in class order.
     template <class T, class P>
     __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow(const Engine<T, P> E)
     {
+        // every class but box-box: [0, off(bb)) and [off(bb + 1), total)
         const uint32_t total = E.gcol[kGcolOff + kPairClasses];
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
-        {
-            const uint2 e = E.nlist[i];
-            const WorldDev W = E.worlds[e.x];
-            uint32_t n_gjk = 0;
-            if (narrow_candidate(E, W, E.wcand[e.x][e.y], E.wcc[e.x][e.y]) == kNeedsGjk)
-                queue_gjk(E, e.x, e.y, n_gjk);
-            if (n_gjk)
-                atomicAdd(world_scratch(E, W).misc + kMiscNGjk, n_gjk);
-        }
+        const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
+        const uint32_t n = total - (bb1 - bb0);
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+            narrow_flat<T, P, kSelNoBoxBox>(E, k < bb0 ? k : k + (bb1 - bb0));
+    }
+
+    // The box-box class on its own: its SAT, clipping buffers and registers
+    // stay out of the kernel that runs every other class.
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow_boxbox(const Engine<T, P> E)
+    {
+        const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
+        for (uint32_t i = bb0 + blockIdx.x * blockDim.x + threadIdx.x; i < bb1; i += gridDim.x * blockDim.x)
+            narrow_flat<T, P, kSelBoxBox>(E, i);
     }
 
     // Jones-Plassmann colouring of one world's contacting candidates by one
@@ -1813,6 +1835,7 @@ namespace rbps_gpu
             if (e.gjk_list)
                 cudaMemsetAsync(e.gjk_count, 0, 4, stream);
             k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+            k_flat_narrow_boxbox<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
             launch_gjk(e, stream);
             k_substep<T, P><<<fl.grid_solve, 128, fl.substep_smem, stream>>>(e);
         }

@@ -948,10 +948,21 @@ namespace rbps_gpu
     };
 
     // dispatch (Dispatcher.hpp:212-217) over the analytic table.
-    template <class T>
-    __device__ int dispatch_pair(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &sb, const tf<T> &tb,
-                                 const HullSetDev &hs, Manifold<T> &m)
+    // Sel selects the routines compiled in: kSelAll every pair; kSelNoBoxBox
+    // all but box-box; kSelBoxBox box-box only (the caller guarantees the
+    // kinds), so a kernel that never meets a box pair carries no box-box
+    // code, registers or clip buffers.
+    constexpr int kSelAll = 0, kSelNoBoxBox = 1, kSelBoxBox = 2;
+
+    template <class T, int Sel = kSelAll>
+    __device__ __forceinline__ int dispatch_pair(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &sb,
+                                                 const tf<T> &tb, const HullSetDev &hs, Manifold<T> &m)
     {
+        if constexpr (Sel == kSelBoxBox)
+            return box_box(vec3<T>(T(sa.p[0]), T(sa.p[1]), T(sa.p[2])), ta, vec3<T>(T(sb.p[0]), T(sb.p[1]), T(sb.p[2])),
+                           tb, m)
+                       ? kHit
+                       : kMiss;
         const int ka = sa.kind, kb = sb.kind;
         bool hit = false;
         bool flip = false;
@@ -992,7 +1003,7 @@ namespace rbps_gpu
             hit = sphere_box(T(sb.p[0]), tb, vec3<T>(T(sa.p[0]), T(sa.p[1]), T(sa.p[2])), ta, m);
             flip = true;
         }
-        else if (ka == kBox && kb == kBox)
+        else if (Sel == kSelAll && ka == kBox && kb == kBox)
             hit = box_box(vec3<T>(T(sa.p[0]), T(sa.p[1]), T(sa.p[2])), ta, vec3<T>(T(sb.p[0]), T(sb.p[1]), T(sb.p[2])), tb, m);
         else if (ka == kSphere && kb == kCapsule)
             hit = sphere_capsule(T(sa.p[0]), ta, T(sb.p[0]), T(sb.p[1]), tb, m);
