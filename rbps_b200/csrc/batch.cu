@@ -446,6 +446,18 @@ struct rbps_batch
             cudaStreamDestroy(io_stream);
         if (io_out_stream)
             cudaStreamDestroy(io_out_stream);
+        if (flat.side)
+        {
+            cudaStreamSynchronize(flat.side);
+            for (int k = 0; k < 8; ++k)
+            {
+                if (flat.fork[k])
+                    cudaEventDestroy(flat.fork[k]);
+                if (flat.join[k])
+                    cudaEventDestroy(flat.join[k]);
+            }
+            cudaStreamDestroy(flat.side);
+        }
         if (graph_exec)
             cudaGraphExecDestroy(graph_exec);
         for (void *p : allocs)
@@ -1329,6 +1341,13 @@ static int commit_typed(rbps_batch *b)
                                         smem_world_bytes<T, P>(b->smem_cap_block));
         CU(prepare_substep<T, P>(b->flat.substep_smem));
         b->use_flat = true;
+        // side stream + events for the parallel narrowphase kernels
+        CU(cudaStreamCreateWithFlags(&b->flat.side, cudaStreamNonBlocking));
+        for (int k = 0; k < 8; ++k)
+        {
+            CU(cudaEventCreateWithFlags(&b->flat.fork[k], cudaEventDisableTiming));
+            CU(cudaEventCreateWithFlags(&b->flat.join[k], cudaEventDisableTiming));
+        }
     }
     // ---- GJK pass: only batches with hull colliders reach it
     {

@@ -1834,8 +1834,22 @@ namespace rbps_gpu
         {
             if (e.gjk_list)
                 cudaMemsetAsync(e.gjk_count, 0, 4, stream);
-            k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
-            k_flat_narrow_boxbox<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+            if (fl.side && s < 8)
+            {
+                // the two narrowphase kernels touch disjoint candidates: run
+                // them side by side (a fork / join the graph capture keeps)
+                cudaEventRecord(fl.fork[s], stream);
+                cudaStreamWaitEvent(fl.side, fl.fork[s], 0);
+                k_flat_narrow_boxbox<T, P><<<fl.grid_narrow, kMaxBlock, 0, fl.side>>>(e);
+                cudaEventRecord(fl.join[s], fl.side);
+                k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+                cudaStreamWaitEvent(stream, fl.join[s], 0);
+            }
+            else
+            {
+                k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+                k_flat_narrow_boxbox<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+            }
             launch_gjk(e, stream);
             k_substep<T, P><<<fl.grid_solve, 128, fl.substep_smem, stream>>>(e);
         }

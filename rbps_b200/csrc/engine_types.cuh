@@ -268,6 +268,10 @@ namespace rbps_gpu
     {
         int grid_narrow, grid_solve, block_solve;
         size_t substep_smem; // dynamic shared memory of k_substep
+        // a second stream on which the box-box narrowphase runs beside the
+        // other classes' (fork / join events), or null for one stream
+        cudaStream_t side;
+        cudaEvent_t fork[8], join[8]; // one pair per substep (substeps <= 8), else sequential
     };
     template <class T, class P>
     cudaError_t launch_step_flat(const Engine<T, P> &e, const PhaseLaunch &pl, const FlatLaunch &fl,
