@@ -71,7 +71,10 @@ enum { RBPS_BODY_STATIC = 0, RBPS_BODY_DYNAMIC = 1 };
 enum {
     RBPS_SHAPE_SPHERE = 0,
     RBPS_SHAPE_BOX = 1,
+    RBPS_SHAPE_ELLIPSOID = 2,   /* params = semi-axes a, b, c (Ellipsoid.hpp)        */
     RBPS_SHAPE_CAPSULE = 3,
+    RBPS_SHAPE_CYLINDER = 4,    /* params = half_height, base_radius; axis local +Y  */
+    RBPS_SHAPE_CONE = 5,        /* params = half_height, base_radius; apex at +Y     */
     RBPS_SHAPE_PLANE = 6,
     RBPS_SHAPE_CONVEX_HULL = 9
 };

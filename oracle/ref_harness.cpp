@@ -173,6 +173,9 @@ namespace
         case RBPS_SHAPE_SPHERE: out = rbc::Sphere(d->params[0]); return true;
         case RBPS_SHAPE_BOX: out = rbc::Box(v3(d->params)); return true;
         case RBPS_SHAPE_CAPSULE: out = rbc::Capsule(d->params[0], d->params[1]); return true;
+        case RBPS_SHAPE_ELLIPSOID: out = rbc::Ellipsoid(v3(d->params)); return true;
+        case RBPS_SHAPE_CYLINDER: out = rbc::Cylinder(d->params[0], d->params[1]); return true;
+        case RBPS_SHAPE_CONE: out = rbc::Cone(d->params[0], d->params[1]); return true;
         case RBPS_SHAPE_PLANE: out = rbc::Plane(v3(d->params), d->params[3]); return true;
         case RBPS_SHAPE_CONVEX_HULL:
             if (d->hull >= rw->hulls.size())

@@ -32,7 +32,10 @@ BODY_DYNAMIC = 1
 # rbc::Shape variant indices (rbc/shapes/ShapeTypes.hpp:67-69)
 SHAPE_SPHERE = 0
 SHAPE_BOX = 1
+SHAPE_ELLIPSOID = 2
 SHAPE_CAPSULE = 3
+SHAPE_CYLINDER = 4
+SHAPE_CONE = 5
 SHAPE_PLANE = 6
 SHAPE_CONVEX_HULL = 9
 

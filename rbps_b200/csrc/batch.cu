@@ -293,6 +293,15 @@ namespace
     size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 } // namespace
 
+// Shapes the device narrowphase covers: the reference's Sphere, Box,
+// Ellipsoid, Capsule, Cylinder, Cone, Plane and ConvexHull (ShapeTypes.hpp);
+// Heightmap and Mesh are not on the device path.
+static bool shape_supported(int s)
+{
+    return s == RBPS_SHAPE_SPHERE || s == RBPS_SHAPE_BOX || s == RBPS_SHAPE_ELLIPSOID || s == RBPS_SHAPE_CAPSULE ||
+           s == RBPS_SHAPE_CYLINDER || s == RBPS_SHAPE_CONE || s == RBPS_SHAPE_PLANE || s == RBPS_SHAPE_CONVEX_HULL;
+}
+
 struct rbps_batch
 {
     rbps_batch_desc desc;
@@ -663,8 +672,7 @@ extern "C" int rbps_world_add_colliders(rbps_batch *b, uint32_t world, uint32_t 
         const rbps_collider_desc &c = d[i];
         if (c.body_id >= w.bodies.size())
             return fail(RBPS_ERR_INVALID, "collider body %u does not exist", c.body_id);
-        if (c.shape != RBPS_SHAPE_SPHERE && c.shape != RBPS_SHAPE_BOX && c.shape != RBPS_SHAPE_CAPSULE &&
-            c.shape != RBPS_SHAPE_PLANE && c.shape != RBPS_SHAPE_CONVEX_HULL)
+        if (!shape_supported(c.shape))
             return fail(RBPS_ERR_INVALID, "unsupported shape kind %d", c.shape);
         if (c.shape == RBPS_SHAPE_CONVEX_HULL && c.hull >= b->hulls.size())
             return fail(RBPS_ERR_INVALID, "hull %u does not exist", c.hull);
@@ -1358,7 +1366,7 @@ static int commit_typed(rbps_batch *b)
             const WorldDev &d = b->wdev[w];
             cap += (size_t)d.pair_cap + 1 + d.n_pc;
             for (const auto &c : b->worlds[w].colliders)
-                any_hull = any_hull || c.shape == RBPS_SHAPE_CONVEX_HULL;
+                any_hull = any_hull || gjk_kind(c.shape); // pairs that go through GJK / EPA
         }
         if (any_hull && cap)
         {
@@ -2046,7 +2054,7 @@ static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> 
     const size_t shape_bytes = (size_t)n * sizeof(ShapeDev), tf_bytes = (size_t)n * 7 * sizeof(double);
     bool gjk = false;
     for (uint32_t i = 0; i < n && !gjk; ++i)
-        gjk = (sa[i].kind == kHull || sb[i].kind == kHull) && sa[i].kind != kPlane && sb[i].kind != kPlane;
+        gjk = (gjk_kind(sa[i].kind) || gjk_kind(sb[i].kind)) && sa[i].kind != kPlane && sb[i].kind != kPlane;
     // GJK pairs need a workspace per thread: fewer threads, each looping
     const uint32_t threads = (uint32_t)std::min<size_t>(((size_t)n + 127) / 128 * 128, gjk ? 1024 : 65536);
     const size_t ws_bytes = gjk ? gjk_work_bytes<T, P>() * threads : 0;
@@ -2091,8 +2099,7 @@ extern "C" int rbps_batch_collide(rbps_batch *b, uint32_t n, const rbps_collider
         for (int side = 0; side < 2; ++side)
         {
             const rbps_collider_desc &c = side ? bd[i] : a[i];
-            if (c.shape != RBPS_SHAPE_SPHERE && c.shape != RBPS_SHAPE_BOX && c.shape != RBPS_SHAPE_CAPSULE &&
-                c.shape != RBPS_SHAPE_PLANE && c.shape != RBPS_SHAPE_CONVEX_HULL)
+            if (!shape_supported(c.shape))
                 return fail(RBPS_ERR_INVALID, "rbps_batch_collide: pair %u has an unknown shape %d", i, c.shape);
             if (c.shape == RBPS_SHAPE_CONVEX_HULL)
             {

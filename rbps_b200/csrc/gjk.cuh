@@ -106,6 +106,10 @@ namespace rbps_gpu
                 return endpoint;
             return endpoint + (d / len) * T(s.p[1]);
         }
+        case kEllipsoid:
+        case kCylinder:
+        case kCone:
+            return support_round<T>(s.kind, s.p, d);
         default: // ConvexHull.hpp:457-472
         {
             const uint32_t v0 = hs.v_off[s.hull], v1 = hs.v_off[s.hull + 1];

@@ -22,10 +22,59 @@ namespace rbps_gpu
     {
         kSphere = 0,
         kBox = 1,
+        kEllipsoid = 2,
         kCapsule = 3,
+        kCylinder = 4,
+        kCone = 5,
         kPlane = 6,
         kHull = 9
     };
+
+    // Shapes whose pairs (other than with a plane) go through GJK / EPA
+    // (gjk_convex_v, Dispatcher.hpp:40-60): the generic convex path.
+    RBPS_HD bool gjk_kind(int k) { return k == kHull || k == kEllipsoid || k == kCylinder || k == kCone; }
+
+    // Local support points (Ellipsoid.hpp, Cylinder.hpp, Cone.hpp support()).
+    template <class T> RBPS_HD vec3<T> support_ellipsoid(const vec3<T> &a, const vec3<T> &d)
+    {
+        const vec3<T> scaled(a.x * a.x * d.x, a.y * a.y * d.y, a.z * a.z * d.z);
+        const T denom = sqrt_t(a.x * a.x * d.x * d.x + a.y * a.y * d.y * d.y + a.z * a.z * d.z * d.z);
+        if (denom < T(kEpsilon))
+            return vec3<T>(a.x, T(0.0), T(0.0));
+        const T inv = T(1.0) / denom; // vec3::operator/ multiplies by the reciprocal
+        return vec3<T>(scaled.x * inv, scaled.y * inv, scaled.z * inv);
+    }
+    template <class T> RBPS_HD vec3<T> support_cylinder(T hh, T r, const vec3<T> &d)
+    {
+        const T sy = (d.y >= T(0.0)) ? hh : -hh;
+        const T d_radial = sqrt_t(d.x * d.x + d.z * d.z);
+        if (d_radial < T(kEpsilon))
+            return vec3<T>(r, sy, T(0.0));
+        const T scale = r / d_radial;
+        return vec3<T>(d.x * scale, sy, d.z * scale);
+    }
+    template <class T> RBPS_HD vec3<T> support_cone(T hh, T r, const vec3<T> &d)
+    {
+        const T d_radial = sqrt_t(d.x * d.x + d.z * d.z);
+        if (d_radial < T(kEpsilon))
+            return (d.y >= T(0.0)) ? vec3<T>(T(0.0), hh, T(0.0)) : vec3<T>(r, -hh, T(0.0));
+        const T apex_dot = d.y * hh;
+        const T base_edge_dot = d_radial * r - d.y * hh;
+        if (apex_dot >= base_edge_dot)
+            return vec3<T>(T(0.0), hh, T(0.0));
+        const T scale = r / d_radial;
+        return vec3<T>(d.x * scale, -hh, d.z * scale);
+    }
+    // the three above by shape kind (params: ellipsoid semi-axes; cylinder
+    // and cone half_height, base_radius)
+    template <class T> RBPS_HD vec3<T> support_round(int kind, const double *p, const vec3<T> &d)
+    {
+        if (kind == kEllipsoid)
+            return support_ellipsoid(vec3<T>(T(p[0]), T(p[1]), T(p[2])), d);
+        if (kind == kCylinder)
+            return support_cylinder(T(p[0]), T(p[1]), d);
+        return support_cone(T(p[0]), T(p[1]), d);
+    }
 
     // Hull geometry of one batch: vertices (double, local frame) per hull.
     // Bases of one hull's polygon / adjacency tables (ConvexHullData,
@@ -106,6 +155,30 @@ namespace rbps_gpu
                                  rabs(R.c[0].y) * half.x + rabs(R.c[1].y) * half.y + rabs(R.c[2].y) * half.z,
                                  rabs(R.c[0].z) * half.x + rabs(R.c[1].z) * half.y + rabs(R.c[2].z) * half.z);
             return {wc - e, wc + e};
+        }
+        if (s.kind == kEllipsoid) // Ellipsoid.hpp compute_aabb
+        {
+            const mat3<double> R = mat3_cast(t.rot);
+            const vec3<double> a(s.p[0], s.p[1], s.p[2]);
+            const vec3<double> e(
+                sqrt_t(R.c[0].x * R.c[0].x * a.x * a.x + R.c[1].x * R.c[1].x * a.y * a.y + R.c[2].x * R.c[2].x * a.z * a.z),
+                sqrt_t(R.c[0].y * R.c[0].y * a.x * a.x + R.c[1].y * R.c[1].y * a.y * a.y + R.c[2].y * R.c[2].y * a.z * a.z),
+                sqrt_t(R.c[0].z * R.c[0].z * a.x * a.x + R.c[1].z * R.c[1].z * a.y * a.y + R.c[2].z * R.c[2].z * a.z * a.z));
+            return {t.pos - e, t.pos + e};
+        }
+        if (s.kind == kCylinder || s.kind == kCone) // Cylinder.hpp / Cone.hpp compute_aabb
+        {
+            const vec3<double> axes[6] = {vec3<double>(1, 0, 0), vec3<double>(-1, 0, 0), vec3<double>(0, 1, 0),
+                                          vec3<double>(0, -1, 0), vec3<double>(0, 0, 1), vec3<double>(0, 0, -1)};
+            vec3<double> mn = t.pos, mx = t.pos;
+            for (int k = 0; k < 6; ++k)
+            {
+                const vec3<double> ld = t.inverse_rotate_vector(axes[k]);
+                const vec3<double> ws = t.pos + t.rotate_vector(support_round<double>(s.kind, s.p, ld));
+                mn = vec3<double>(rmin(mn.x, ws.x), rmin(mn.y, ws.y), rmin(mn.z, ws.z));
+                mx = vec3<double>(rmax(mx.x, ws.x), rmax(mx.y, ws.y), rmax(mx.z, ws.z));
+            }
+            return {mn, mx};
         }
         // Plane (Plane.hpp:46-50): infinite; planes never enter the SAP.
         const double inf = HUGE_VAL;
@@ -727,6 +800,92 @@ namespace rbps_gpu
         return true;
     }
 
+    // convex_vs_plane for Ellipsoid and Cone (PlaneCollision.hpp:40-61,
+    // RBC_PLANE_SPEC): the support point along -n, one contact.
+    template <class T>
+    __device__ bool round_plane(const ShapeDev &s, const tf<T> &ts, const ShapeDev &pl, const tf<T> &tp,
+                                Manifold<T> &out)
+    {
+        vec3<T> wn;
+        T wd;
+        plane_world(pl, tp, wn, wd);
+        const vec3<T> ld = ts.inverse_rotate_vector(-wn);
+        const vec3<T> ls = support_round<T>(s.kind, s.p, ld);
+        const vec3<T> ws = ts.pos + ts.rotate_vector(ls);
+        const T sd = dot(ws, wn) - wd;
+        if (sd >= T(0))
+            return false;
+        out.normal = -wn;
+        out.n = 1;
+        out.depth[0] = -sd;
+        out.pos[0] = ws;
+        return true;
+    }
+
+    // Cylinder vs Plane (PlaneCollision.hpp:416-536): the four cardinal rim
+    // points of the facing cap when the axis is within 10 degrees of the
+    // normal, else one rim point per cap, each kept when its distance is at
+    // most 1e-4f.
+    template <class T>
+    __device__ bool cylinder_plane(T hh, T r, const tf<T> &ta, const ShapeDev &pl, const tf<T> &tp, Manifold<T> &out)
+    {
+        vec3<T> wn;
+        T wd;
+        plane_world(pl, tp, wn, wd);
+        const vec3<T> axis = ta.rotate_vector(vec3<T>(T(0), T(1), T(0)));
+        const T cos_theta = dot(axis, wn);
+        const vec3<T> lneg = ta.inverse_rotate_vector(-wn);
+        const vec3<T> sl = support_cylinder(hh, r, lneg);
+        const vec3<T> sw = ta.transform_point(sl);
+        const T sdist = dot(sw, wn) - wd;
+        const T eps = T(1e-4f);
+        if (sdist > eps)
+            return false;
+        out.normal = -wn;
+        out.n = 0;
+        const T abs_cos = rabs(cos_theta);
+        if (abs_cos >= T(0.985f))
+        {
+            const T cap_sign = (cos_theta < T(0.0f)) ? T(1.0f) : T(-1.0f);
+            const vec3<T> cap = ta.pos + axis * (cap_sign * hh);
+            vec3<T> r1 = cross(axis, vec3<T>(T(1), T(0), T(0)));
+            if (dot(r1, r1) < T(1e-6f))
+                r1 = cross(axis, vec3<T>(T(0), T(0), T(1)));
+            r1 = normalize(r1);
+            const vec3<T> r2 = normalize(cross(axis, r1));
+            const vec3<T> rim[4] = {cap + r1 * r, cap - r1 * r, cap + r2 * r, cap - r2 * r};
+            for (int i = 0; i < 4; ++i)
+            {
+                const T dist = dot(rim[i], wn) - wd;
+                if (dist <= eps)
+                {
+                    out.pos[out.n] = rim[i];
+                    out.depth[out.n] = -dist;
+                    out.n++;
+                }
+            }
+        }
+        else
+        {
+            const T radial_len = sqrt_t(sl.x * sl.x + sl.z * sl.z);
+            vec3<T> radial_world(T(0), T(0), T(0));
+            if (radial_len > T(kEpsilon))
+                radial_world = ta.rotate_vector(vec3<T>(sl.x / radial_len * r, T(0.0f), sl.z / radial_len * r));
+            const vec3<T> pts[2] = {ta.pos + axis * hh + radial_world, ta.pos - axis * hh + radial_world};
+            for (int i = 0; i < 2; ++i)
+            {
+                const T dist = dot(pts[i], wn) - wd;
+                if (dist <= eps)
+                {
+                    out.pos[out.n] = pts[i];
+                    out.depth[out.n] = -dist;
+                    out.n++;
+                }
+            }
+        }
+        return out.n > 0;
+    }
+
     // Box vs Plane (PlaneCollision.hpp:289-337)
     template <class T>
     __device__ bool box_plane(const vec3<T> &h, const tf<T> &ta, const ShapeDev &pl, const tf<T> &tp, Manifold<T> &out)
@@ -976,6 +1135,10 @@ namespace rbps_gpu
                 hit = capsule_plane(T(sa.p[0]), T(sa.p[1]), ta, sb, tb, m);
             else if (ka == kHull)
                 hit = hull_plane(hs, sa.hull, ta, sb, tb, m);
+            else if (ka == kCylinder)
+                hit = cylinder_plane(T(sa.p[0]), T(sa.p[1]), ta, sb, tb, m);
+            else if (ka == kEllipsoid || ka == kCone)
+                hit = round_plane(sa, ta, sb, tb, m);
             return hit ? kHit : kMiss;
         }
         if (ka == kPlane)
@@ -988,11 +1151,15 @@ namespace rbps_gpu
                 hit = capsule_plane(T(sb.p[0]), T(sb.p[1]), tb, sa, ta, m);
             else if (kb == kHull)
                 hit = hull_plane(hs, sb.hull, tb, sa, ta, m);
+            else if (kb == kCylinder)
+                hit = cylinder_plane(T(sb.p[0]), T(sb.p[1]), tb, sa, ta, m);
+            else if (kb == kEllipsoid || kb == kCone)
+                hit = round_plane(sb, tb, sa, ta, m);
             if (hit)
                 m.normal = -m.normal;
             return hit ? kHit : kMiss;
         }
-        if (ka == kHull || kb == kHull)
+        if (gjk_kind(ka) || gjk_kind(kb))
             return kNeedsGjk;
         if (ka == kSphere && kb == kSphere)
             hit = sphere_sphere(T(sa.p[0]), ta, T(sb.p[0]), tb, m);

@@ -83,6 +83,34 @@ def capsule_mass(hh, r):
     return vol * DENSITY, np.array([ixx, iyy, ixx, 0.0, 0.0, 0.0]) * DENSITY
 
 
+def ellipsoid_mass(a):
+    """Ellipsoid.hpp compute_volume / compute_inertia_tensor (x density)."""
+    vol = (4.0 / 3.0) * PI * a[0] * a[1] * a[2]
+    ax2, ay2, az2 = a[0] * a[0], a[1] * a[1], a[2] * a[2]
+    inertia = np.array([(2.0 / 5.0) * vol * (ay2 + az2), (2.0 / 5.0) * vol * (ax2 + az2),
+                        (2.0 / 5.0) * vol * (ax2 + ay2), 0.0, 0.0, 0.0])
+    return vol * DENSITY, inertia * DENSITY
+
+
+def cylinder_mass(hh, r):
+    """Cylinder.hpp compute_volume / compute_inertia_tensor (x density)."""
+    vol = PI * r * r * (2.0 * hh)
+    r2, h2 = r * r, (2.0 * hh) * (2.0 * hh)
+    iyy = 0.5 * vol * r2
+    ixx = (1.0 / 12.0) * vol * (3.0 * r2 + h2)
+    return vol * DENSITY, np.array([ixx, iyy, ixx, 0.0, 0.0, 0.0]) * DENSITY
+
+
+def cone_mass(hh, r):
+    """Cone.hpp compute_volume / compute_inertia_tensor (x density)."""
+    vol = (1.0 / 3.0) * PI * r * r * (2.0 * hh)
+    r2, h = r * r, 2.0 * hh
+    iyy = (3.0 / 10.0) * vol * r2
+    ixx_apex = (3.0 / 5.0) * vol * (r2 / 4.0 + h * h)
+    d = 3.0 * h / 8.0 - hh
+    return vol * DENSITY, np.array([ixx_apex - vol * d * d, iyy, ixx_apex - vol * d * d, 0.0, 0.0, 0.0]) * DENSITY
+
+
 def hull_mass(verts, tris):
     """Volume and inertia about the origin of a closed CCW triangle mesh
     (signed tetrahedra from the origin), scaled by the density."""
@@ -491,6 +519,45 @@ def capsule_world(seed=0, n=48, friction=0.5, restitution=0.0):
             c = _collider(abi.SHAPE_BOX, h, bid, friction, restitution)
         else:
             r = rng.uniform(0.2, 0.5)
+            m, inertia = sphere_mass(r)
+            c = _collider(abi.SHAPE_SPHERE, [r], bid, friction, restitution)
+        b, f = _dyn_body(pos[i], quats[i], m, inertia)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(c)
+    return _finish(bodies, forces, colliders, [])
+
+
+def round_world(seed=0, n=24, friction=0.5, restitution=0.0):
+    """Ground plane + ellipsoids, cylinders, cones, boxes and spheres
+    dropped close to the ground: the ellipsoid / cylinder / cone plane
+    routines and their GJK / EPA pairs."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    bodies, forces, colliders = [], [], []
+    _ground(bodies, colliders, forces, friction, restitution)
+    kind = rng.integers(0, 5, n)
+    quats = random_quats(rng, n)
+    pos = rng.uniform((-2.0, 0.6, -2.0), (2.0, 3.0, 2.0), (n, 3))
+    for i in range(n):
+        bid = len(bodies)
+        if kind[i] == 0:
+            a = rng.uniform(0.2, 0.45, 3)
+            m, inertia = ellipsoid_mass(a)
+            c = _collider(abi.SHAPE_ELLIPSOID, a, bid, friction, restitution)
+        elif kind[i] == 1:
+            hh, r = rng.uniform(0.15, 0.4), rng.uniform(0.15, 0.4)
+            m, inertia = cylinder_mass(hh, r)
+            c = _collider(abi.SHAPE_CYLINDER, [hh, r], bid, friction, restitution)
+        elif kind[i] == 2:
+            hh, r = rng.uniform(0.15, 0.4), rng.uniform(0.15, 0.4)
+            m, inertia = cone_mass(hh, r)
+            c = _collider(abi.SHAPE_CONE, [hh, r], bid, friction, restitution)
+        elif kind[i] == 3:
+            h = rng.uniform(0.2, 0.4, 3)
+            m, inertia = box_mass(h)
+            c = _collider(abi.SHAPE_BOX, h, bid, friction, restitution)
+        else:
+            r = rng.uniform(0.2, 0.4)
             m, inertia = sphere_mass(r)
             c = _collider(abi.SHAPE_SPHERE, [r], bid, friction, restitution)
         b, f = _dyn_body(pos[i], quats[i], m, inertia)

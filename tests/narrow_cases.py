@@ -58,6 +58,18 @@ def capsule(half_height, radius):
     return (abi.SHAPE_CAPSULE, (half_height, radius, 0, 0), 0)
 
 
+def ellipsoid(a, b, c):
+    return (abi.SHAPE_ELLIPSOID, (a, b, c, 0), 0)
+
+
+def cylinder(half_height, radius):
+    return (abi.SHAPE_CYLINDER, (half_height, radius, 0, 0), 0)
+
+
+def cone(half_height, radius):
+    return (abi.SHAPE_CONE, (half_height, radius, 0, 0), 0)
+
+
 def plane(nx, ny, nz, d):
     return (abi.SHAPE_PLANE, (nx, ny, nz, d), 0)
 
@@ -233,6 +245,9 @@ def random_quats(rng, n):
 
 
 ANALYTIC_KINDS = ("sphere", "box", "capsule")
+# convex shapes without analytic pair routines (GJK / EPA, one EPA point),
+# with their own plane routines (PlaneCollision.hpp:40-61, 416-536)
+ROUND_KINDS = ("ellipsoid", "cylinder", "cone")
 HULL_NAMES = ("tet", "cube", "ellA", "ellB")
 # hull scale: the fixture tet / cube span [-1, 1]; the ellipsoids ~0.5
 
@@ -244,6 +259,12 @@ def random_shape(rng, kind):
         return box(*rng.uniform(0.2, 0.6, 3))
     if kind == "capsule":
         return capsule(rng.uniform(0.1, 0.5), rng.uniform(0.1, 0.3))
+    if kind == "ellipsoid":
+        return ellipsoid(*rng.uniform(0.2, 0.6, 3))
+    if kind == "cylinder":
+        return cylinder(rng.uniform(0.1, 0.5), rng.uniform(0.15, 0.5))
+    if kind == "cone":
+        return cone(rng.uniform(0.15, 0.5), rng.uniform(0.15, 0.5))
     raise ValueError(kind)
 
 

@@ -123,7 +123,15 @@ PAIRINGS += [(a, "plane") for a in NC.ANALYTIC_KINDS] + [("hull", "plane")]
 PAIRINGS += [("hull", k) for k in NC.ANALYTIC_KINDS] + [(k, "hull") for k in NC.ANALYTIC_KINDS] + [("hull", "hull")]
 
 
-@pytest.mark.parametrize("pairing", PAIRINGS, ids=[f"{a}-{b}" for a, b in PAIRINGS])
+# ellipsoid / cylinder / cone: their plane routines, and GJK / EPA (one EPA
+# point, ContactManifoldGenerator.cpp:405-412) against every convex shape
+ROUND_PAIRINGS = [(k, "plane") for k in NC.ROUND_KINDS]
+ROUND_PAIRINGS += [(k, m) for k in NC.ROUND_KINDS for m in NC.ANALYTIC_KINDS + NC.ROUND_KINDS + ("hull",)]
+ROUND_PAIRINGS += [(m, k) for k in NC.ROUND_KINDS for m in NC.ANALYTIC_KINDS + ("hull",)]
+
+
+@pytest.mark.parametrize("pairing", PAIRINGS + ROUND_PAIRINGS,
+                         ids=[f"{a}-{b}" for a, b in PAIRINGS + ROUND_PAIRINGS])
 def test_random_poses_fp64_bit_exact(engines, pairing):
     ka, kb = pairing
     sa, ta, sb, tb = NC.random_pairs(zlib.crc32(f"{ka}-{kb}".encode()), ka, kb, 2000)
