@@ -76,6 +76,7 @@ enum {
     RBPS_SHAPE_CYLINDER = 4,    /* params = half_height, base_radius; axis local +Y  */
     RBPS_SHAPE_CONE = 5,        /* params = half_height, base_radius; apex at +Y     */
     RBPS_SHAPE_PLANE = 6,
+    RBPS_SHAPE_HEIGHTMAP = 7,   /* collider `hull` = heightmap id (rbps_heightmap_create) */
     RBPS_SHAPE_CONVEX_HULL = 9
 };
 
@@ -237,6 +238,14 @@ RBPS_API int rbps_batch_destroy(rbps_batch *batch);
  * (ConvexHull.hpp:126-420); the data is copied.  verts = 3*n_verts doubles. */
 RBPS_API int rbps_hull_create(rbps_batch *batch, const double *verts, uint32_t n_verts,
                               const uint32_t *tris, uint32_t n_tris, uint32_t *hull_id);
+/* Replaces heightmap_data_create (Heightmap.hpp): rows x cols float height
+ * samples (row-major; sample (r, c) sits at origin + (c * scale.x,
+ * h * scale.y, r * scale.z) in world space), copied at call time.  Colliders
+ * with shape RBPS_SHAPE_HEIGHTMAP name the returned id in their `hull` field;
+ * spheres, capsules and boxes collide with it (HeightmapCollision.hpp), other
+ * shapes do not, as in the reference.  Before rbps_batch_commit. */
+RBPS_API int rbps_heightmap_create(rbps_batch *batch, const float *heights, uint32_t rows, uint32_t cols,
+                                   const double *scale, const double *origin, uint32_t *heightmap_id);
 /* Quickhull helper (the reference ships no hull builder, ConvexHull.hpp:29-33):
  * CCW outward triangles of the convex hull of n points.  Writes at most
  * tri_cap triangles; *n_tris receives the count. */

@@ -35,6 +35,8 @@ def lib():
         L.ref_world_destroy.argtypes = [_P]
         L.ref_hull_create.restype = C.c_uint32
         L.ref_hull_create.argtypes = [_P, _D, C.c_uint32, _U, C.c_uint32]
+        L.ref_heightmap_create.restype = C.c_uint32
+        L.ref_heightmap_create.argtypes = [_P, C.POINTER(C.c_float), C.c_uint32, C.c_uint32, _D, _D]
         L.ref_add_body.restype = C.c_uint32
         L.ref_add_body.argtypes = [_P, _P]
         L.ref_set_body_force.argtypes = [_P, C.c_uint32, _D, _D]
@@ -92,6 +94,12 @@ class RefWorld:
             v = np.ascontiguousarray(verts, np.float64)
             t = np.ascontiguousarray(tris, np.uint32)
             L.ref_hull_create(self.h, _dp(v), len(v), t.ctypes.data_as(_U), len(t))
+        for heights, scale, origin in getattr(spec, "heightmaps", []):
+            hh = np.ascontiguousarray(heights, np.float32)
+            sc = np.ascontiguousarray(scale, np.float64)
+            og = np.ascontiguousarray(origin, np.float64)
+            L.ref_heightmap_create(self.h, hh.ctypes.data_as(C.POINTER(C.c_float)), hh.shape[0], hh.shape[1],
+                                   _dp(sc), _dp(og))
         bodies = np.ascontiguousarray(spec.bodies)
         for i in range(len(bodies)):
             L.ref_add_body(self.h, C.c_void_p(bodies.ctypes.data + i * bodies.itemsize))

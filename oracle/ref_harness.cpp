@@ -50,10 +50,18 @@ namespace
         uint32_t row_attach, row_cone; // constraint ids
     };
 
+    struct HeightmapStore
+    {
+        std::vector<float> heights;
+        rbc::HeightmapData *data = nullptr;
+        ~HeightmapStore() { rbc::heightmap_data_destroy(data); }
+    };
+
     struct RefWorld
     {
         rbps::World w;
         std::vector<std::unique_ptr<HullStore>> hulls;
+        std::vector<std::unique_ptr<HeightmapStore>> heightmaps;
         std::vector<SphJoint> sph;
         RefWorld(double dt, int substeps) : w(dt, substeps) {}
     };
@@ -177,6 +185,11 @@ namespace
         case RBPS_SHAPE_CYLINDER: out = rbc::Cylinder(d->params[0], d->params[1]); return true;
         case RBPS_SHAPE_CONE: out = rbc::Cone(d->params[0], d->params[1]); return true;
         case RBPS_SHAPE_PLANE: out = rbc::Plane(v3(d->params), d->params[3]); return true;
+        case RBPS_SHAPE_HEIGHTMAP:
+            if (d->hull >= rw->heightmaps.size())
+                return false;
+            out = rbc::Heightmap(rw->heightmaps[d->hull]->data);
+            return true;
         case RBPS_SHAPE_CONVEX_HULL:
             if (d->hull >= rw->hulls.size())
                 return false;
@@ -214,6 +227,17 @@ extern "C"
                                                 hs->tris.data(), n_tris);
         rw->hulls.push_back(std::move(hs));
         return static_cast<uint32_t>(rw->hulls.size() - 1);
+    }
+
+    uint32_t ref_heightmap_create(void *h, const float *heights, uint32_t rows, uint32_t cols, const double *scale,
+                                  const double *origin)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        auto hs = std::make_unique<HeightmapStore>();
+        hs->heights.assign(heights, heights + (size_t)rows * cols);
+        hs->data = rbc::heightmap_data_create(hs->heights.data(), rows, cols, v3(scale), v3(origin));
+        rw->heightmaps.push_back(std::move(hs));
+        return static_cast<uint32_t>(rw->heightmaps.size() - 1);
     }
 
     uint32_t ref_add_body(void *h, const rbps_body_desc *d)

@@ -69,6 +69,7 @@ def lib():
             "rbps_batch_create": (i, [C.POINTER(BatchDesc), C.POINTER(_P)]),
             "rbps_batch_destroy": (i, [_P]),
             "rbps_hull_create": (i, [_P, _D, C.c_uint32, _U, C.c_uint32, _U]),
+            "rbps_heightmap_create": (i, [_P, C.POINTER(C.c_float), C.c_uint32, C.c_uint32, _D, _D, _U]),
             "rbps_quickhull": (i, [_D, C.c_uint32, _U, C.c_uint32, _U]),
             "rbps_hull_tables": (i, [_D, C.c_uint32, _U, C.c_uint32, C.c_uint32, _U, _U, _U, _D, _U, _U, _U, _U, _U,
                                      _U]),
@@ -219,10 +220,22 @@ class Batch:
         forces = np.ascontiguousarray(spec.forces, np.float64)
         if len(bodies):
             _check(L.rbps_world_set_body_forces(self.h, w, first.value, len(bodies), _dp(forces)))
+        hm_base = []
+        for heights, scale, origin in getattr(spec, "heightmaps", []):
+            hh = np.ascontiguousarray(heights, np.float32)
+            sc = np.ascontiguousarray(scale, np.float64)
+            og = np.ascontiguousarray(origin, np.float64)
+            hid = C.c_uint32(0)
+            _check(L.rbps_heightmap_create(self.h, hh.ctypes.data_as(C.POINTER(C.c_float)), hh.shape[0], hh.shape[1],
+                                           _dp(sc), _dp(og), C.byref(hid)))
+            hm_base.append(hid.value)
         cols = np.ascontiguousarray(spec.colliders).copy()
         if hull_base:
             m = cols["shape"] == abi.SHAPE_CONVEX_HULL
             cols["hull"][m] = np.asarray(hull_base, np.uint32)[cols["hull"][m]]
+        if hm_base:
+            m = cols["shape"] == abi.SHAPE_HEIGHTMAP
+            cols["hull"][m] = np.asarray(hm_base, np.uint32)[cols["hull"][m]]
         if len(cols):
             _check(L.rbps_world_add_colliders(self.h, w, len(cols), C.c_void_p(cols.ctypes.data), None))
         joints = np.ascontiguousarray(spec.joints)

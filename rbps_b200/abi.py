@@ -37,6 +37,7 @@ SHAPE_CAPSULE = 3
 SHAPE_CYLINDER = 4
 SHAPE_CONE = 5
 SHAPE_PLANE = 6
+SHAPE_HEIGHTMAP = 7
 SHAPE_CONVEX_HULL = 9
 
 JOINT_PRISMATIC = 0

@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -299,14 +300,25 @@ namespace
 static bool shape_supported(int s)
 {
     return s == RBPS_SHAPE_SPHERE || s == RBPS_SHAPE_BOX || s == RBPS_SHAPE_ELLIPSOID || s == RBPS_SHAPE_CAPSULE ||
-           s == RBPS_SHAPE_CYLINDER || s == RBPS_SHAPE_CONE || s == RBPS_SHAPE_PLANE || s == RBPS_SHAPE_CONVEX_HULL;
+           s == RBPS_SHAPE_CYLINDER || s == RBPS_SHAPE_CONE || s == RBPS_SHAPE_PLANE || s == RBPS_SHAPE_HEIGHTMAP ||
+           s == RBPS_SHAPE_CONVEX_HULL;
 }
+
+// A heightmap as heightmap_data_create builds it (Heightmap.hpp).
+struct HostHeightmap
+{
+    std::vector<float> heights;
+    HmDesc d{};
+};
 
 struct rbps_batch
 {
     rbps_batch_desc desc;
     std::vector<HostWorld> worlds;
     std::vector<HostHull> hulls;
+    std::vector<HostHeightmap> heightmaps;
+    float *hm_heights = nullptr;
+    HmDesc *hm_desc = nullptr;
     bool committed = false;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -609,6 +621,39 @@ extern "C" int rbps_hull_create(rbps_batch *b, const double *verts, uint32_t n_v
     return RBPS_OK;
 }
 
+extern "C" int rbps_heightmap_create(rbps_batch *b, const float *heights, uint32_t rows, uint32_t cols,
+                                     const double *scale, const double *origin, uint32_t *id)
+{
+    if (!b || !heights || !scale || !origin || rows < 2 || cols < 2)
+        return fail(RBPS_ERR_INVALID, "rbps_heightmap_create: need heights, scale, origin and a 2 x 2 grid at least");
+    if (b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_heightmap_create: batch already committed");
+    HostHeightmap h;
+    const size_t n = (size_t)rows * cols;
+    h.heights.assign(heights, heights + n);
+    h.d.rows = rows;
+    h.d.cols = cols;
+    for (int k = 0; k < 3; ++k)
+    {
+        h.d.scale[k] = scale[k];
+        h.d.origin[k] = origin[k];
+    }
+    // heightmap_data_create: min / max over the samples in float, then
+    // scaled into world heights in double
+    float mn = std::numeric_limits<float>::max(), mx = std::numeric_limits<float>::lowest();
+    for (size_t i = 0; i < n; ++i)
+    {
+        mn = std::min(mn, heights[i]);
+        mx = std::max(mx, heights[i]);
+    }
+    h.d.min_h = (double)mn * scale[1] + origin[1];
+    h.d.max_h = (double)mx * scale[1] + origin[1];
+    b->heightmaps.push_back(std::move(h));
+    if (id)
+        *id = (uint32_t)(b->heightmaps.size() - 1);
+    return RBPS_OK;
+}
+
 extern "C" int rbps_world_add_bodies(rbps_batch *b, uint32_t world, uint32_t n, const rbps_body_desc *d,
                                      uint32_t *first_id)
 {
@@ -674,6 +719,8 @@ extern "C" int rbps_world_add_colliders(rbps_batch *b, uint32_t world, uint32_t 
             return fail(RBPS_ERR_INVALID, "collider body %u does not exist", c.body_id);
         if (!shape_supported(c.shape))
             return fail(RBPS_ERR_INVALID, "unsupported shape kind %d", c.shape);
+        if (c.shape == RBPS_SHAPE_HEIGHTMAP && c.hull >= b->heightmaps.size())
+            return fail(RBPS_ERR_INVALID, "collider %u: unknown heightmap %u", i, c.hull);
         if (c.shape == RBPS_SHAPE_CONVEX_HULL && c.hull >= b->hulls.size())
             return fail(RBPS_ERR_INVALID, "hull %u does not exist", c.hull);
         w.colliders.push_back(c);
@@ -733,6 +780,8 @@ namespace
         e.hulls.desc = b->hull_desc;
         e.hulls.u32 = b->hull_u32;
         e.hulls.poly_n = b->hull_pn;
+        e.hulls.hm_heights = b->hm_heights;
+        e.hulls.hm_desc = b->hm_desc;
         e.bp_coll = b->bp_coll;
         e.fat = b->fat;
         e.ep_key = b->ep_key;
@@ -1044,6 +1093,20 @@ static int commit_typed(rbps_batch *b)
             (rc = b->upload(&b->hull_u32, u32)) || (rc = b->upload(&b->hull_pn, pn)))
             return rc;
     }
+    // ---- heightmaps
+    {
+        std::vector<float> hh;
+        std::vector<HmDesc> hd;
+        for (const auto &h : b->heightmaps)
+        {
+            HmDesc d = h.d;
+            d.off = (uint32_t)hh.size();
+            hh.insert(hh.end(), h.heights.begin(), h.heights.end());
+            hd.push_back(d);
+        }
+        if ((rc = b->upload(&b->hm_heights, hh)) || (rc = b->upload(&b->hm_desc, hd)))
+            return rc;
+    }
     HullSetDev hs_host{nullptr, nullptr, nullptr};
 
     // ---- colliders + initial SAP state (broad_phase_insert, BroadPhase.cpp:169-197)
@@ -1095,6 +1158,8 @@ static int commit_typed(rbps_batch *b)
                 la.assign(b->hulls[cd.hull].aabb, b->hulls[cd.hull].aabb + 6);
                 hs.local_aabb = la.data();
             }
+            if (cd.shape == RBPS_SHAPE_HEIGHTMAP)
+                hs.hm_desc = &b->heightmaps[cd.hull].d;
             ShapeDev s = shp[d.coll_off + c];
             s.hull = 0;
             const aabb tight = compute_aabb(s, t, hs);
@@ -2050,7 +2115,8 @@ template <class T, class P>
 static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> &sa, const double *tf_a,
                          const std::vector<ShapeDev> &sb, const double *tf_b, rbps_manifold *out)
 {
-    HullSetDev hs{b->hull_verts, b->hull_voff, b->hull_aabb, b->hull_desc, b->hull_u32, b->hull_pn};
+    HullSetDev hs{b->hull_verts, b->hull_voff, b->hull_aabb, b->hull_desc, b->hull_u32, b->hull_pn, b->hm_heights,
+                  b->hm_desc};
     const size_t shape_bytes = (size_t)n * sizeof(ShapeDev), tf_bytes = (size_t)n * 7 * sizeof(double);
     bool gjk = false;
     for (uint32_t i = 0; i < n && !gjk; ++i)
@@ -2101,6 +2167,12 @@ extern "C" int rbps_batch_collide(rbps_batch *b, uint32_t n, const rbps_collider
             const rbps_collider_desc &c = side ? bd[i] : a[i];
             if (!shape_supported(c.shape))
                 return fail(RBPS_ERR_INVALID, "rbps_batch_collide: pair %u has an unknown shape %d", i, c.shape);
+            if (c.shape == RBPS_SHAPE_HEIGHTMAP)
+            {
+                if (c.hull >= b->heightmaps.size())
+                    return fail(RBPS_ERR_INVALID, "rbps_batch_collide: heightmap %u does not exist", c.hull);
+                uses_hull = true;
+            }
             if (c.shape == RBPS_SHAPE_CONVEX_HULL)
             {
                 if (c.hull >= b->hulls.size())

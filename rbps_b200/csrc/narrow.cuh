@@ -27,6 +27,7 @@ namespace rbps_gpu
         kCylinder = 4,
         kCone = 5,
         kPlane = 6,
+        kHeightmap = 7,
         kHull = 9
     };
 
@@ -89,6 +90,16 @@ namespace rbps_gpu
         uint32_t p2p_o, p2p_i;   // polygon -> polygons (offsets: np + 1)
     };
 
+    // One heightmap (HeightmapData, Heightmap.hpp): rows x cols float
+    // samples at heights[off ..], grid spacing / height scale, the (0, 0)
+    // vertex, and the precomputed world height range.
+    struct HmDesc
+    {
+        uint32_t rows, cols, off, pad_;
+        double scale[3], origin[3];
+        double min_h, max_h;
+    };
+
     struct HullSetDev
     {
         const double *verts;      // 3 per vertex
@@ -97,6 +108,8 @@ namespace rbps_gpu
         const HullDesc *desc;     // per hull
         const uint32_t *u32;      // all index tables
         const double *poly_n;     // 3 per polygon
+        const float *hm_heights;  // heightmap samples (ShapeDev::hull = heightmap id)
+        const HmDesc *hm_desc;    // per heightmap
     };
 
     struct ShapeDev
@@ -179,6 +192,13 @@ namespace rbps_gpu
                 mx = vec3<double>(rmax(mx.x, ws.x), rmax(mx.y, ws.y), rmax(mx.z, ws.z));
             }
             return {mn, mx};
+        }
+        if (s.kind == kHeightmap) // Heightmap.hpp compute_aabb (world frame, tf unused)
+        {
+            const HmDesc &h = hs.hm_desc[s.hull];
+            return {vec3<double>(h.origin[0], h.min_h, h.origin[2]),
+                    vec3<double>(h.origin[0] + double(h.cols - 1) * h.scale[0], h.max_h,
+                                 h.origin[2] + double(h.rows - 1) * h.scale[2])};
         }
         // Plane (Plane.hpp:46-50): infinite; planes never enter the SAP.
         const double inf = HUGE_VAL;
@@ -1107,6 +1127,258 @@ namespace rbps_gpu
     };
 
     // dispatch (Dispatcher.hpp:212-217) over the analytic table.
+    // ------------------------------------------------------- Heightmaps
+    // Triangle helpers (TriangleUtils.hpp) and the sphere / capsule / box vs
+    // heightmap tests (HeightmapCollision.hpp): every cell under the shape's
+    // AABB, two triangles per cell, the deepest single contact kept.
+    template <class T>
+    __device__ vec3<T> tri_closest(const vec3<T> &P, const vec3<T> &A, const vec3<T> &B, const vec3<T> &C)
+    {
+        const vec3<T> AB = B - A, AC = C - A, AP = P - A;
+        const T d1 = dot(AB, AP), d2 = dot(AC, AP);
+        if (d1 <= T(0.0) && d2 <= T(0.0))
+            return A;
+        const vec3<T> BP = P - B;
+        const T d3 = dot(AB, BP), d4 = dot(AC, BP);
+        if (d3 >= T(0.0) && d4 <= d3)
+            return B;
+        const T vc = d1 * d4 - d3 * d2;
+        if (vc <= T(0.0) && d1 >= T(0.0) && d3 <= T(0.0))
+            return A + AB * (d1 / (d1 - d3));
+        const vec3<T> CP = P - C;
+        const T d5 = dot(AB, CP), d6 = dot(AC, CP);
+        if (d6 >= T(0.0) && d5 <= d6)
+            return C;
+        const T vb = d5 * d2 - d1 * d6;
+        if (vb <= T(0.0) && d2 >= T(0.0) && d6 <= T(0.0))
+            return A + AC * (d2 / (d2 - d6));
+        const T va = d3 * d6 - d5 * d4;
+        if (va <= T(0.0) && (d4 - d3) >= T(0.0) && (d5 - d6) >= T(0.0))
+        {
+            const T w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+            return B + (C - B) * w;
+        }
+        const T denom = T(1.0) / (va + vb + vc);
+        const T v = vb * denom, w = vc * denom;
+        return A + AB * v + AC * w;
+    }
+
+    template <class T>
+    __device__ T tri_seg_seg_sq(const vec3<T> &p1, const vec3<T> &p2, const vec3<T> &q1, const vec3<T> &q2)
+    {
+        const vec3<T> d1 = p2 - p1, d2 = q2 - q1, r = p1 - q1;
+        const T a = length_sq(d1), e = length_sq(d2), f = dot(d2, r);
+        T s, t;
+        if (a < T(kEpsilon) && e < T(kEpsilon))
+            s = t = T(0.0);
+        else if (a < T(kEpsilon))
+        {
+            s = T(0.0);
+            t = rclamp(f / e, T(0), T(1));
+        }
+        else
+        {
+            const T c = dot(d1, r);
+            if (e < T(kEpsilon))
+            {
+                t = T(0.0);
+                s = rclamp(-c / a, T(0), T(1));
+            }
+            else
+            {
+                const T b = dot(d1, d2);
+                const T denom = a * e - b * b;
+                s = denom > T(kEpsilon) ? rclamp((b * f - c * e) / denom, T(0), T(1)) : T(0.0);
+                t = (b * s + f) / e;
+                if (t < T(0.0))
+                {
+                    t = T(0.0);
+                    s = rclamp(-c / a, T(0), T(1));
+                }
+                else if (t > T(1.0))
+                {
+                    t = T(1.0);
+                    s = rclamp((b - c) / a, T(0), T(1));
+                }
+            }
+        }
+        return length_sq((p1 + d1 * s) - (q1 + d2 * t));
+    }
+
+    template <class T>
+    __device__ T tri_seg_sq(const vec3<T> &P, const vec3<T> &Q, const vec3<T> &A, const vec3<T> &B, const vec3<T> &C)
+    {
+        T best = length_sq(P - tri_closest(P, A, B, C));
+        best = rmin(best, length_sq(Q - tri_closest(Q, A, B, C)));
+        best = rmin(best, tri_seg_seg_sq(P, Q, A, B));
+        best = rmin(best, tri_seg_seg_sq(P, Q, B, C));
+        best = rmin(best, tri_seg_seg_sq(P, Q, C, A));
+        return best;
+    }
+
+    // kind: 0 sphere (p0 = centre, r), 1 capsule (segment p0-p1, r), 2 box
+    // (tb, half-extents h); one triangle, one point, normal from the
+    // triangle toward the shape.
+    template <class T>
+    __device__ bool tri_contact(int kind, const vec3<T> &p0, const vec3<T> &p1, T r, const tf<T> &tb, const vec3<T> &h,
+                                const vec3<T> &A, const vec3<T> &B, const vec3<T> &C, const vec3<T> &n,
+                                Manifold<T> &m)
+    {
+        if (kind == 0) // tri::sphere_vs_triangle
+        {
+            const vec3<T> closest = tri_closest(p0, A, B, C);
+            const vec3<T> delta = p0 - closest;
+            const T dist2 = length_sq(delta);
+            if (dist2 > r * r)
+                return false;
+            const T dist = sqrt_t(dist2);
+            if (dist > T(kEpsilon))
+            {
+                const T inv = T(1.0) / dist;
+                m.normal = vec3<T>(delta.x * inv, delta.y * inv, delta.z * inv);
+                m.depth[0] = r - dist;
+                m.pos[0] = closest;
+            }
+            else
+            {
+                const T side = dot(n, p0 - A);
+                m.normal = (side >= T(0.0)) ? n : -n;
+                m.depth[0] = r + rabs(side);
+                m.pos[0] = p0 - m.normal * r;
+            }
+            m.n = 1;
+            return true;
+        }
+        if (kind == 1) // tri::capsule_vs_triangle
+        {
+            const T d1 = dot(n, p0 - A), d2 = dot(n, p1 - A);
+            if (d1 > r && d2 > r)
+                return false;
+            if (d1 < -r && d2 < -r)
+                return false;
+            const T sq = tri_seg_sq(p0, p1, A, B, C);
+            if (sq > r * r)
+                return false;
+            const T dist = sqrt_t(sq);
+            const vec3<T> cp1 = tri_closest(p0, A, B, C), cp2 = tri_closest(p1, A, B, C);
+            const T d1sq = length_sq(p0 - cp1), d2sq = length_sq(p1 - cp2);
+            const vec3<T> &rs = (d1sq <= d2sq) ? p0 : p1;
+            const vec3<T> &rt = (d1sq <= d2sq) ? cp1 : cp2;
+            const vec3<T> delta = rs - rt;
+            if (dist > T(kEpsilon))
+            {
+                const T inv = T(1.0) / dist;
+                m.normal = vec3<T>(delta.x * inv, delta.y * inv, delta.z * inv);
+                m.depth[0] = r - dist;
+            }
+            else
+            {
+                m.normal = n;
+                m.depth[0] = r;
+            }
+            m.pos[0] = rt;
+            m.n = 1;
+            return true;
+        }
+        // box vs one heightmap triangle (HeightmapCollision.hpp, Box)
+        const T centre_dist = dot(tb.pos - A, n);
+        const vec3<T> ln = tb.inverse_rotate_vector(n);
+        const T box_r = rabs(ln.x) * h.x + rabs(ln.y) * h.y + rabs(ln.z) * h.z;
+        if (centre_dist > box_r)
+            return false;
+        const vec3<T> proj = tb.pos - n * centre_dist;
+        const vec3<T> closest = tri_closest(proj, A, B, C);
+        if (length(proj - closest) > box_r)
+            return false;
+        const T depth = box_r - centre_dist;
+        if (depth <= T(0.0))
+            return false;
+        m.normal = n;
+        m.n = 1;
+        m.pos[0] = closest;
+        m.depth[0] = depth;
+        return true;
+    }
+
+    // heightmap_test (HeightmapCollision.hpp): shape `kind` (see
+    // tri_contact) with world AABB [qmn, qmx] against heightmap `id`.
+    template <class T>
+    __device__ bool heightmap_contact(const HullSetDev &hs, uint32_t id, int kind, const vec3<T> &p0,
+                                      const vec3<T> &p1, T r, const tf<T> &tb, const vec3<T> &h,
+                                      const vec3<T> &qmn, const vec3<T> &qmx, Manifold<T> &out)
+    {
+        const HmDesc &hd = hs.hm_desc[id];
+        const float *H = hs.hm_heights + hd.off;
+        const T ox = T(hd.origin[0]), oy = T(hd.origin[1]), oz = T(hd.origin[2]);
+        const T sx = T(hd.scale[0]), sy = T(hd.scale[1]), sz = T(hd.scale[2]);
+        const int r0 = max(0, int((qmn.z - oz) / sz));
+        const int r1 = min(int(hd.rows) - 2, int((qmx.z - oz) / sz));
+        const int c0 = max(0, int((qmn.x - ox) / sx));
+        const int c1 = min(int(hd.cols) - 2, int((qmx.x - ox) / sx));
+        auto vtx = [&](int row, int col) {
+            return vec3<T>(ox + T(col) * sx, T(H[(uint32_t)row * hd.cols + (uint32_t)col]) * sy + oy, oz + T(row) * sz);
+        };
+        bool hit = false;
+        T best = T(0.0);
+        for (int rr = r0; rr <= r1; ++rr)
+            for (int cc = c0; cc <= c1; ++cc)
+            {
+                const vec3<T> V00 = vtx(rr, cc), V10 = vtx(rr + 1, cc), V01 = vtx(rr, cc + 1), V11 = vtx(rr + 1, cc + 1);
+                for (int k = 0; k < 2; ++k)
+                {
+                    const vec3<T> A = k ? V10 : V00, B = k ? V11 : V10, C = V01;
+                    const vec3<T> n = normalize(cross(B - A, C - A));
+                    Manifold<T> cand;
+                    cand.n = 0;
+                    if (tri_contact(kind, p0, p1, r, tb, h, A, B, C, n, cand) && cand.depth[0] > best)
+                    {
+                        best = cand.depth[0];
+                        out = cand;
+                        hit = true;
+                    }
+                }
+            }
+        return hit;
+    }
+
+    // Sphere / Capsule / Box (shape a) against heightmap hm; other shapes
+    // against a heightmap find no contact (the primary CollisionAlgorithm of
+    // a non-convex pair, Dispatcher.hpp:40-60).
+    template <class T>
+    __device__ bool shape_heightmap(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &hm, const HullSetDev &hs,
+                                    Manifold<T> &m)
+    {
+        const vec3<T> zero(T(0), T(0), T(0));
+        if (sa.kind == kSphere) // compute_aabb(Sphere)
+        {
+            const T r = T(sa.p[0]);
+            const vec3<T> rr(r, r, r);
+            return heightmap_contact(hs, uint32_t(hm.hull), 0, ta.pos, zero, r, ta, zero, ta.pos - rr, ta.pos + rr, m);
+        }
+        if (sa.kind == kCapsule) // capsule_endpoints + compute_aabb(Capsule)
+        {
+            const T hh = T(sa.p[0]), r = T(sa.p[1]);
+            vec3<T> p1, p2;
+            capsule_endpoints(hh, ta, p1, p2);
+            const vec3<T> axis = ta.rotate_vector(vec3<T>(T(0.0), hh, T(0.0)));
+            const vec3<T> a1 = ta.pos + axis, a2 = ta.pos - axis;
+            const vec3<T> rr(r, r, r);
+            const vec3<T> qmn = vec3<T>(rmin(a1.x, a2.x), rmin(a1.y, a2.y), rmin(a1.z, a2.z)) - rr;
+            const vec3<T> qmx = vec3<T>(rmax(a1.x, a2.x), rmax(a1.y, a2.y), rmax(a1.z, a2.z)) + rr;
+            return heightmap_contact(hs, uint32_t(hm.hull), 1, p1, p2, r, ta, zero, qmn, qmx, m);
+        }
+        if (sa.kind == kBox) // compute_aabb(Box)
+        {
+            const vec3<T> h(T(sa.p[0]), T(sa.p[1]), T(sa.p[2]));
+            const mat3<T> R = mat3_cast(ta.rot);
+            const vec3<T> e(rabs(R.c[0].x) * h.x + rabs(R.c[1].x) * h.y + rabs(R.c[2].x) * h.z,
+                            rabs(R.c[0].y) * h.x + rabs(R.c[1].y) * h.y + rabs(R.c[2].y) * h.z,
+                            rabs(R.c[0].z) * h.x + rabs(R.c[1].z) * h.y + rabs(R.c[2].z) * h.z);
+            return heightmap_contact(hs, uint32_t(hm.hull), 2, zero, zero, T(0), ta, h, ta.pos - e, ta.pos + e, m);
+        }
+        return false;
+    }
+
     // Sel selects the routines compiled in: kSelAll every pair; kSelNoBoxBox
     // all but box-box; kSelBoxBox box-box only (the caller guarantees the
     // kinds), so a kernel that never meets a box pair carries no box-box
@@ -1157,6 +1429,18 @@ namespace rbps_gpu
                 hit = round_plane(sb, tb, sa, ta, m);
             if (hit)
                 m.normal = -m.normal;
+            return hit ? kHit : kMiss;
+        }
+        if (ka == kHeightmap || kb == kHeightmap)
+        {
+            if (kb == kHeightmap)
+                hit = shape_heightmap(sa, ta, sb, hs, m);
+            else
+            {
+                hit = shape_heightmap(sb, tb, sa, hs, m); // CollisionAlgorithmSym
+                if (hit)
+                    m.normal = -m.normal;
+            }
             return hit ? kHit : kMiss;
         }
         if (gjk_kind(ka) || gjk_kind(kb))

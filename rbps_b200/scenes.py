@@ -29,6 +29,9 @@ class WorldSpec:
     colliders: np.ndarray              # abi.COLLIDER_DT
     joints: np.ndarray                 # abi.JOINT_DT
     hulls: List[Tuple[np.ndarray, np.ndarray]] = field(default_factory=list)
+    # (heights (rows, cols) float32, scale (3,), origin (3,)); a heightmap
+    # collider's `hull` field indexes this list
+    heightmaps: List[Tuple[np.ndarray, np.ndarray, np.ndarray]] = field(default_factory=list)
 
     @property
     def n_bodies(self):
@@ -565,6 +568,67 @@ def round_world(seed=0, n=24, friction=0.5, restitution=0.0):
         forces.append(f)
         colliders.append(c)
     return _finish(bodies, forces, colliders, [])
+
+
+def terrain_heights(rng, rows=33, cols=33, amp=0.6):
+    """Smooth random terrain: a sum of a few random bumps (float32)."""
+    r, c = np.meshgrid(np.arange(rows), np.arange(cols), indexing="ij")
+    h = np.zeros((rows, cols))
+    for _ in range(6):
+        cr, cc = rng.uniform(0, rows), rng.uniform(0, cols)
+        w = rng.uniform(3.0, 8.0)
+        h += rng.uniform(-1.0, 1.0) * np.exp(-((r - cr) ** 2 + (c - cc) ** 2) / (2.0 * w * w))
+    return (amp * h).astype(np.float32)
+
+
+def terrain_world(seed=0, n=32, rows=33, cols=33, cell=0.5, friction=0.5, restitution=0.0):
+    """A static heightmap terrain (rows x cols samples, `cell` m apart,
+    centred on the origin) with spheres, boxes and capsules dropped onto it
+    (HeightmapCollision.hpp's sphere / capsule / box routines)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    heights = terrain_heights(rng, rows, cols)
+    origin = np.array([-0.5 * (cols - 1) * cell, 0.0, -0.5 * (rows - 1) * cell])
+    scale = np.array([cell, 1.0, cell])
+    bodies, forces, colliders = [], [], []
+    g = abi.body_default()
+    g["type"] = abi.BODY_STATIC
+    g["mass"] = 0.0
+    bodies.append(g)
+    forces.append((0.0, 0.0, 0.0))
+    c = abi.collider_default()
+    c["shape"] = abi.SHAPE_HEIGHTMAP
+    c["hull"] = 0
+    c["body_id"] = 0
+    c["is_static"] = 1
+    c["restitution"] = restitution
+    c["static_friction"] = friction
+    c["dynamic_friction"] = friction
+    colliders.append(c)
+    kind = rng.integers(0, 3, n)
+    quats = random_quats(rng, n)
+    half = 0.4 * (cols - 1) * cell
+    pos = rng.uniform((-half, 1.2, -half), (half, 3.5, half), (n, 3))
+    for i in range(n):
+        bid = len(bodies)
+        if kind[i] == 0:
+            r = rng.uniform(0.2, 0.4)
+            m, inertia = sphere_mass(r)
+            cl = _collider(abi.SHAPE_SPHERE, [r], bid, friction, restitution)
+        elif kind[i] == 1:
+            h = rng.uniform(0.2, 0.4, 3)
+            m, inertia = box_mass(h)
+            cl = _collider(abi.SHAPE_BOX, h, bid, friction, restitution)
+        else:
+            hh, r = rng.uniform(0.1, 0.4), rng.uniform(0.1, 0.25)
+            m, inertia = capsule_mass(hh, r)
+            cl = _collider(abi.SHAPE_CAPSULE, [hh, r], bid, friction, restitution)
+        b, f = _dyn_body(pos[i], quats[i], m, inertia)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(cl)
+    w = _finish(bodies, forces, colliders, [])
+    w.heightmaps = [(heights, scale, origin)]
+    return w
 
 
 def hull_world(seed=0, n=24, n_shapes=4, friction=0.5, restitution=0.0):
