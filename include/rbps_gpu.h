@@ -77,6 +77,7 @@ enum {
     RBPS_SHAPE_CONE = 5,        /* params = half_height, base_radius; apex at +Y     */
     RBPS_SHAPE_PLANE = 6,
     RBPS_SHAPE_HEIGHTMAP = 7,   /* collider `hull` = heightmap id (rbps_heightmap_create) */
+    RBPS_SHAPE_MESH = 8,        /* collider `hull` = mesh id (rbps_mesh_create)           */
     RBPS_SHAPE_CONVEX_HULL = 9
 };
 
@@ -246,6 +247,15 @@ RBPS_API int rbps_hull_create(rbps_batch *batch, const double *verts, uint32_t n
  * shapes do not, as in the reference.  Before rbps_batch_commit. */
 RBPS_API int rbps_heightmap_create(rbps_batch *batch, const float *heights, uint32_t rows, uint32_t cols,
                                    const double *scale, const double *origin, uint32_t *heightmap_id);
+/* Replaces mesh_data_create (Mesh.hpp): a triangle mesh of n_verts local
+ * vertices (3 doubles each) and n_faces triangles (3 indices each), copied
+ * at call time, face normals and local AABB precomputed as the reference
+ * does.  Colliders with shape RBPS_SHAPE_MESH name the returned id in their
+ * `hull` field; spheres, capsules, boxes, planes and meshes collide with it
+ * (MeshCollision.hpp, PlaneCollision.hpp), other shapes do not, as in the
+ * reference.  Before rbps_batch_commit. */
+RBPS_API int rbps_mesh_create(rbps_batch *batch, const double *verts, uint32_t n_verts, const uint32_t *indices,
+                              uint32_t n_faces, uint32_t *mesh_id);
 /* Quickhull helper (the reference ships no hull builder, ConvexHull.hpp:29-33):
  * CCW outward triangles of the convex hull of n points.  Writes at most
  * tri_cap triangles; *n_tris receives the count. */

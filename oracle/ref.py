@@ -35,6 +35,8 @@ def lib():
         L.ref_world_destroy.argtypes = [_P]
         L.ref_hull_create.restype = C.c_uint32
         L.ref_hull_create.argtypes = [_P, _D, C.c_uint32, _U, C.c_uint32]
+        L.ref_mesh_create.restype = C.c_uint32
+        L.ref_mesh_create.argtypes = [_P, _D, C.c_uint32, _U, C.c_uint32]
         L.ref_heightmap_create.restype = C.c_uint32
         L.ref_heightmap_create.argtypes = [_P, C.POINTER(C.c_float), C.c_uint32, C.c_uint32, _D, _D]
         L.ref_add_body.restype = C.c_uint32
@@ -94,6 +96,10 @@ class RefWorld:
             v = np.ascontiguousarray(verts, np.float64)
             t = np.ascontiguousarray(tris, np.uint32)
             L.ref_hull_create(self.h, _dp(v), len(v), t.ctypes.data_as(_U), len(t))
+        for verts, faces in getattr(spec, "meshes", []):
+            v = np.ascontiguousarray(verts, np.float64)
+            f = np.ascontiguousarray(faces, np.uint32)
+            L.ref_mesh_create(self.h, _dp(v), len(v), f.ctypes.data_as(_U), len(f))
         for heights, scale, origin in getattr(spec, "heightmaps", []):
             hh = np.ascontiguousarray(heights, np.float32)
             sc = np.ascontiguousarray(scale, np.float64)

@@ -57,9 +57,18 @@ namespace
         ~HeightmapStore() { rbc::heightmap_data_destroy(data); }
     };
 
+    struct MeshStore
+    {
+        std::vector<m3d::vec3> verts;
+        std::vector<uint32_t> idx;
+        rbc::MeshData *data = nullptr;
+        ~MeshStore() { rbc::mesh_data_destroy(data); }
+    };
+
     struct RefWorld
     {
         rbps::World w;
+        std::vector<std::unique_ptr<MeshStore>> meshes;
         std::vector<std::unique_ptr<HullStore>> hulls;
         std::vector<std::unique_ptr<HeightmapStore>> heightmaps;
         std::vector<SphJoint> sph;
@@ -185,6 +194,11 @@ namespace
         case RBPS_SHAPE_CYLINDER: out = rbc::Cylinder(d->params[0], d->params[1]); return true;
         case RBPS_SHAPE_CONE: out = rbc::Cone(d->params[0], d->params[1]); return true;
         case RBPS_SHAPE_PLANE: out = rbc::Plane(v3(d->params), d->params[3]); return true;
+        case RBPS_SHAPE_MESH:
+            if (d->hull >= rw->meshes.size())
+                return false;
+            out = rbc::Mesh(rw->meshes[d->hull]->data);
+            return true;
         case RBPS_SHAPE_HEIGHTMAP:
             if (d->hull >= rw->heightmaps.size())
                 return false;
@@ -238,6 +252,19 @@ extern "C"
         hs->data = rbc::heightmap_data_create(hs->heights.data(), rows, cols, v3(scale), v3(origin));
         rw->heightmaps.push_back(std::move(hs));
         return static_cast<uint32_t>(rw->heightmaps.size() - 1);
+    }
+
+    uint32_t ref_mesh_create(void *h, const double *verts, uint32_t n_verts, const uint32_t *idx, uint32_t n_faces)
+    {
+        auto *rw = static_cast<RefWorld *>(h);
+        auto ms = std::make_unique<MeshStore>();
+        ms->verts.resize(n_verts);
+        for (uint32_t i = 0; i < n_verts; ++i)
+            ms->verts[i] = v3(verts + 3 * i);
+        ms->idx.assign(idx, idx + 3 * (size_t)n_faces);
+        ms->data = rbc::mesh_data_create(ms->verts.data(), n_verts, ms->idx.data(), n_faces);
+        rw->meshes.push_back(std::move(ms));
+        return static_cast<uint32_t>(rw->meshes.size() - 1);
     }
 
     uint32_t ref_add_body(void *h, const rbps_body_desc *d)

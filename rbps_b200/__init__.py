@@ -70,6 +70,7 @@ def lib():
             "rbps_batch_destroy": (i, [_P]),
             "rbps_hull_create": (i, [_P, _D, C.c_uint32, _U, C.c_uint32, _U]),
             "rbps_heightmap_create": (i, [_P, C.POINTER(C.c_float), C.c_uint32, C.c_uint32, _D, _D, _U]),
+            "rbps_mesh_create": (i, [_P, _D, C.c_uint32, _U, C.c_uint32, _U]),
             "rbps_quickhull": (i, [_D, C.c_uint32, _U, C.c_uint32, _U]),
             "rbps_hull_tables": (i, [_D, C.c_uint32, _U, C.c_uint32, C.c_uint32, _U, _U, _U, _D, _U, _U, _U, _U, _U,
                                      _U]),
@@ -229,7 +230,17 @@ class Batch:
             _check(L.rbps_heightmap_create(self.h, hh.ctypes.data_as(C.POINTER(C.c_float)), hh.shape[0], hh.shape[1],
                                            _dp(sc), _dp(og), C.byref(hid)))
             hm_base.append(hid.value)
+        mesh_base = []
+        for verts, faces in getattr(spec, "meshes", []):
+            v = np.ascontiguousarray(verts, np.float64)
+            f = np.ascontiguousarray(faces, np.uint32)
+            mid = C.c_uint32(0)
+            _check(L.rbps_mesh_create(self.h, _dp(v), len(v), f.ctypes.data_as(_U), len(f), C.byref(mid)))
+            mesh_base.append(mid.value)
         cols = np.ascontiguousarray(spec.colliders).copy()
+        if mesh_base:
+            m = cols["shape"] == abi.SHAPE_MESH
+            cols["hull"][m] = np.asarray(mesh_base, np.uint32)[cols["hull"][m]]
         if hull_base:
             m = cols["shape"] == abi.SHAPE_CONVEX_HULL
             cols["hull"][m] = np.asarray(hull_base, np.uint32)[cols["hull"][m]]

@@ -38,6 +38,7 @@ SHAPE_CYLINDER = 4
 SHAPE_CONE = 5
 SHAPE_PLANE = 6
 SHAPE_HEIGHTMAP = 7
+SHAPE_MESH = 8
 SHAPE_CONVEX_HULL = 9
 
 JOINT_PRISMATIC = 0

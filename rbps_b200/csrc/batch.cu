@@ -301,8 +301,16 @@ static bool shape_supported(int s)
 {
     return s == RBPS_SHAPE_SPHERE || s == RBPS_SHAPE_BOX || s == RBPS_SHAPE_ELLIPSOID || s == RBPS_SHAPE_CAPSULE ||
            s == RBPS_SHAPE_CYLINDER || s == RBPS_SHAPE_CONE || s == RBPS_SHAPE_PLANE || s == RBPS_SHAPE_HEIGHTMAP ||
-           s == RBPS_SHAPE_CONVEX_HULL;
+           s == RBPS_SHAPE_MESH || s == RBPS_SHAPE_CONVEX_HULL;
 }
+
+// A triangle mesh as mesh_data_create builds it (Mesh.hpp).
+struct HostMesh
+{
+    std::vector<double> verts, normals;
+    std::vector<uint32_t> idx;
+    MeshDesc d{};
+};
 
 // A heightmap as heightmap_data_create builds it (Heightmap.hpp).
 struct HostHeightmap
@@ -317,6 +325,10 @@ struct rbps_batch
     std::vector<HostWorld> worlds;
     std::vector<HostHull> hulls;
     std::vector<HostHeightmap> heightmaps;
+    std::vector<HostMesh> meshes;
+    MeshDesc *mesh_desc = nullptr;
+    double *mesh_v = nullptr, *mesh_n = nullptr;
+    uint32_t *mesh_i = nullptr;
     float *hm_heights = nullptr;
     HmDesc *hm_desc = nullptr;
     bool committed = false;
@@ -654,6 +666,47 @@ extern "C" int rbps_heightmap_create(rbps_batch *b, const float *heights, uint32
     return RBPS_OK;
 }
 
+extern "C" int rbps_mesh_create(rbps_batch *b, const double *verts, uint32_t n_verts, const uint32_t *indices,
+                                uint32_t n_faces, uint32_t *id)
+{
+    if (!b || !verts || !indices || n_verts == 0 || n_faces == 0)
+        return fail(RBPS_ERR_INVALID, "rbps_mesh_create: need vertices and faces");
+    if (b->committed)
+        return fail(RBPS_ERR_INVALID, "rbps_mesh_create: batch already committed");
+    for (uint32_t t = 0; t < 3 * n_faces; ++t)
+        if (indices[t] >= n_verts)
+            return fail(RBPS_ERR_INVALID, "rbps_mesh_create: face index out of range");
+    HostMesh m;
+    m.verts.assign(verts, verts + 3 * (size_t)n_verts);
+    m.idx.assign(indices, indices + 3 * (size_t)n_faces);
+    auto v = [&](uint32_t k) { return vec3<double>(verts[3 * k], verts[3 * k + 1], verts[3 * k + 2]); };
+    for (uint32_t f = 0; f < n_faces; ++f)
+    {
+        const vec3<double> A = v(indices[3 * f]), B = v(indices[3 * f + 1]), C = v(indices[3 * f + 2]);
+        const vec3<double> n = normalize(cross(B - A, C - A));
+        m.normals.insert(m.normals.end(), {n.x, n.y, n.z});
+    }
+    double mn[3] = {(double)1e30f, (double)1e30f, (double)1e30f};
+    double mx[3] = {(double)-1e30f, (double)-1e30f, (double)-1e30f};
+    for (uint32_t k = 0; k < n_verts; ++k)
+        for (int a = 0; a < 3; ++a)
+        {
+            mn[a] = rmin(mn[a], verts[3 * k + a]);
+            mx[a] = rmax(mx[a], verts[3 * k + a]);
+        }
+    for (int a = 0; a < 3; ++a)
+    {
+        m.d.aabb[a] = mn[a];
+        m.d.aabb[3 + a] = mx[a];
+    }
+    m.d.nv = n_verts;
+    m.d.nf = n_faces;
+    b->meshes.push_back(std::move(m));
+    if (id)
+        *id = (uint32_t)(b->meshes.size() - 1);
+    return RBPS_OK;
+}
+
 extern "C" int rbps_world_add_bodies(rbps_batch *b, uint32_t world, uint32_t n, const rbps_body_desc *d,
                                      uint32_t *first_id)
 {
@@ -721,6 +774,8 @@ extern "C" int rbps_world_add_colliders(rbps_batch *b, uint32_t world, uint32_t 
             return fail(RBPS_ERR_INVALID, "unsupported shape kind %d", c.shape);
         if (c.shape == RBPS_SHAPE_HEIGHTMAP && c.hull >= b->heightmaps.size())
             return fail(RBPS_ERR_INVALID, "collider %u: unknown heightmap %u", i, c.hull);
+        if (c.shape == RBPS_SHAPE_MESH && c.hull >= b->meshes.size())
+            return fail(RBPS_ERR_INVALID, "collider %u: unknown mesh %u", i, c.hull);
         if (c.shape == RBPS_SHAPE_CONVEX_HULL && c.hull >= b->hulls.size())
             return fail(RBPS_ERR_INVALID, "hull %u does not exist", c.hull);
         w.colliders.push_back(c);
@@ -782,6 +837,10 @@ namespace
         e.hulls.poly_n = b->hull_pn;
         e.hulls.hm_heights = b->hm_heights;
         e.hulls.hm_desc = b->hm_desc;
+        e.hulls.mesh = b->mesh_desc;
+        e.hulls.mesh_v = b->mesh_v;
+        e.hulls.mesh_i = b->mesh_i;
+        e.hulls.mesh_n = b->mesh_n;
         e.bp_coll = b->bp_coll;
         e.fat = b->fat;
         e.ep_key = b->ep_key;
@@ -1107,6 +1166,25 @@ static int commit_typed(rbps_batch *b)
         if ((rc = b->upload(&b->hm_heights, hh)) || (rc = b->upload(&b->hm_desc, hd)))
             return rc;
     }
+    // ---- triangle meshes
+    {
+        std::vector<double> mv, mnrm;
+        std::vector<uint32_t> mi;
+        std::vector<MeshDesc> md;
+        for (const auto &m : b->meshes)
+        {
+            MeshDesc d = m.d;
+            d.v0 = (uint32_t)(mv.size() / 3);
+            d.f0 = (uint32_t)(mi.size() / 3);
+            mv.insert(mv.end(), m.verts.begin(), m.verts.end());
+            mi.insert(mi.end(), m.idx.begin(), m.idx.end());
+            mnrm.insert(mnrm.end(), m.normals.begin(), m.normals.end());
+            md.push_back(d);
+        }
+        if ((rc = b->upload(&b->mesh_desc, md)) || (rc = b->upload(&b->mesh_v, mv)) ||
+            (rc = b->upload(&b->mesh_i, mi)) || (rc = b->upload(&b->mesh_n, mnrm)))
+            return rc;
+    }
     HullSetDev hs_host{nullptr, nullptr, nullptr};
 
     // ---- colliders + initial SAP state (broad_phase_insert, BroadPhase.cpp:169-197)
@@ -1160,6 +1238,8 @@ static int commit_typed(rbps_batch *b)
             }
             if (cd.shape == RBPS_SHAPE_HEIGHTMAP)
                 hs.hm_desc = &b->heightmaps[cd.hull].d;
+            if (cd.shape == RBPS_SHAPE_MESH)
+                hs.mesh = &b->meshes[cd.hull].d;
             ShapeDev s = shp[d.coll_off + c];
             s.hull = 0;
             const aabb tight = compute_aabb(s, t, hs);
@@ -2116,7 +2196,7 @@ static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> 
                          const std::vector<ShapeDev> &sb, const double *tf_b, rbps_manifold *out)
 {
     HullSetDev hs{b->hull_verts, b->hull_voff, b->hull_aabb, b->hull_desc, b->hull_u32, b->hull_pn, b->hm_heights,
-                  b->hm_desc};
+                  b->hm_desc, b->mesh_desc, b->mesh_v, b->mesh_i, b->mesh_n};
     const size_t shape_bytes = (size_t)n * sizeof(ShapeDev), tf_bytes = (size_t)n * 7 * sizeof(double);
     bool gjk = false;
     for (uint32_t i = 0; i < n && !gjk; ++i)
@@ -2171,6 +2251,12 @@ extern "C" int rbps_batch_collide(rbps_batch *b, uint32_t n, const rbps_collider
             {
                 if (c.hull >= b->heightmaps.size())
                     return fail(RBPS_ERR_INVALID, "rbps_batch_collide: heightmap %u does not exist", c.hull);
+                uses_hull = true;
+            }
+            if (c.shape == RBPS_SHAPE_MESH)
+            {
+                if (c.hull >= b->meshes.size())
+                    return fail(RBPS_ERR_INVALID, "rbps_batch_collide: mesh %u does not exist", c.hull);
                 uses_hull = true;
             }
             if (c.shape == RBPS_SHAPE_CONVEX_HULL)

@@ -28,6 +28,7 @@ namespace rbps_gpu
         kCone = 5,
         kPlane = 6,
         kHeightmap = 7,
+        kMesh = 8,
         kHull = 9
     };
 
@@ -100,6 +101,14 @@ namespace rbps_gpu
         double min_h, max_h;
     };
 
+    // One triangle mesh (MeshData, Mesh.hpp): vertices [v0, v0 + nv), faces
+    // [f0, f0 + nf) of the batch arrays, its local AABB.
+    struct MeshDesc
+    {
+        uint32_t v0, nv, f0, nf;
+        double aabb[6];
+    };
+
     struct HullSetDev
     {
         const double *verts;      // 3 per vertex
@@ -110,6 +119,10 @@ namespace rbps_gpu
         const double *poly_n;     // 3 per polygon
         const float *hm_heights;  // heightmap samples (ShapeDev::hull = heightmap id)
         const HmDesc *hm_desc;    // per heightmap
+        const MeshDesc *mesh;     // per triangle mesh (ShapeDev::hull = mesh id)
+        const double *mesh_v;     // local vertices, 3 per vertex
+        const uint32_t *mesh_i;   // 3 vertex indices per face (mesh-relative)
+        const double *mesh_n;     // unit face normals, 3 per face
     };
 
     struct ShapeDev
@@ -192,6 +205,19 @@ namespace rbps_gpu
                 mx = vec3<double>(rmax(mx.x, ws.x), rmax(mx.y, ws.y), rmax(mx.z, ws.z));
             }
             return {mn, mx};
+        }
+        if (s.kind == kMesh) // Mesh.hpp compute_aabb
+        {
+            const double *la = hs.mesh[s.hull].aabb;
+            const vec3<double> lmn(la[0], la[1], la[2]), lmx(la[3], la[4], la[5]);
+            const vec3<double> centre = (lmn + lmx) * 0.5;
+            const vec3<double> half = (lmx - lmn) * 0.5;
+            const mat3<double> R = mat3_cast(t.rot);
+            const vec3<double> wc = t.pos + t.rotate_vector(centre);
+            const vec3<double> e(rabs(R.c[0].x) * half.x + rabs(R.c[1].x) * half.y + rabs(R.c[2].x) * half.z,
+                                 rabs(R.c[0].y) * half.x + rabs(R.c[1].y) * half.y + rabs(R.c[2].y) * half.z,
+                                 rabs(R.c[0].z) * half.x + rabs(R.c[1].z) * half.y + rabs(R.c[2].z) * half.z);
+            return {wc - e, wc + e};
         }
         if (s.kind == kHeightmap) // Heightmap.hpp compute_aabb (world frame, tf unused)
         {
@@ -1379,6 +1405,165 @@ namespace rbps_gpu
         return false;
     }
 
+    // ------------------------------------------------------------ Meshes
+    // mesh_world_triangle (MeshCollision.hpp): face f of mesh `id` in world
+    // space under tm, with its rotated precomputed normal.
+    template <class T>
+    __device__ __forceinline__ void mesh_triangle(const HullSetDev &hs, const MeshDesc &md, uint32_t f, const tf<T> &tm,
+                                                  vec3<T> &A, vec3<T> &B, vec3<T> &C, vec3<T> &n)
+    {
+        const uint32_t *ix = hs.mesh_i + 3 * (size_t)(md.f0 + f);
+        auto v = [&](uint32_t k) {
+            const double *p = hs.mesh_v + 3 * (size_t)(md.v0 + k);
+            return vec3<T>(T(p[0]), T(p[1]), T(p[2]));
+        };
+        A = tm.pos + tm.rotate_vector(v(ix[0]));
+        B = tm.pos + tm.rotate_vector(v(ix[1]));
+        C = tm.pos + tm.rotate_vector(v(ix[2]));
+        const double *fn = hs.mesh_n + 3 * (size_t)(md.f0 + f);
+        n = tm.rotate_vector(vec3<T>(T(fn[0]), T(fn[1]), T(fn[2])));
+    }
+
+    // mesh_test_all with the sphere / capsule / box per-triangle tests
+    // (kind 0 / 1 / 2; the box test is the mesh's own: depth = box_r -
+    // edge distance, kept when positive), deepest contact of all faces.
+    template <class T>
+    __device__ bool mesh_contact(const HullSetDev &hs, uint32_t id, const tf<T> &tm, int kind, const vec3<T> &p0,
+                                 const vec3<T> &p1, T r, const tf<T> &tb, const vec3<T> &h, Manifold<T> &out)
+    {
+        const MeshDesc &md = hs.mesh[id];
+        bool hit = false;
+        T best = T(0.0);
+        for (uint32_t f = 0; f < md.nf; ++f)
+        {
+            vec3<T> A, B, C, n;
+            mesh_triangle(hs, md, f, tm, A, B, C, n);
+            Manifold<T> cand;
+            cand.n = 0;
+            bool ok;
+            if (kind == 2)
+            {
+                const T centre_dist = dot(tb.pos - A, n);
+                const vec3<T> ln = tb.inverse_rotate_vector(n);
+                const T box_r = rabs(ln.x) * h.x + rabs(ln.y) * h.y + rabs(ln.z) * h.z;
+                ok = false;
+                if (centre_dist <= box_r)
+                {
+                    const vec3<T> proj = tb.pos - n * centre_dist;
+                    const vec3<T> closest = tri_closest(proj, A, B, C);
+                    const T edge_d = length(proj - closest);
+                    if (edge_d <= box_r)
+                    {
+                        cand.normal = n;
+                        cand.n = 1;
+                        cand.depth[0] = box_r - edge_d;
+                        cand.pos[0] = closest;
+                        ok = cand.depth[0] > T(0.0);
+                    }
+                }
+            }
+            else
+                ok = tri_contact(kind, p0, p1, r, tb, h, A, B, C, n, cand);
+            if (ok && cand.depth[0] > best)
+            {
+                best = cand.depth[0];
+                out = cand;
+                hit = true;
+            }
+        }
+        return hit;
+    }
+
+    // Mesh vs Mesh (MeshCollision.hpp): every vertex of every face of A as a
+    // sphere of radius 0 against all faces of B, the deepest kept.
+    template <class T>
+    __device__ bool mesh_mesh(const HullSetDev &hs, uint32_t ia, const tf<T> &ta, uint32_t ib, const tf<T> &tb,
+                              Manifold<T> &out)
+    {
+        const MeshDesc &ma = hs.mesh[ia];
+        bool hit = false;
+        T best = T(0.0);
+        Manifold<T> cand;
+        cand.n = 0;
+        const vec3<T> zero(T(0), T(0), T(0));
+        for (uint32_t f = 0; f < ma.nf; ++f)
+        {
+            vec3<T> A, B, C, n;
+            mesh_triangle(hs, ma, f, ta, A, B, C, n);
+            const vec3<T> verts[3] = {A, B, C};
+            for (int k = 0; k < 3; ++k)
+                if (mesh_contact(hs, ib, tb, 0, verts[k], zero, T(0.0), tb, zero, cand) && cand.depth[0] > best)
+                {
+                    best = cand.depth[0];
+                    out = cand;
+                    hit = true;
+                }
+        }
+        return hit;
+    }
+
+    // Sphere / Capsule / Box (shape a) or a mesh against mesh `mesh`; other
+    // shapes find no contact (the primary algorithm of a non-convex pair).
+    template <class T>
+    __device__ bool shape_mesh(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &mesh, const tf<T> &tm,
+                               const HullSetDev &hs, Manifold<T> &m)
+    {
+        const vec3<T> zero(T(0), T(0), T(0));
+        const uint32_t id = uint32_t(mesh.hull);
+        if (sa.kind == kSphere)
+            return mesh_contact(hs, id, tm, 0, ta.pos, zero, T(sa.p[0]), ta, zero, m);
+        if (sa.kind == kCapsule)
+        {
+            vec3<T> p1, p2;
+            capsule_endpoints(T(sa.p[0]), ta, p1, p2);
+            return mesh_contact(hs, id, tm, 1, p1, p2, T(sa.p[1]), ta, zero, m);
+        }
+        if (sa.kind == kBox)
+            return mesh_contact(hs, id, tm, 2, zero, zero, T(0), ta, vec3<T>(T(sa.p[0]), T(sa.p[1]), T(sa.p[2])), m);
+        if (sa.kind == kMesh)
+            return mesh_mesh(hs, uint32_t(sa.hull), ta, id, tm, m);
+        return false;
+    }
+
+    // convex_vs_plane for a mesh (RBC_PLANE_SPEC(Mesh)): the support vertex
+    // along -n (first of the largest dot products, Mesh.hpp support).
+    template <class T>
+    __device__ bool mesh_plane(const HullSetDev &hs, uint32_t id, const tf<T> &ts, const ShapeDev &pl, const tf<T> &tp,
+                               Manifold<T> &out)
+    {
+        vec3<T> wn;
+        T wd;
+        plane_world(pl, tp, wn, wd);
+        const vec3<T> ld = ts.inverse_rotate_vector(-wn);
+        const MeshDesc &md = hs.mesh[id];
+        vec3<T> ls(T(0), T(0), T(0));
+        if (md.nv)
+        {
+            const double *V = hs.mesh_v + 3 * (size_t)md.v0;
+            ls = vec3<T>(T(V[0]), T(V[1]), T(V[2]));
+            T bd = dot(ls, ld);
+            for (uint32_t i = 1; i < md.nv; ++i)
+            {
+                const vec3<T> p{T(V[3 * i]), T(V[3 * i + 1]), T(V[3 * i + 2])};
+                const T d = dot(p, ld);
+                if (d > bd)
+                {
+                    bd = d;
+                    ls = p;
+                }
+            }
+        }
+        const vec3<T> ws = ts.pos + ts.rotate_vector(ls);
+        const T sd = dot(ws, wn) - wd;
+        if (sd >= T(0))
+            return false;
+        out.normal = -wn;
+        out.n = 1;
+        out.depth[0] = -sd;
+        out.pos[0] = ws;
+        return true;
+    }
+
     // Sel selects the routines compiled in: kSelAll every pair; kSelNoBoxBox
     // all but box-box; kSelBoxBox box-box only (the caller guarantees the
     // kinds), so a kernel that never meets a box pair carries no box-box
@@ -1411,6 +1596,8 @@ namespace rbps_gpu
                 hit = cylinder_plane(T(sa.p[0]), T(sa.p[1]), ta, sb, tb, m);
             else if (ka == kEllipsoid || ka == kCone)
                 hit = round_plane(sa, ta, sb, tb, m);
+            else if (ka == kMesh)
+                hit = mesh_plane(hs, uint32_t(sa.hull), ta, sb, tb, m);
             return hit ? kHit : kMiss;
         }
         if (ka == kPlane)
@@ -1427,8 +1614,24 @@ namespace rbps_gpu
                 hit = cylinder_plane(T(sb.p[0]), T(sb.p[1]), tb, sa, ta, m);
             else if (kb == kEllipsoid || kb == kCone)
                 hit = round_plane(sb, tb, sa, ta, m);
+            else if (kb == kMesh)
+                hit = mesh_plane(hs, uint32_t(sb.hull), tb, sa, ta, m);
             if (hit)
                 m.normal = -m.normal;
+            return hit ? kHit : kMiss;
+        }
+        if (ka == kMesh || kb == kMesh)
+        {
+            if (ka == kHeightmap || kb == kHeightmap)
+                return kMiss; // no Mesh / Heightmap algorithm: the primary one finds nothing
+            if (kb == kMesh)
+                hit = shape_mesh(sa, ta, sb, tb, hs, m);
+            else
+            {
+                hit = shape_mesh(sb, tb, sa, ta, hs, m); // CollisionAlgorithmSym
+                if (hit)
+                    m.normal = -m.normal;
+            }
             return hit ? kHit : kMiss;
         }
         if (ka == kHeightmap || kb == kHeightmap)

@@ -32,6 +32,8 @@ class WorldSpec:
     # (heights (rows, cols) float32, scale (3,), origin (3,)); a heightmap
     # collider's `hull` field indexes this list
     heightmaps: List[Tuple[np.ndarray, np.ndarray, np.ndarray]] = field(default_factory=list)
+    # (vertices (n, 3), faces (m, 3)); a mesh collider's `hull` indexes this
+    meshes: List[Tuple[np.ndarray, np.ndarray]] = field(default_factory=list)
 
     @property
     def n_bodies(self):
@@ -628,6 +630,70 @@ def terrain_world(seed=0, n=32, rows=33, cols=33, cell=0.5, friction=0.5, restit
         colliders.append(cl)
     w = _finish(bodies, forces, colliders, [])
     w.heightmaps = [(heights, scale, origin)]
+    return w
+
+
+def grid_mesh(heights, cell, origin):
+    """An open triangle mesh over a height grid (2 triangles per cell, CCW
+    seen from +Y): vertices (rows * cols, 3) and faces (m, 3)."""
+    rows, cols = heights.shape
+    r, c = np.meshgrid(np.arange(rows), np.arange(cols), indexing="ij")
+    verts = np.stack([origin[0] + c * cell, heights.astype(np.float64), origin[2] + r * cell], -1).reshape(-1, 3)
+    faces = []
+    for i in range(rows - 1):
+        for j in range(cols - 1):
+            v00, v01, v10, v11 = i * cols + j, i * cols + j + 1, (i + 1) * cols + j, (i + 1) * cols + j + 1
+            faces.append((v00, v10, v01))
+            faces.append((v10, v11, v01))
+    return verts, np.array(faces, np.uint32)
+
+
+def mesh_world(seed=0, n=24, rows=17, cols=17, cell=0.75, friction=0.5, restitution=0.0):
+    """A static bumpy ground mesh (an open grid mesh) with spheres, boxes
+    and capsules dropped onto it (MeshCollision.hpp's routines)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    heights = terrain_heights(rng, rows, cols, amp=0.5)
+    origin = np.array([-0.5 * (cols - 1) * cell, 0.0, -0.5 * (rows - 1) * cell])
+    verts, faces = grid_mesh(heights, cell, origin)
+    bodies, forces, colliders = [], [], []
+    g = abi.body_default()
+    g["type"] = abi.BODY_STATIC
+    g["mass"] = 0.0
+    bodies.append(g)
+    forces.append((0.0, 0.0, 0.0))
+    c = abi.collider_default()
+    c["shape"] = abi.SHAPE_MESH
+    c["hull"] = 0
+    c["body_id"] = 0
+    c["is_static"] = 1
+    c["restitution"] = restitution
+    c["static_friction"] = friction
+    c["dynamic_friction"] = friction
+    colliders.append(c)
+    kind = rng.integers(0, 3, n)
+    quats = random_quats(rng, n)
+    half = 0.4 * (cols - 1) * cell
+    pos = rng.uniform((-half, 1.2, -half), (half, 3.5, half), (n, 3))
+    for i in range(n):
+        bid = len(bodies)
+        if kind[i] == 0:
+            r = rng.uniform(0.2, 0.4)
+            m, inertia = sphere_mass(r)
+            cl = _collider(abi.SHAPE_SPHERE, [r], bid, friction, restitution)
+        elif kind[i] == 1:
+            h = rng.uniform(0.2, 0.4, 3)
+            m, inertia = box_mass(h)
+            cl = _collider(abi.SHAPE_BOX, h, bid, friction, restitution)
+        else:
+            hh, r = rng.uniform(0.1, 0.4), rng.uniform(0.1, 0.25)
+            m, inertia = capsule_mass(hh, r)
+            cl = _collider(abi.SHAPE_CAPSULE, [hh, r], bid, friction, restitution)
+        b, f = _dyn_body(pos[i], quats[i], m, inertia)
+        bodies.append(b)
+        forces.append(f)
+        colliders.append(cl)
+    w = _finish(bodies, forces, colliders, [])
+    w.meshes = [(verts, faces)]
     return w
 
 
