@@ -105,3 +105,20 @@ def test_mesh_world_live_oracle(rbps, ref):
     assert saw_mesh
     st, rs = b.state(0), w.state()
     assert bit_equal(st, rs) or max(state_err(st, rs).values()) <= 1e-6
+
+
+def test_fp32_mesh_world_runs(rbps, ref):
+    """The FP32 colored engine on the bumpy-mesh world: finite, and one step
+    within 1e-4 of the FP64 oracle (the step before any body lands)."""
+    spec = scenes.mesh_world(seed=5, n=24)
+    sc = scenes.Scene("mesh", 1.0 / 60.0, 10, 60, [spec])
+    w = ref.RefWorld(spec, sc.timestep, sc.substeps)
+    w.step(1)
+    b = rbps.Batch.from_scene(sc, abi.PRECISION_FP32, abi.SOLVE_COLORED)
+    b.step(1)
+    err = state_err(b.state(0), w.state())
+    assert max(err["position"], err["orientation"]) <= 1e-4, err
+    b.step(59)
+    st = b.state(0)
+    for k in st:
+        assert np.isfinite(st[k]).all(), k
