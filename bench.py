@@ -258,7 +258,8 @@ def single_world(args, ws, rank, local):
     # SAP pairs grow past the default 8 per object within ~20 steps
     pair_cap = 1 << 21 if args.workload == "joint_heavy" else 0
     batch = rbps_b200.Batch.from_scene(scene, abi.PRECISION_FP32, abi.SOLVE_COLORED, device=local,
-                                       stream=stream.cuda_stream, max_pairs_per_world=pair_cap)
+                                       stream=stream.cuda_stream, max_pairs_per_world=pair_cap,
+                                       block_threads=args.block)
     batch.step(args.warmup)
     batch.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
