@@ -403,6 +403,71 @@ namespace rbps_gpu
     // Candidates whose bodies have used all 64 colours go to the serial
     // colour; idle candidates get kColorIdle and are not bucketed.  Returns
     // the number of regular colours; corder / colour offsets are filled.
+    // Second-level colours for the overflow bucket [coff[64], coff[65]) of
+    // corder: the team leader colours its candidates first-fit in order on
+    // a second set of body masks (bprio, free after the Jones-Plassmann
+    // rounds), and the bucket is reordered by those colours, so that the
+    // solves can relax it colour by colour (kMiscC2Off) instead of on one
+    // thread; entry 64 keeps what still does not fit.  The bucket comes
+    // after every first-level colour, so the Gauss-Seidel order stays a
+    // sequence of conflict-free sets.
+    template <class T, class P, class Team>
+    __device__ void color_overflow(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S)
+    {
+        uint32_t *misc = S.misc;
+        const uint32_t s0 = misc[kMiscCOff + kColorSerial], s1 = misc[kMiscCOff + kColorSerial + 1];
+        uint32_t *cnt = misc + kMiscC2Count, *off = misc + kMiscC2Off;
+        for (uint32_t k = tm.rank(); k < 66; k += tm.size())
+            cnt[k] = 0u;
+        if (s1 > s0)
+        {
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+                S.bprio[b] = 0ull;
+            for (uint32_t q = s0 + tm.rank(); q < s1; q += tm.size())
+                S.alist[q - s0] = S.corder[q];
+        }
+        tm.sync();
+        if (tm.leader())
+        {
+            const uint8_t *type = E.B.type + W.body_off;
+            for (uint32_t q = 0; q < s1 - s0; ++q)
+            {
+                const uint32_t c = S.alist[q];
+                const Cand cd = S.cand[c];
+                const bool da = type[cd.ba] == kDynamic, db = type[cd.bb] == kDynamic;
+                const unsigned long long used = (da ? S.bprio[cd.ba] : 0ull) | (db ? S.bprio[cd.bb] : 0ull);
+                uint32_t col = kColorSerial;
+                if (used != ~0ull)
+                {
+                    col = (uint32_t)(__ffsll((long long)~used) - 1);
+                    const unsigned long long bit = 1ull << col;
+                    if (da)
+                        S.bprio[cd.ba] |= bit;
+                    if (db)
+                        S.bprio[cd.bb] |= bit;
+                }
+                S.act[c] = col;
+                cnt[col] += 1u;
+            }
+            uint32_t run = s0;
+            for (uint32_t k = 0; k <= kColorSerial; ++k)
+            {
+                const uint32_t n = cnt[k];
+                off[k] = run;
+                cnt[k] = run; // fill cursor
+                run += n;
+            }
+            off[kColorSerial + 1] = run;
+        }
+        tm.sync();
+        for (uint32_t q = tm.rank(); q < s1 - s0; q += tm.size())
+        {
+            const uint32_t c = S.alist[q];
+            S.corder[atomicAdd(&cnt[S.act[c]], 1u)] = c;
+        }
+        tm.sync();
+    }
+
     template <class T, class P, class Team>
     __device__ uint32_t color_active(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
                                      uint32_t n_cand, BlockShared &sh)
@@ -513,6 +578,7 @@ namespace rbps_gpu
             S.corder[slot] = c;
         }
         tm.sync();
+        color_overflow(E, tm, W, S);
         return misc[kMiscFlags + 1];
     }
 
@@ -872,8 +938,28 @@ namespace rbps_gpu
             }
             if (coff[kColorSerial + 1] > coff[kColorSerial])
             {
+                // the overflow bucket: second-level colours (global misc),
+                // then on one thread what is left
+                const uint32_t *c2 = S.misc + kMiscC2Off;
+                uint32_t serial0 = coff[kColorSerial];
+                if (!book)
+                {
+                    for (uint32_t col = 0; col < kColorSerial; ++col)
+                    {
+                        if (c2[col + 1] == c2[col])
+                            continue;
+                        for (uint32_t q = c2[col] + tm.rank(); q < c2[col + 1]; q += tm.size())
+                        {
+                            const uint32_t c = S.corder[q];
+                            const Cand cd = S.cand[c];
+                            solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                        }
+                        tm.sync();
+                    }
+                    serial0 = c2[kColorSerial];
+                }
                 if (tm.leader())
-                    for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
+                    for (uint32_t q = serial0; q < coff[kColorSerial + 1]; ++q)
                     {
                         const uint32_t c = S.corder[q];
                         const Cand cd = S.cand[c];
@@ -965,8 +1051,26 @@ namespace rbps_gpu
             }
             if (coff[kColorSerial + 1] > coff[kColorSerial])
             {
+                const uint32_t *c2 = S.misc + kMiscC2Off;
+                uint32_t serial0 = coff[kColorSerial];
+                if (!book)
+                {
+                    for (uint32_t col = 0; col < kColorSerial; ++col)
+                    {
+                        if (c2[col + 1] == c2[col])
+                            continue;
+                        for (uint32_t q = c2[col] + tm.rank(); q < c2[col + 1]; q += tm.size())
+                        {
+                            const uint32_t c = S.corder[q];
+                            const Cand cd = S.cand[c];
+                            solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                        }
+                        tm.sync();
+                    }
+                    serial0 = c2[kColorSerial];
+                }
                 if (tm.leader())
-                    for (uint32_t q = coff[kColorSerial]; q < coff[kColorSerial + 1]; ++q)
+                    for (uint32_t q = serial0; q < coff[kColorSerial + 1]; ++q)
                     {
                         const uint32_t c = S.corder[q];
                         const Cand cd = S.cand[c];
@@ -1336,135 +1440,6 @@ namespace rbps_gpu
             narrow_flat<T, P, kSelBoxBox>(E, i);
     }
 
-    // Jones-Plassmann colouring of one world's contacting candidates by one
-    // warp (same rule as color_active) and its colour buckets (corder /
-    // colour offsets in misc).
-    template <class T, class P>
-    __device__ void warp_color_world(const Engine<T, P> &E, uint32_t w)
-    {
-        const uint32_t lane = lane_id();
-        const uint32_t full = 0xffffffffu;
-        const WorldDev W = E.worlds[w];
-        const Scr<T, P> S = world_scratch(E, W);
-        uint32_t *misc = S.misc;
-        const uint32_t n_cand = misc[kMiscNCand];
-        for (uint32_t b = lane; b < W.n_bodies; b += 32)
-        {
-            S.bmask[b] = 0ull;
-            S.bprio[b] = 0ull;
-        }
-        for (uint32_t k = lane; k < 66; k += 32)
-            misc[kMiscCCount + k] = 0u;
-        // compact the contacting candidates into alist
-        uint32_t n_act = 0;
-        const uint32_t lt = (1u << lane) - 1u;
-        for (uint32_t base = 0; base < n_cand; base += 32)
-        {
-            const uint32_t c = base + lane;
-            const bool live = c < n_cand;
-            const bool act = live && S.cc[c].n > 0;
-            const uint32_t m = __ballot_sync(full, act);
-            if (act)
-            {
-                S.alist[n_act + __popc(m & lt)] = c;
-                S.color[c] = 0xffffffffu;
-            }
-            else if (live)
-                S.color[c] = kColorIdle;
-            n_act += __popc(m);
-        }
-        __syncwarp();
-        const uint8_t *type = E.B.type + W.body_off;
-        uint32_t round = 1;
-        for (; round <= kMaxColorRounds && n_act; ++round)
-        {
-            for (uint32_t q = lane; q < n_act; q += 32)
-            {
-                const uint32_t c = S.alist[q];
-                if (S.color[c] != 0xffffffffu)
-                    continue;
-                const Cand cd = S.cand[c];
-                const unsigned long long val = ((unsigned long long)round << 56) |
-                                               ((unsigned long long)(hash32(c) & 0xffffffu) << 32) | c;
-                if (type[cd.ba] == kDynamic)
-                    atomicMax(&S.bprio[cd.ba], val);
-                if (type[cd.bb] == kDynamic)
-                    atomicMax(&S.bprio[cd.bb], val);
-            }
-            __syncwarp();
-            uint32_t left = 0;
-            for (uint32_t q = lane; q < n_act; q += 32)
-            {
-                const uint32_t c = S.alist[q];
-                if (S.color[c] != 0xffffffffu)
-                    continue;
-                const Cand cd = S.cand[c];
-                const unsigned long long val = ((unsigned long long)round << 56) |
-                                               ((unsigned long long)(hash32(c) & 0xffffffu) << 32) | c;
-                const bool da = type[cd.ba] == kDynamic, db = type[cd.bb] == kDynamic;
-                const bool won = (!da || S.bprio[cd.ba] == val) && (!db || S.bprio[cd.bb] == val);
-                if (!won)
-                {
-                    ++left;
-                    continue;
-                }
-                const unsigned long long used = (da ? S.bmask[cd.ba] : 0ull) | (db ? S.bmask[cd.bb] : 0ull);
-                uint32_t col;
-                if (used == ~0ull)
-                    col = kColorSerial;
-                else
-                {
-                    col = (uint32_t)(__ffsll((long long)~used) - 1);
-                    const unsigned long long bit = 1ull << col;
-                    if (da)
-                        S.bmask[cd.ba] |= bit;
-                    if (db)
-                        S.bmask[cd.bb] |= bit;
-                }
-                S.color[c] = col;
-            }
-            left = __reduce_add_sync(full, left);
-            __syncwarp();
-            if (left == 0)
-                break;
-        }
-        if (round > kMaxColorRounds)
-        {
-            for (uint32_t q = lane; q < n_act; q += 32)
-                if (S.color[S.alist[q]] == 0xffffffffu)
-                    S.color[S.alist[q]] = kColorSerial;
-            __syncwarp();
-        }
-        for (uint32_t q = lane; q < n_act; q += 32)
-            atomicAdd(&misc[kMiscCCount + S.color[S.alist[q]]], 1u);
-        __syncwarp();
-        if (lane == 0)
-        {
-            uint32_t run = 0, ncol = 0;
-            for (uint32_t k = 0; k <= kColorSerial; ++k)
-            {
-                const uint32_t n = misc[kMiscCCount + k];
-                misc[kMiscCOff + k] = run;
-                misc[kMiscCCount + k] = run; // becomes the fill cursor
-                if (n && k < kColorSerial)
-                    ncol = k + 1;
-                run += n;
-            }
-            misc[kMiscCOff + kColorSerial + 1] = run;
-            misc[kMiscNColors] = ncol;
-            if (ncol > misc[kMiscMaxColors])
-                misc[kMiscMaxColors] = ncol;
-        }
-        __syncwarp();
-        for (uint32_t q = lane; q < n_act; q += 32)
-        {
-            const uint32_t c = S.alist[q];
-            const uint32_t slot = atomicAdd(&misc[kMiscCCount + S.color[c]], 1u);
-            S.corder[slot] = c;
-        }
-        __syncwarp();
-    }
-
     // The rest of a substep for one world per warp: colouring, integrate
     // (Body.cpp:18-39), position solve + velocity update, velocity solve.
     // The contacting candidates of world W into S.alist, in candidate
@@ -1650,6 +1625,8 @@ namespace rbps_gpu
             for (uint32_t k = tm.rank(); k < 66; k += tm.size())
                 misc[kMiscCOff + k] = off[k];
         tm.sync();
+        if (!book) // the solves then take the overflow bucket by second-level colours
+            color_overflow(E, tm, W, S);
         return book ? book[132] : misc[kMiscNColors];
     }
 

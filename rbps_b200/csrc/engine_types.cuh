@@ -84,12 +84,16 @@ namespace rbps_gpu
     constexpr uint32_t kColorStage = 256;  // candidates staged in shared memory per colouring chunk
     constexpr uint32_t kColorIdle = 65;    // candidate without contact rows this substep
     constexpr uint32_t kMaxColorRounds = 96;
-    constexpr uint32_t kMiscWords = 64 + 2 * 66 + kMaxColorRounds + 8;
+    constexpr uint32_t kMiscWords = 64 + 4 * 66 + kMaxColorRounds + 8;
     // misc layout (u32 words)
     constexpr uint32_t kMiscFlags = 0;                  // [0..7] scalars
     constexpr uint32_t kMiscCCount = 8;                 // 66 colour counts
     constexpr uint32_t kMiscCOff = 8 + 66;              // 66 colour offsets (+ fill)
     constexpr uint32_t kMiscLeft = 8 + 2 * 66;          // per-round "uncoloured left"
+    // second-level colours of the overflow bucket (colour kColorSerial):
+    // 66 counts, then 66 offsets into corder (entry 64: still serial)
+    constexpr uint32_t kMiscC2Count = kMiscLeft + kMaxColorRounds;
+    constexpr uint32_t kMiscC2Off = kMiscC2Count + 66;
     // misc scalars: kMiscFlags + 1 colours of this substep, + 2 contact rows,
     // + 3 GJK candidates, + 4 unclamped SAP pairs, + 5 SAP pairs, + 6 narrowphase
     // candidates, + 7 most colours over the step's substeps
