@@ -430,24 +430,41 @@ namespace rbps_gpu
         if (tm.leader())
         {
             const uint8_t *type = E.B.type + W.body_off;
-            for (uint32_t q = 0; q < s1 - s0; ++q)
+            constexpr uint32_t kAhead = 8; // candidates loaded ahead of the mask updates
+            const uint32_t ns = s1 - s0;
+            for (uint32_t q0 = 0; q0 < ns; q0 += kAhead)
             {
-                const uint32_t c = S.alist[q];
-                const Cand cd = S.cand[c];
-                const bool da = type[cd.ba] == kDynamic, db = type[cd.bb] == kDynamic;
-                const unsigned long long used = (da ? S.bprio[cd.ba] : 0ull) | (db ? S.bprio[cd.bb] : 0ull);
-                uint32_t col = kColorSerial;
-                if (used != ~0ull)
-                {
-                    col = (uint32_t)(__ffsll((long long)~used) - 1);
-                    const unsigned long long bit = 1ull << col;
-                    if (da)
-                        S.bprio[cd.ba] |= bit;
-                    if (db)
-                        S.bprio[cd.bb] |= bit;
-                }
-                S.act[c] = col;
-                cnt[col] += 1u;
+                uint32_t cs[kAhead];
+                Cand cd[kAhead];
+                bool da[kAhead], db[kAhead];
+#pragma unroll
+                for (uint32_t k = 0; k < kAhead; ++k)
+                    if (q0 + k < ns)
+                    {
+                        cs[k] = S.alist[q0 + k];
+                        cd[k] = S.cand[cs[k]];
+                        da[k] = type[cd[k].ba] == kDynamic;
+                        db[k] = type[cd[k].bb] == kDynamic;
+                    }
+#pragma unroll
+                for (uint32_t k = 0; k < kAhead; ++k)
+                    if (q0 + k < ns)
+                    {
+                        const unsigned long long used =
+                            (da[k] ? S.bprio[cd[k].ba] : 0ull) | (db[k] ? S.bprio[cd[k].bb] : 0ull);
+                        uint32_t col = kColorSerial;
+                        if (used != ~0ull)
+                        {
+                            col = (uint32_t)(__ffsll((long long)~used) - 1);
+                            const unsigned long long bit = 1ull << col;
+                            if (da[k])
+                                S.bprio[cd[k].ba] |= bit;
+                            if (db[k])
+                                S.bprio[cd[k].bb] |= bit;
+                        }
+                        S.act[cs[k]] = col;
+                        cnt[col] += 1u;
+                    }
             }
             uint32_t run = s0;
             for (uint32_t k = 0; k <= kColorSerial; ++k)
