@@ -819,6 +819,27 @@ namespace rbps_gpu
                                   make_layout(W.n_bp, W.n_bodies, W.pair_cap, W.n_pc, sizeof(CandContacts<T, P>)));
     }
 
+    // Bodies of corder slot q (candidate c): from the packed pair written at
+    // colouring when the team keeps its world in shared memory (book), else
+    // from the candidate.
+    template <class T, class P>
+    __device__ __forceinline__ void slot_pair(const Scr<T, P> &S, const uint32_t *book, uint32_t q, uint32_t c,
+                                              uint32_t &ba, uint32_t &bb)
+    {
+        if (book)
+        {
+            const uint32_t pr = S.act[q];
+            ba = pr & 0xffffu;
+            bb = pr >> 16;
+        }
+        else
+        {
+            const Cand cd = S.cand[c];
+            ba = cd.ba;
+            bb = cd.bb;
+        }
+    }
+
     // Asks L2 for every 128-byte line of [p, p + bytes) (prefetch.global.L2).
     __device__ __forceinline__ void prefetch_l2_range(const void *p, size_t bytes)
     {
@@ -948,8 +969,9 @@ namespace rbps_gpu
                 for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
                 {
                     const uint32_t c = S.corder[q];
-                    const Cand cd = S.cand[c];
-                    solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                    uint32_t ba, bb;
+                    slot_pair(S, book, q, c, ba, bb);
+                    solve_pair_position(B, E.inv_h, boff + ba, boff + bb, S.cc[c]);
                 }
                 tm.sync();
             }
@@ -1061,8 +1083,9 @@ namespace rbps_gpu
                 for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
                 {
                     const uint32_t c = S.corder[q];
-                    const Cand cd = S.cand[c];
-                    solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                    uint32_t ba, bb;
+                    slot_pair(S, book, q, c, ba, bb);
+                    solve_pair_velocity(B, E.h, boff + ba, boff + bb, S.cc[c]);
                 }
                 tm.sync();
             }
@@ -1633,6 +1656,14 @@ namespace rbps_gpu
             const uint32_t c = S.alist[q];
             const uint32_t slot = atomicAdd(&cnt[S.color[c]], 1u);
             S.corder[slot] = c;
+            // a team with its world in shared memory keeps the body pair of
+            // each slot beside corder (world-local indices < 65536), so the
+            // colour-by-colour solves need not read the candidate first
+            if (book)
+            {
+                const Cand cd = S.cand[c];
+                S.act[slot] = cd.ba | (cd.bb << 16);
+            }
             // the position and velocity solves read this candidate's contact
             // block colour by colour, each read behind a barrier: start it
             // on its way to L2 now, while integrate runs
