@@ -455,6 +455,7 @@ def main():
                     help="untimed steps before the warm-up (240 = 2 s simulated: the bodies have landed)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--autotune", type=int, default=1, help="1: run the launch-shape autotuner before timing")
     ap.add_argument("--plain-worlds", type=int, default=64,
                     help="worlds in the plain per-world GPU sample (0 = skip it)")
     ap.add_argument("--workload", default="batched",
@@ -520,6 +521,9 @@ def main():
     if args.preroll:
         batch.step(args.preroll)
     batch.step(args.warmup)
+    # launch shapes picked by the project autotuner on these worlds (untimed;
+    # it rewinds the batch to where it started)
+    tune = batch.autotune(trial_steps=3) if args.autotune else None
     # the e2e leg rewinds here, so that both legs time the same steps
     snap = batch.snapshot()
     batch.synchronize()
@@ -616,6 +620,7 @@ def main():
                            "l2": f"inputs larger than L2: {dev_bytes / 1e6:.0f} MB of world state and scratch "
                                  "touched every step (L2 126 MB)",
                            "parallelism": f"world-sharded replicas x{ws}", "seed": args.seed,
+                           "autotune": tune,
                            "state_finite": finite},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,

@@ -344,6 +344,26 @@ RBPS_API int rbps_batch_restore(rbps_batch *batch, uint32_t slot);
 /* Overwrites snapshot `slot` with the current state. */
 RBPS_API int rbps_batch_snapshot_update(rbps_batch *batch, uint32_t slot);
 
+/* Launch configuration chosen by rbps_batch_autotune. */
+typedef struct rbps_tune_result {
+    int32_t frame_block;          /* threads per CTA of the frame (SAP) kernel */
+    int32_t narrow_grid;          /* CTAs of the narrowphase kernels           */
+    double ms_per_step;           /* trial time of the chosen configuration    */
+    double ms_per_step_default;   /* trial time of the configuration before    */
+    uint32_t trials;              /* configurations timed                      */
+    uint32_t pad_;
+} rbps_tune_result;
+
+/* Project autotuner (no reference counterpart; the batched design picks its
+ * launch shapes by measurement): times `trial_steps` steps of the batch's
+ * own worlds under each candidate configuration -- frame kernel at 128 or
+ * 256 threads, narrowphase grid at 1/2, 1 or 2 times its occupancy bound --
+ * from the same device snapshot, keeps the fastest and rewinds the batch to
+ * the snapshot, so the state is as before the call.  The configuration
+ * changes launch shapes only: results stay bit for bit the same.  Blocks
+ * the host until done. */
+RBPS_API int rbps_batch_autotune(rbps_batch *batch, int32_t trial_steps, rbps_tune_result *result);
+
 /* Per-world body state, host doubles (converted from the device precision). */
 RBPS_API int rbps_batch_get_state(rbps_batch *batch, uint32_t world, const rbps_state_view *view);
 RBPS_API int rbps_batch_set_state(rbps_batch *batch, uint32_t world, const rbps_state_view *view);

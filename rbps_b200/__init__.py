@@ -49,6 +49,11 @@ class StateView(C.Structure):
     _fields_ = [("position", _D), ("orientation", _D), ("linear_velocity", _D), ("angular_velocity", _D)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("frame_block", C.c_int32), ("narrow_grid", C.c_int32), ("ms_per_step", C.c_double),
+                ("ms_per_step_default", C.c_double), ("trials", C.c_uint32), ("pad_", C.c_uint32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("steps", C.c_uint64), ("pairs", C.c_uint64), ("candidates", C.c_uint64),
                 ("contacts", C.c_uint64), ("max_colors", C.c_uint32), ("serial_overflow", C.c_uint32),
@@ -83,6 +88,7 @@ def lib():
             "rbps_batch_snapshot": (i, [_P, C.POINTER(C.c_uint32)]),
             "rbps_batch_snapshot_update": (i, [_P, C.c_uint32]),
             "rbps_batch_restore": (i, [_P, C.c_uint32]),
+            "rbps_batch_autotune": (i, [_P, C.c_int32, C.POINTER(TuneResult)]),
             "rbps_world_add_collider": (i, [_P, C.c_uint32, _P, _U]),
             "rbps_world_add_colliders": (i, [_P, C.c_uint32, C.c_uint32, _P, _U]),
             "rbps_world_add_joint": (i, [_P, C.c_uint32, _P, _U]),
@@ -305,6 +311,13 @@ class Batch:
     def step_io(self, force_ptr, pos_ptr, rot_ptr):
         """One step with host I/O through raw host pointers (ints or None)."""
         _check(lib().rbps_batch_step_io(self.h, force_ptr, pos_ptr, rot_ptr))
+
+    def autotune(self, trial_steps=3):
+        """Times the launch-shape candidates on this batch's own worlds from
+        one snapshot, keeps the fastest, rewinds; returns the choice."""
+        r = TuneResult()
+        _check(lib().rbps_batch_autotune(self.h, trial_steps, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_ if k != "pad_"}
 
     def snapshot(self):
         """Device-side snapshot of the whole batch state; returns its slot."""

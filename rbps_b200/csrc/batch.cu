@@ -2461,6 +2461,98 @@ extern "C" int rbps_batch_restore(rbps_batch *b, uint32_t slot)
     return DISPATCH_PREC(b, snapshot_copy, b, b->snaps[slot], 1);
 }
 
+// ------------------------------------------------------------ autotuner
+// Frame-kernel block (its grid follows from occupancy) and narrowphase grid.
+template <class T, class P>
+static int apply_launch(rbps_batch *b, int frame_block, int narrow_grid)
+{
+    if (!b->small_ids.empty())
+    {
+        int per_sm = 0;
+        CU(occupancy_phase<T, P>(kKFrame, frame_block, &per_sm));
+        if (per_sm < 1)
+            return fail(RBPS_ERR_CUDA, "frame kernel cannot be resident with %d threads", frame_block);
+        b->phase.block[kKFrame] = frame_block;
+        b->phase.grid[kKFrame] = std::min<int>((int)b->small_ids.size(), per_sm * b->sm_count);
+    }
+    if (b->use_flat)
+        b->flat.grid_narrow = std::max(1, narrow_grid);
+    b->graph_key = -1; // recapture the step graph with the new shapes
+    return RBPS_OK;
+}
+
+template <class T, class P>
+static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
+{
+    int rc;
+    uint32_t slot = 0;
+    if ((rc = snapshot_new<T, P>(b, &slot)))
+        return rc;
+    const uint64_t steps0 = b->steps_done;
+    const int fb0 = b->phase.block[kKFrame], ng0 = b->flat.grid_narrow;
+    std::vector<std::pair<int, int>> cand = {{fb0, ng0}};
+    for (int fb : {128, 256})
+        for (int f2 : {1, 2, 4}) // narrowphase grid x 1/2, 1, 2
+        {
+            const std::pair<int, int> c(fb, std::max(1, ng0 * f2 / 2));
+            if (std::find(cand.begin(), cand.end(), c) == cand.end())
+                cand.push_back(c);
+        }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    double best = 1e300, first = 0.0;
+    std::pair<int, int> best_c = cand[0];
+    for (size_t k = 0; k < cand.size(); ++k)
+    {
+        if ((rc = apply_launch<T, P>(b, cand[k].first, cand[k].second)) ||
+            (rc = snapshot_copy<T, P>(b, b->snaps[slot], 1)) || (rc = step_typed<T, P>(b, 1)))
+            break;
+        CU(cudaEventRecord(e0, b->stream));
+        if ((rc = step_typed<T, P>(b, trials)))
+            break;
+        CU(cudaEventRecord(e1, b->stream));
+        CU(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CU(cudaEventElapsedTime(&ms, e0, e1));
+        const double per = ms / trials;
+        if (k == 0)
+            first = per;
+        if (per < best)
+        {
+            best = per;
+            best_c = cand[k];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc)
+        return rc;
+    if ((rc = apply_launch<T, P>(b, best_c.first, best_c.second)) ||
+        (rc = snapshot_copy<T, P>(b, b->snaps[slot], 1)))
+        return rc;
+    CU(cudaStreamSynchronize(b->stream));
+    b->steps_done = steps0;
+    if (out)
+    {
+        std::memset(out, 0, sizeof(*out));
+        out->frame_block = best_c.first;
+        out->narrow_grid = best_c.second;
+        out->ms_per_step = best;
+        out->ms_per_step_default = first;
+        out->trials = (uint32_t)cand.size();
+    }
+    return check_device_error(b);
+}
+
+extern "C" int rbps_batch_autotune(rbps_batch *b, int32_t trial_steps, rbps_tune_result *out)
+{
+    if (!b || !b->committed || trial_steps < 1)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_autotune: commit first; trial_steps >= 1");
+    CU(cudaSetDevice(b->desc.device));
+    return DISPATCH_PREC(b, autotune_typed, b, trial_steps, out);
+}
+
 extern "C" int rbps_batch_step_io(rbps_batch *b, const double *force_in, double *position_out, double *orientation_out)
 {
     if (!b || !b->committed)
