@@ -222,6 +222,44 @@ def plain_gpu_run(scene, batch, n_sample, steps, warmup, stream):
                    f"FP32 colored, {warmup} untimed + {steps} timed steps from the batched state")
 
 
+def one_step_error(scene, n_worlds, stream):
+    """Per-world one-step state error of FP32 against the FP64
+    reference-order engine (the device engine that matches the oracle bit
+    for bit) on the first n_worlds worlds of the scene, from the initial
+    state: max over a world's bodies of the relative position / orientation
+    error (relative to max(|x|, 1)).  Two FP32 runs: the colored solver the
+    bench times (its colour order differs from the reference's sequential
+    order) and the FP32 reference order (precision alone).  Worlds where
+    the reference itself goes non-finite are counted, not compared."""
+    import rbps_b200
+    from rbps_b200 import abi
+    sub = type(scene)(scene.name, scene.timestep, scene.substeps, scene.steps, scene.worlds[:n_worlds])
+    runs = {}
+    for name, prec, solve in (("fp32_colored", abi.PRECISION_FP32, abi.SOLVE_COLORED),
+                              ("fp32_reference_order", abi.PRECISION_FP32, abi.SOLVE_REFERENCE_ORDER),
+                              ("fp64", abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER)):
+        b = rbps_b200.Batch.from_scene(sub, prec, solve, stream=stream.cuda_stream)
+        b.step(1)
+        runs[name] = [b.state(w) for w in range(len(sub.worlds))]
+        b.close()
+    ok = [np.isfinite(r["position"]).all() and np.isfinite(r["orientation"]).all() for r in runs["fp64"]]
+    out = {"worlds": int(sum(ok)), "fp64_nonfinite_worlds": int(len(ok) - sum(ok)),
+           "against": "FP64 reference order (bit-identical to the reference engine), state after step 1"}
+    for name in ("fp32_colored", "fp32_reference_order"):
+        e = []
+        for a, r, good in zip(runs[name], runs["fp64"], ok):
+            if not good:
+                continue
+            ep = np.abs(a["position"] - r["position"]) / np.maximum(np.abs(r["position"]), 1.0)
+            sign = np.where((a["orientation"] * r["orientation"]).sum(1, keepdims=True) < 0, -1.0, 1.0)
+            eq = np.abs(a["orientation"] * sign - r["orientation"])
+            e.append(float(max(ep.max(), eq.max())))
+        e = np.array(e) if e else np.zeros(1)
+        out[name] = {"median": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
+                     "within_1e-5": int((e <= 1e-5).sum())}
+    return out
+
+
 SINGLE_WORLD = {
     "collision_stress": ("config1_collision_stress",
                          "body-substeps/s (collision stress: 65,536 mixed bodies incl. convex hulls, one world)"),
@@ -592,6 +630,8 @@ def main():
     e2e_value = n_dyn_all * scene.substeps * e2e_steps / (e2e_ms / 1e3)
     finite = bool(np.isfinite(p_host.numpy()).all() and np.isfinite(p_host2.numpy()).all())
 
+    err1 = one_step_error(scene, min(256, len(scene.worlds)), stream) if rank == 0 else None
+
     plain = None
     if args.plain_worlds > 0:
         pv, pinfo = plain_gpu_run(scene, batch, args.plain_worlds, min(args.steps, 20), args.warmup, stream)
@@ -628,6 +668,7 @@ def main():
                              "kernel": f"one step = {st['kernel_launches'] // max(args.steps, 1)} phase-kernel launches"},
                 "cpu_baseline": cpu,
                 "plain_gpu": plain,
+                "one_step_error_vs_fp64": err1,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n_tot_all) * 24,
                         "d2h_bytes_per_step": int(n_tot_all) * 56, "steps": e2e_steps,
                         "window": "the same steps as value (device snapshot after the warm-up, restored)"},
