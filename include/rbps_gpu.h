@@ -351,13 +351,15 @@ typedef struct rbps_tune_result {
     double ms_per_step;           /* trial time of the chosen configuration    */
     double ms_per_step_default;   /* trial time of the configuration before    */
     uint32_t trials;              /* configurations timed                      */
-    uint32_t pad_;
+    uint32_t team_bodies;         /* worlds this large step on a whole CTA     */
 } rbps_tune_result;
 
 /* Project autotuner (no reference counterpart; the batched design picks its
  * launch shapes by measurement): times `trial_steps` steps of the batch's
  * own worlds under each candidate configuration -- frame kernel at 128 or
- * 256 threads, narrowphase grid at 1/2, 1 or 2 times its occupancy bound --
+ * 256 threads, narrowphase grid at 1/2, 1 or 2 times its occupancy bound,
+ * then the body count from which a world steps on a whole CTA instead of a
+ * warp (64 to 192) --
  * from the same device snapshot, keeps the fastest and rewinds the batch to
  * the snapshot, so the state is as before the call.  The configuration
  * changes launch shapes only: results stay bit for bit the same.  Blocks

@@ -51,7 +51,7 @@ class StateView(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("frame_block", C.c_int32), ("narrow_grid", C.c_int32), ("ms_per_step", C.c_double),
-                ("ms_per_step_default", C.c_double), ("trials", C.c_uint32), ("pad_", C.c_uint32)]
+                ("ms_per_step_default", C.c_double), ("trials", C.c_uint32), ("team_bodies", C.c_uint32)]
 
 
 class Stats(C.Structure):

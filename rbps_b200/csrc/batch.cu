@@ -326,6 +326,7 @@ struct rbps_batch
     std::vector<HostHull> hulls;
     std::vector<HostHeightmap> heightmaps;
     std::vector<HostMesh> meshes;
+    uint32_t team_bodies = 0; // worlds this large step on a whole CTA (set_team_split)
     MeshDesc *mesh_desc = nullptr;
     double *mesh_v = nullptr, *mesh_n = nullptr;
     uint32_t *mesh_i = nullptr;
@@ -918,6 +919,31 @@ namespace
     constexpr uint32_t kSmemBodiesMax = 1024;   // bodies a CTA world keeps in shared memory (137 KB in FP32)
 } // namespace
 
+// Worlds of `threshold` bodies or more step on a whole CTA in the substep
+// kernel, the rest on one warp each (small_ids is sorted by body count);
+// shared-memory world copies hold the largest CTA world or four warp worlds
+// (a world beyond its cap runs on the batch arrays).
+template <class T, class P>
+static int set_team_split(rbps_batch *b, uint32_t threshold)
+{
+    const uint32_t ns = (uint32_t)b->small_ids.size();
+    uint32_t nbw = 0;
+    while (nbw < ns && b->wdev[b->small_ids[nbw]].n_bodies >= threshold)
+        ++nbw;
+    b->n_block_worlds = nbw;
+    b->flat.grid_solve = (int)(nbw + (ns - nbw + 3) / 4);
+    auto round16 = [](uint32_t x) { return (x + 15u) / 16u * 16u; };
+    b->smem_cap_warp = round16(threshold);
+    b->smem_cap_block = 0;
+    if (nbw)
+        b->smem_cap_block = round16(std::min<uint32_t>(b->wdev[b->small_ids[0]].n_bodies, kSmemBodiesMax));
+    b->flat.substep_smem =
+        std::max(4 * smem_world_bytes<T, P>(b->smem_cap_warp), smem_world_bytes<T, P>(b->smem_cap_block));
+    CU(prepare_substep<T, P>(b->flat.substep_smem));
+    b->team_bodies = threshold;
+    return RBPS_OK;
+}
+
 template <class T, class P>
 static int commit_typed(rbps_batch *b)
 {
@@ -1476,23 +1502,8 @@ static int commit_typed(rbps_batch *b)
         CU(occupancy_flat<T, P>(0, kMaxBlockHost, &per_sm, 0));
         b->flat.grid_narrow = std::max(1, per_sm) * b->sm_count;
         b->flat.block_solve = 128;
-        // worlds of kBlockTeamBodies bodies or more step on a whole CTA, the
-        // rest on one warp each (small_ids is sorted by body count)
-        uint32_t nbw = 0;
-        while (nbw < ns && b->wdev[b->small_ids[nbw]].n_bodies >= kBlockTeamBodies)
-            ++nbw;
-        b->n_block_worlds = nbw;
-        b->flat.grid_solve = (int)(nbw + (ns - nbw + 3) / 4);
-        // shared-memory world copies: the largest CTA world, or four warp
-        // worlds (a world beyond its cap runs on the batch arrays)
-        auto round16 = [](uint32_t x) { return (x + 15u) / 16u * 16u; };
-        b->smem_cap_warp = round16(kBlockTeamBodies);
-        b->smem_cap_block = 0;
-        if (nbw)
-            b->smem_cap_block = round16(std::min<uint32_t>(b->wdev[b->small_ids[0]].n_bodies, kSmemBodiesMax));
-        b->flat.substep_smem = std::max(4 * smem_world_bytes<T, P>(b->smem_cap_warp),
-                                        smem_world_bytes<T, P>(b->smem_cap_block));
-        CU(prepare_substep<T, P>(b->flat.substep_smem));
+        if ((rc = set_team_split<T, P>(b, kBlockTeamBodies)))
+            return rc;
         b->use_flat = true;
         // side stream + events for the parallel narrowphase kernels
         CU(cudaStreamCreateWithFlags(&b->flat.side, cudaStreamNonBlocking));
@@ -2524,6 +2535,38 @@ static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
             best_c = cand[k];
         }
     }
+    // then the CTA / warp team split of the substep kernel, with the best
+    // shapes above
+    const uint32_t tb0 = b->team_bodies;
+    uint32_t best_t = tb0;
+    uint32_t n_trials = (uint32_t)cand.size();
+    if (!rc && b->use_flat)
+    {
+        rc = apply_launch<T, P>(b, best_c.first, best_c.second);
+        for (uint32_t tb : {64u, 96u, 160u, 192u})
+        {
+            if (rc || tb == tb0)
+                continue;
+            ++n_trials;
+            if ((rc = set_team_split<T, P>(b, tb)) || (rc = apply_launch<T, P>(b, best_c.first, best_c.second)) ||
+                (rc = snapshot_copy<T, P>(b, b->snaps[slot], 1)) || (rc = step_typed<T, P>(b, 1)))
+                break;
+            CU(cudaEventRecord(e0, b->stream));
+            if ((rc = step_typed<T, P>(b, trials)))
+                break;
+            CU(cudaEventRecord(e1, b->stream));
+            CU(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CU(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms / trials < best)
+            {
+                best = ms / trials;
+                best_t = tb;
+            }
+        }
+        if (!rc)
+            rc = set_team_split<T, P>(b, best_t);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc)
@@ -2540,7 +2583,8 @@ static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
         out->narrow_grid = best_c.second;
         out->ms_per_step = best;
         out->ms_per_step_default = first;
-        out->trials = (uint32_t)cand.size();
+        out->trials = n_trials;
+        out->team_bodies = best_t;
     }
     return check_device_error(b);
 }
