@@ -610,8 +610,9 @@ def main():
     p_host = torch.empty((n_tot, 3), dtype=torch.float64, pin_memory=True)
     q_host = torch.empty((n_tot, 4), dtype=torch.float64, pin_memory=True)
     # two pose buffers, alternating: every step's poses land on the host
-    p_host2 = torch.empty_like(p_host)
-    q_host2 = torch.empty_like(q_host)
+    # (torch.empty_like would not pin them: a pageable target turns the copy synchronous)
+    p_host2 = torch.empty((n_tot, 3), dtype=torch.float64, pin_memory=True)
+    q_host2 = torch.empty((n_tot, 4), dtype=torch.float64, pin_memory=True)
     batch.step_io_async(f_host.data_ptr(), p_host.data_ptr(), q_host.data_ptr())  # stage buffers
     batch.restore(snap)  # back to the first timed step
     batch.synchronize()
