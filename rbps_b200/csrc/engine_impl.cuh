@@ -23,6 +23,7 @@
 #include "engine_types.cuh"
 #include "gjk.cuh"
 #include "team.cuh"
+#include <type_traits>
 
 namespace rbps_gpu
 {
@@ -69,7 +70,7 @@ namespace rbps_gpu
         Cand *cand;
         CandContacts<T, P> *cc;
         uint32_t *color;
-        unsigned long long *bmask, *bprio;
+        unsigned long long *bmask, *bprio, *claim;
         uint32_t *corder, *misc, *act, *alist;
     };
 
@@ -94,6 +95,7 @@ namespace rbps_gpu
         s.color = (uint32_t *)(base + L.color);
         s.bmask = (unsigned long long *)(base + L.bmask);
         s.bprio = (unsigned long long *)(base + L.bprio);
+        s.claim = (unsigned long long *)(base + L.claim);
         s.corder = (uint32_t *)(base + L.corder);
         s.misc = (uint32_t *)(base + L.misc);
         s.act = (uint32_t *)(base + L.act);
@@ -396,13 +398,23 @@ namespace rbps_gpu
         return n_sap + W.n_pc;
     }
 
-    // Jones-Plassmann colouring of the candidates that produced contact rows
-    // in this substep (the others have nothing to relax): a candidate takes
-    // the lowest colour free on both of its dynamic bodies once it holds the
-    // highest priority among the uncoloured candidates sharing them.
-    // Candidates whose bodies have used all 64 colours go to the serial
-    // colour; idle candidates get kColorIdle and are not bucketed.  Returns
-    // the number of regular colours; corder / colour offsets are filled.
+    // Colouring of the candidates that produced contact rows in this substep
+    // (the others have nothing to relax), in rounds:
+    // * up to kClaimBodiesMin bodies, Jones-Plassmann: a candidate takes the
+    //   lowest colour free on both of its dynamic bodies once it holds the
+    //   highest priority among the uncoloured candidates sharing them.  A
+    //   body gets at most one colour a round, so a body with d contacts takes
+    //   d rounds or more;
+    // * larger worlds, claims: every uncoloured candidate picks one colour
+    //   free on both bodies (hashed among the lowest few) and claims that
+    //   (body, colour) slot on each; the highest claim on both slots wins.
+    //   Many contacts of one body are coloured per round: on tangled chains
+    //   (contacts up to 53 per body) 8 rounds instead of more than 96.
+    // Both are deterministic (priorities are hashes of the candidate index).
+    // Candidates whose bodies have used all 64 colours, or still uncoloured
+    // after kMaxColorRounds, go to the serial colour; idle candidates get
+    // kColorIdle and are not bucketed.  Returns the number of regular
+    // colours; corder / colour offsets are filled.
     // Second-level colours for the overflow bucket [coff[64], coff[65]) of
     // corder: the team leader colours its candidates first-fit in order on
     // a second set of body masks (bprio, free after the Jones-Plassmann
@@ -498,6 +510,10 @@ namespace rbps_gpu
             S.bmask[b] = 0ull;
             S.bprio[b] = 0ull;
         }
+        const bool by_claim = W.n_bodies > kClaimBodiesMin;
+        if (by_claim)
+            for (uint32_t x = tm.rank(); x < W.n_bodies * 64u; x += tm.size())
+                S.claim[x] = 0ull;
         for (uint32_t x = tm.rank(); x < kMaxColorRounds + 2 * 66; x += tm.size())
             misc[kMiscCCount + x] = 0u;
         tm.sync();
@@ -511,7 +527,94 @@ namespace rbps_gpu
         tm.sync();
         const uint8_t *type = E.B.type + W.body_off;
         uint32_t round = 1;
-        for (; round <= kMaxColorRounds && n_act; ++round)
+        if (by_claim)
+        {
+            // uncoloured contacts per body (bprio's words reused as counters)
+            uint32_t *ucnt = (uint32_t *)S.bprio;
+            for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
+            {
+                const Cand cd = S.cand[S.alist[q]];
+                if (type[cd.ba] == kDynamic)
+                    atomicAdd(&ucnt[cd.ba], 1u);
+                if (type[cd.bb] == kDynamic)
+                    atomicAdd(&ucnt[cd.bb], 1u);
+            }
+            tm.sync();
+            for (; round <= kMaxColorRounds && n_act; ++round)
+            {
+                // each uncoloured candidate claims one colour free on both
+                // bodies, drawn from the lowest max(1, u / 2) free colours (u:
+                // the larger uncoloured count of its bodies), so a body's
+                // candidates spread over several colours in one round
+                for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
+                {
+                    const uint32_t c = S.alist[q];
+                    if (S.color[c] != 0xffffffffu)
+                        continue;
+                    const Cand cd = S.cand[c];
+                    const bool da = type[cd.ba] == kDynamic, db = type[cd.bb] == kDynamic;
+                    const unsigned long long used = (da ? S.bmask[cd.ba] : 0ull) | (db ? S.bmask[cd.bb] : 0ull);
+                    if (used == ~0ull)
+                    {
+                        S.color[c] = kColorSerial;
+                        continue;
+                    }
+                    unsigned long long f = ~used;
+                    const uint32_t u = max(da ? ucnt[cd.ba] : 1u, db ? ucnt[cd.bb] : 1u);
+                    const uint32_t span = min((uint32_t)__popcll(f), max(1u, u / 2u));
+                    for (uint32_t k = hash32(c * 0x9e3779b1u + round) % span; k; --k)
+                        f &= f - 1ull;
+                    const uint32_t col = (uint32_t)(__ffsll((long long)f) - 1);
+                    S.act[c] = col;
+                    const unsigned long long val = ((unsigned long long)round << 56) |
+                                                   ((unsigned long long)(hash32(c ^ (round << 24)) & 0xffffffu) << 32) | c;
+                    if (da)
+                        atomicMax(&S.claim[(size_t)cd.ba * 64u + col], val);
+                    if (db)
+                        atomicMax(&S.claim[(size_t)cd.bb * 64u + col], val);
+                }
+                tm.sync();
+                // the highest claim on each (body, colour) slot wins it
+                uint32_t lost = 0;
+                for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
+                {
+                    const uint32_t c = S.alist[q];
+                    if (S.color[c] != 0xffffffffu)
+                        continue;
+                    const Cand cd = S.cand[c];
+                    const bool da = type[cd.ba] == kDynamic, db = type[cd.bb] == kDynamic;
+                    const uint32_t col = S.act[c];
+                    const unsigned long long val = ((unsigned long long)round << 56) |
+                                                   ((unsigned long long)(hash32(c ^ (round << 24)) & 0xffffffu) << 32) | c;
+                    const bool won = (!da || S.claim[(size_t)cd.ba * 64u + col] == val) &&
+                                     (!db || S.claim[(size_t)cd.bb * 64u + col] == val);
+                    if (!won)
+                    {
+                        ++lost;
+                        continue;
+                    }
+                    S.color[c] = col;
+                    const unsigned long long bit = 1ull << col;
+                    if (da)
+                    {
+                        atomicOr(&S.bmask[cd.ba], bit);
+                        atomicSub(&ucnt[cd.ba], 1u);
+                    }
+                    if (db)
+                    {
+                        atomicOr(&S.bmask[cd.bb], bit);
+                        atomicSub(&ucnt[cd.bb], 1u);
+                    }
+                }
+                lost = __reduce_add_sync(0xffffffffu, lost);
+                if (lost && lane_id() == 0)
+                    atomicAdd(&misc[kMiscLeft + round - 1], lost);
+                tm.sync();
+                if (misc[kMiscLeft + round - 1] == 0u)
+                    break;
+            }
+        }
+        for (; !by_claim && round <= kMaxColorRounds && n_act; ++round)
         {
             for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
             {
@@ -923,6 +1026,45 @@ namespace rbps_gpu
     // then the velocity update (Body.cpp:41-57).  B is the body view the
     // team works on and boff the view index of the world's body 0
     // (W.body_off for the batch arrays, 0 for a shared-memory copy).
+    // Relaxes colours [0, n) of a colour-ordered slot list (offsets off),
+    // solve(q) per slot, with a team barrier after each colour.  On a grid
+    // team the trailing colours of at most one CTA's worth of slots each run
+    // on CTA 0 alone, separated by block barriers, and one grid barrier
+    // follows them: a colour's slots share no dynamic body, so which threads
+    // relax them does not change the result.  Tangled worlds end in dozens
+    // of such colours (a body with 60 contacts needs 60 colours, most of
+    // them nearly empty), and a grid barrier costs several block barriers.
+    template <class Team, class F>
+    __device__ __forceinline__ void sweep_colors(const Team &tm, const uint32_t *off, uint32_t n, F &&solve)
+    {
+        uint32_t tail = n;
+        if constexpr (std::is_same<Team, GridTeam>::value)
+            while (tail > 0 && off[tail] - off[tail - 1] <= blockDim.x)
+                --tail;
+        for (uint32_t col = 0; col < tail; ++col)
+        {
+            if (off[col + 1] == off[col])
+                continue;
+            for (uint32_t q = off[col] + tm.rank(); q < off[col + 1]; q += tm.size())
+                solve(q);
+            tm.sync();
+        }
+        if constexpr (std::is_same<Team, GridTeam>::value)
+            if (tail < n)
+            {
+                if (blockIdx.x == 0)
+                    for (uint32_t col = tail; col < n; ++col)
+                    {
+                        if (off[col + 1] == off[col])
+                            continue;
+                        for (uint32_t q = off[col] + threadIdx.x; q < off[col + 1]; q += blockDim.x)
+                            solve(q);
+                        __syncthreads();
+                    }
+                tm.sync();
+            }
+    }
+
     template <class T, class P, class Team>
     __device__ void phase_position_on(const Engine<T, P> &E, const Team &tm, uint32_t w, const Bodies<T, P> &B,
                                       uint32_t boff, const uint32_t *book = nullptr)
@@ -964,17 +1106,12 @@ namespace rbps_gpu
         {
             const uint32_t *coff = book ? book + 66 : S.misc + kMiscCOff;
             const uint32_t n_colors = book ? book[132] : S.misc[kMiscNColors];
-            for (uint32_t col = 0; col < n_colors; ++col)
-            {
-                for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
-                {
-                    const uint32_t c = S.corder[q];
-                    uint32_t ba, bb;
-                    slot_pair(S, book, q, c, ba, bb);
-                    solve_pair_position(B, E.inv_h, boff + ba, boff + bb, S.cc[c]);
-                }
-                tm.sync();
-            }
+            sweep_colors(tm, coff, n_colors, [&](uint32_t q) {
+                const uint32_t c = S.corder[q];
+                uint32_t ba, bb;
+                slot_pair(S, book, q, c, ba, bb);
+                solve_pair_position(B, E.inv_h, boff + ba, boff + bb, S.cc[c]);
+            });
             if (coff[kColorSerial + 1] > coff[kColorSerial])
             {
                 // the overflow bucket: second-level colours (global misc),
@@ -983,18 +1120,11 @@ namespace rbps_gpu
                 uint32_t serial0 = coff[kColorSerial];
                 if (!book)
                 {
-                    for (uint32_t col = 0; col < kColorSerial; ++col)
-                    {
-                        if (c2[col + 1] == c2[col])
-                            continue;
-                        for (uint32_t q = c2[col] + tm.rank(); q < c2[col + 1]; q += tm.size())
-                        {
-                            const uint32_t c = S.corder[q];
-                            const Cand cd = S.cand[c];
-                            solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
-                        }
-                        tm.sync();
-                    }
+                    sweep_colors(tm, c2, kColorSerial, [&](uint32_t q) {
+                        const uint32_t c = S.corder[q];
+                        const Cand cd = S.cand[c];
+                        solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                    });
                     serial0 = c2[kColorSerial];
                 }
                 if (tm.leader())
@@ -1078,35 +1208,23 @@ namespace rbps_gpu
         {
             const uint32_t *coff = book ? book + 66 : S.misc + kMiscCOff;
             const uint32_t n_colors = book ? book[132] : S.misc[kMiscNColors];
-            for (uint32_t col = 0; col < n_colors; ++col)
-            {
-                for (uint32_t q = coff[col] + tm.rank(); q < coff[col + 1]; q += tm.size())
-                {
-                    const uint32_t c = S.corder[q];
-                    uint32_t ba, bb;
-                    slot_pair(S, book, q, c, ba, bb);
-                    solve_pair_velocity(B, E.h, boff + ba, boff + bb, S.cc[c]);
-                }
-                tm.sync();
-            }
+            sweep_colors(tm, coff, n_colors, [&](uint32_t q) {
+                const uint32_t c = S.corder[q];
+                uint32_t ba, bb;
+                slot_pair(S, book, q, c, ba, bb);
+                solve_pair_velocity(B, E.h, boff + ba, boff + bb, S.cc[c]);
+            });
             if (coff[kColorSerial + 1] > coff[kColorSerial])
             {
                 const uint32_t *c2 = S.misc + kMiscC2Off;
                 uint32_t serial0 = coff[kColorSerial];
                 if (!book)
                 {
-                    for (uint32_t col = 0; col < kColorSerial; ++col)
-                    {
-                        if (c2[col + 1] == c2[col])
-                            continue;
-                        for (uint32_t q = c2[col] + tm.rank(); q < c2[col + 1]; q += tm.size())
-                        {
-                            const uint32_t c = S.corder[q];
-                            const Cand cd = S.cand[c];
-                            solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
-                        }
-                        tm.sync();
-                    }
+                    sweep_colors(tm, c2, kColorSerial, [&](uint32_t q) {
+                        const uint32_t c = S.corder[q];
+                        const Cand cd = S.cand[c];
+                        solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
+                    });
                     serial0 = c2[kColorSerial];
                 }
                 if (tm.leader())

@@ -65,6 +65,7 @@ namespace rbps_gpu
         size_t color;            // colour per candidate
         size_t bmask;            // per-body colour mask (u64)
         size_t bprio;            // per-body priority (u64)
+        size_t claim;            // per-(body, colour) claims (u64), worlds above kClaimBodiesMin only
         size_t corder;           // candidates sorted by colour
         size_t misc;             // small counters
         size_t act, alist;       // active-candidate flags / compacted list (colored mode)
@@ -84,6 +85,10 @@ namespace rbps_gpu
     constexpr uint32_t kColorStage = 256;  // candidates staged in shared memory per colouring chunk
     constexpr uint32_t kColorIdle = 65;    // candidate without contact rows this substep
     constexpr uint32_t kMaxColorRounds = 96;
+    // Worlds with more bodies colour by claims on (body, colour) slots, which
+    // colours many contacts of one body per round; smaller ones use
+    // Jones-Plassmann, which needs no claim table.
+    constexpr uint32_t kClaimBodiesMin = 4096;
     constexpr uint32_t kMiscWords = 64 + 4 * 66 + kMaxColorRounds + 8;
     // misc layout (u32 words)
     constexpr uint32_t kMiscFlags = 0;                  // [0..7] scalars
@@ -137,6 +142,7 @@ namespace rbps_gpu
         take(L.color, nc * 4);
         take(L.bmask, (size_t)nb * 8 + 8);
         take(L.bprio, (size_t)nb * 8 + 8);
+        take(L.claim, nb > kClaimBodiesMin ? (size_t)nb * 64 * 8 : 8);
         take(L.corder, nc * 4);
         take(L.misc, kMiscWords * 4);
         take(L.act, nc * 4);

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from rbps_b200 import abi, scenes
-from helpers import load_golden, state_err
+from helpers import bit_equal, load_golden, state_err
 
 pytestmark = pytest.mark.gpu
 
@@ -78,3 +78,34 @@ def test_batches_of_different_sizes_coexist(rbps):
     big.step(2)
     for b in (big, small):
         assert np.isfinite(b.state_all()["position"]).all()
+
+
+def test_large_world_colouring(rbps):
+    """Worlds above 4,096 bodies colour by claims on (body, colour) slots,
+    many contacts of one body per round.  Tangled chains (scenes.config2,
+    196 chains of 32 capsules: 6,468 bodies, up to 25 contacts per body by
+    step 28): the colouring is valid, nothing is left to the serial bucket,
+    the colour count lies between the largest body degree (a lower bound)
+    and twice it, and two batches stepped from the same scene agree bit for
+    bit (the colouring is deterministic, and so is relaxing the trailing
+    small colours on one CTA)."""
+    sc = scenes.config2(seed=0, n_chains=196, n_links=32)
+    dyn = sc.worlds[0].bodies["type"] == abi.BODY_DYNAMIC
+    runs = []
+    for _ in range(2):
+        b = rbps.Batch.from_scene(sc, abi.PRECISION_FP32, abi.SOLVE_COLORED, max_pairs_per_world=1 << 20)
+        b.set_dump(True)
+        b.step(28)
+        col, ba, bb = b.colors(0)
+        st = b.stats()
+        runs.append((b.state(0), col))
+    assert colour_valid(col, ba, bb, dyn)
+    act = col < 64
+    a, c = ba[act], bb[act]
+    deg = np.bincount(np.concatenate([a[dyn[a]], c[dyn[c]]]))
+    assert deg.max() >= 12, deg.max()  # tangled enough to need many colours
+    assert st["serial_overflow"] == 0, st
+    ncol = int(col[act].max()) + 1
+    assert deg.max() <= ncol <= 2 * deg.max(), (ncol, deg.max())
+    assert bit_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
