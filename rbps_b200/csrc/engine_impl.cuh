@@ -1031,38 +1031,37 @@ namespace rbps_gpu
     // team the trailing colours of at most one CTA's worth of slots each run
     // on CTA 0 alone, separated by block barriers, and one grid barrier
     // follows them: a colour's slots share no dynamic body, so which threads
-    // relax them does not change the result.  Tangled worlds end in dozens
-    // of such colours (a body with 60 contacts needs 60 colours, most of
-    // them nearly empty), and a grid barrier costs several block barriers.
+    // relax them does not change the result.  solve has one call site, so
+    // the same machine code (and FP32 contraction) relaxes a slot either way.
+    // Tangled worlds end in dozens of such colours (a body with 60 contacts
+    // needs 60 colours, most of them nearly empty), and a grid barrier costs
+    // several block barriers.
     template <class Team, class F>
     __device__ __forceinline__ void sweep_colors(const Team &tm, const uint32_t *off, uint32_t n, F &&solve)
     {
+        constexpr bool kGrid = std::is_same<Team, GridTeam>::value;
         uint32_t tail = n;
-        if constexpr (std::is_same<Team, GridTeam>::value)
+        if constexpr (kGrid)
             while (tail > 0 && off[tail] - off[tail - 1] <= blockDim.x)
                 --tail;
-        for (uint32_t col = 0; col < tail; ++col)
+        for (uint32_t col = 0; col < n; ++col)
         {
             if (off[col + 1] == off[col])
                 continue;
-            for (uint32_t q = off[col] + tm.rank(); q < off[col + 1]; q += tm.size())
-                solve(q);
-            tm.sync();
-        }
-        if constexpr (std::is_same<Team, GridTeam>::value)
-            if (tail < n)
+            const bool on_cta = kGrid && col >= tail; // uniform over the team
+            if (!on_cta || blockIdx.x == 0)
             {
-                if (blockIdx.x == 0)
-                    for (uint32_t col = tail; col < n; ++col)
-                    {
-                        if (off[col + 1] == off[col])
-                            continue;
-                        for (uint32_t q = off[col] + threadIdx.x; q < off[col + 1]; q += blockDim.x)
-                            solve(q);
-                        __syncthreads();
-                    }
-                tm.sync();
+                const uint32_t r = on_cta ? threadIdx.x : tm.rank(), step = on_cta ? blockDim.x : tm.size();
+                for (uint32_t q = off[col] + r; q < off[col + 1]; q += step)
+                    solve(q);
             }
+            if (on_cta)
+                __syncthreads();
+            else
+                tm.sync();
+        }
+        if (kGrid && tail < n)
+            tm.sync();
     }
 
     template <class T, class P, class Team>
