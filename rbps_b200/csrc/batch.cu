@@ -913,7 +913,7 @@ namespace
         p[0] = T(x); p[1] = T(y); p[2] = T(z); p[3] = T(w);
     }
 
-    constexpr uint32_t kSmallWorldBodies = 4096;
+    constexpr uint32_t kSmallWorldBodies = kGridWorldBodies; // larger worlds step on the cooperative grid
     constexpr int kMaxBlockHost = 256; // block of the flat kernels (their __launch_bounds__)
     constexpr uint32_t kBlockTeamBodies = 128; // colored batches: worlds this large step on a whole CTA
     constexpr uint32_t kSmemBodiesMax = 1024;   // bodies a CTA world keeps in shared memory (137 KB in FP32)

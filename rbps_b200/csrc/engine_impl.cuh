@@ -72,6 +72,7 @@ namespace rbps_gpu
         uint32_t *color;
         unsigned long long *bmask, *bprio, *claim;
         uint32_t *corder, *misc, *act, *alist;
+        float4 *yz;
     };
 
     template <class T, class P>
@@ -96,6 +97,7 @@ namespace rbps_gpu
         s.bmask = (unsigned long long *)(base + L.bmask);
         s.bprio = (unsigned long long *)(base + L.bprio);
         s.claim = (unsigned long long *)(base + L.claim);
+        s.yz = (float4 *)(base + L.yz);
         s.corder = (uint32_t *)(base + L.corder);
         s.misc = (uint32_t *)(base + L.misc);
         s.act = (uint32_t *)(base + L.act);
@@ -144,6 +146,13 @@ namespace rbps_gpu
                (a.mn[2] <= b.mx[2] && a.mx[2] >= b.mn[2]);
     }
 
+    // The y / z part of fat_overlap on float copies rounded outward
+    // (mn down, mx up): false only where fat_overlap is false too.
+    __device__ __forceinline__ bool yz_may_overlap(const float4 &a, const float4 &b)
+    {
+        return a.x <= b.y && a.y >= b.x && a.z <= b.w && a.w >= b.z;
+    }
+
     // ------------------------------------------------------------ broadphase
     // Sort + sweep of one SAP state (BroadPhase.cpp:80-152).  On return
     // S.pk / S.pv hold the pairs in the reference emission order (pv indexes
@@ -153,7 +162,8 @@ namespace rbps_gpu
     template <class Team, class SC>
     __device__ __noinline__ uint32_t sap_sort_sweep(const Team &tm, const FatBox *fat, uint32_t *ep_key, uint32_t *ep_id,
                                        uint32_t *ep_pos, uint32_t nbp, uint32_t id_limit, uint32_t pair_cap,
-                                       int *error, const SC &S, BlockShared &sh, uint32_t *sort_smem = nullptr)
+                                       int *error, const SC &S, BlockShared &sh, uint32_t *sort_smem = nullptr,
+                                       float4 *yz = nullptr)
     {
         const uint32_t nep = 2 * nbp;
         // stable sort of the endpoints, previous order as the tie-break
@@ -169,6 +179,18 @@ namespace rbps_gpu
             if (i + 1 < nep && ep_key[i] > ep_key[i + 1])
                 set_error_at(error, kErrInternal, 4, i); // the endpoint sort must leave the keys ordered
         }
+        // A grid team's sweep reads every object of an overlap run; most fail
+        // on y or z.  With yz, it first tests 16-byte float extents rounded
+        // outward and reads the 48-byte double box only where they overlap,
+        // so the pairs are exactly those of fat_overlap.
+        const bool pre = tm.ncta() > 1 && yz != nullptr;
+        if (pre)
+            for (uint32_t o = tm.rank(); o < nbp; o += tm.size())
+            {
+                const FatBox f = fat[o];
+                yz[o] = make_float4(__double2float_rd(f.mn[1]), __double2float_ru(f.mx[1]),
+                                    __double2float_rd(f.mn[2]), __double2float_ru(f.mx[2]));
+            }
         tm.sync();
         // count the pairs each opening endpoint emits.  A team spread over
         // the cooperative grid (one large world) gives each opening endpoint
@@ -186,6 +208,7 @@ namespace rbps_gpu
                 if (!(id & 1u) && id < id_limit)
                 {
                     const FatBox fa = fat[id >> 1];
+                    const float4 fq = pre ? yz[id >> 1] : float4{};
                     const uint32_t end = min(ep_pos[id + 1], nep);
                     for (uint32_t j0 = i + 1; j0 < end; j0 += 32)
                     {
@@ -194,7 +217,8 @@ namespace rbps_gpu
                         if (j < end)
                         {
                             const uint32_t id2 = ep_id[j];
-                            hit = !(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]);
+                            hit = !(id2 & 1u) && id2 < id_limit && (!pre || yz_may_overlap(fq, yz[id2 >> 1])) &&
+                                  fat_overlap(fa, fat[id2 >> 1]);
                         }
                         c += __popc(__ballot_sync(0xffffffffu, hit));
                     }
@@ -241,6 +265,7 @@ namespace rbps_gpu
                     continue;
                 uint32_t k = S.cnt[i];
                 const FatBox fa = fat[id >> 1];
+                const float4 fq = pre ? yz[id >> 1] : float4{};
                 const uint32_t end = min(ep_pos[id + 1], nep);
                 for (uint32_t j0 = i + 1; j0 < end && k < total; j0 += 32)
                 {
@@ -250,7 +275,8 @@ namespace rbps_gpu
                     if (j < end)
                     {
                         id2 = ep_id[j];
-                        hit = !(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]);
+                        hit = !(id2 & 1u) && id2 < id_limit && (!pre || yz_may_overlap(fq, yz[id2 >> 1])) &&
+                              fat_overlap(fa, fat[id2 >> 1]);
                     }
                     const uint32_t m = __ballot_sync(0xffffffffu, hit);
                     const uint32_t kk = k + __popc(m & ((1u << lane) - 1u));
@@ -340,7 +366,8 @@ namespace rbps_gpu
             ep_key[ep_pos[2 * o + 1]] = order_key(__double2float_rn(f1.mx.x));
         }
         tm.sync();
-        return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, 2 * nbp, W.pair_cap, E.error, S, sh, sort_smem);
+        return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, 2 * nbp, W.pair_cap, E.error, S, sh, sort_smem,
+                              W.n_bodies > kGridWorldBodies ? S.yz : nullptr);
     }
 
     // Filtered SAP pairs followed by the plane candidates; returns the count.
@@ -400,7 +427,7 @@ namespace rbps_gpu
 
     // Colouring of the candidates that produced contact rows in this substep
     // (the others have nothing to relax), in rounds:
-    // * up to kClaimBodiesMin bodies, Jones-Plassmann: a candidate takes the
+    // * up to kGridWorldBodies bodies, Jones-Plassmann: a candidate takes the
     //   lowest colour free on both of its dynamic bodies once it holds the
     //   highest priority among the uncoloured candidates sharing them.  A
     //   body gets at most one colour a round, so a body with d contacts takes
@@ -510,7 +537,7 @@ namespace rbps_gpu
             S.bmask[b] = 0ull;
             S.bprio[b] = 0ull;
         }
-        const bool by_claim = W.n_bodies > kClaimBodiesMin;
+        const bool by_claim = W.n_bodies > kGridWorldBodies;
         if (by_claim)
             for (uint32_t x = tm.rank(); x < W.n_bodies * 64u; x += tm.size())
                 S.claim[x] = 0ull;

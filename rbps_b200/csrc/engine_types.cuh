@@ -65,7 +65,8 @@ namespace rbps_gpu
         size_t color;            // colour per candidate
         size_t bmask;            // per-body colour mask (u64)
         size_t bprio;            // per-body priority (u64)
-        size_t claim;            // per-(body, colour) claims (u64), worlds above kClaimBodiesMin only
+        size_t claim;            // per-(body, colour) claims (u64), grid worlds only
+        size_t yz;               // float y / z extents per SAP object (float4), grid worlds only
         size_t corder;           // candidates sorted by colour
         size_t misc;             // small counters
         size_t act, alist;       // active-candidate flags / compacted list (colored mode)
@@ -85,10 +86,11 @@ namespace rbps_gpu
     constexpr uint32_t kColorStage = 256;  // candidates staged in shared memory per colouring chunk
     constexpr uint32_t kColorIdle = 65;    // candidate without contact rows this substep
     constexpr uint32_t kMaxColorRounds = 96;
-    // Worlds with more bodies colour by claims on (body, colour) slots, which
-    // colours many contacts of one body per round; smaller ones use
-    // Jones-Plassmann, which needs no claim table.
-    constexpr uint32_t kClaimBodiesMin = 4096;
+    // Worlds with more bodies step on the whole cooperative grid.  They
+    // colour by claims on (body, colour) slots, which colours many contacts
+    // of one body per round (smaller ones use Jones-Plassmann, which needs no
+    // claim table), and their SAP sweep prefilters on float y / z extents.
+    constexpr uint32_t kGridWorldBodies = 4096;
     constexpr uint32_t kMiscWords = 64 + 4 * 66 + kMaxColorRounds + 8;
     // misc layout (u32 words)
     constexpr uint32_t kMiscFlags = 0;                  // [0..7] scalars
@@ -142,7 +144,8 @@ namespace rbps_gpu
         take(L.color, nc * 4);
         take(L.bmask, (size_t)nb * 8 + 8);
         take(L.bprio, (size_t)nb * 8 + 8);
-        take(L.claim, nb > kClaimBodiesMin ? (size_t)nb * 64 * 8 : 8);
+        take(L.claim, nb > kGridWorldBodies ? (size_t)nb * 64 * 8 : 8);
+        take(L.yz, nb > kGridWorldBodies ? (size_t)nbp * 16 : 16);
         take(L.corder, nc * 4);
         take(L.misc, kMiscWords * 4);
         take(L.act, nc * 4);
