@@ -1067,6 +1067,18 @@ namespace rbps_gpu
     __device__ __forceinline__ void sweep_colors(const Team &tm, const uint32_t *off, uint32_t n, F &&solve)
     {
         constexpr bool kGrid = std::is_same<Team, GridTeam>::value;
+        if constexpr (!kGrid)
+        {
+            // one CTA or one warp: every colour behind a team barrier (the
+            // skip test for empty colours measured 0.4 % slower here)
+            for (uint32_t col = 0; col < n; ++col)
+            {
+                for (uint32_t q = off[col] + tm.rank(); q < off[col + 1]; q += tm.size())
+                    solve(q);
+                tm.sync();
+            }
+            return;
+        }
         uint32_t tail = n;
         if constexpr (kGrid)
             while (tail > 0 && off[tail] - off[tail - 1] <= blockDim.x)
