@@ -307,6 +307,14 @@ RBPS_API int rbps_batch_commit(rbps_batch *batch);
 RBPS_API int rbps_batch_step(rbps_batch *batch, int32_t n_steps);
 /* Waits for every step and copy enqueued on the batch (both its streams). */
 RBPS_API int rbps_batch_synchronize(rbps_batch *batch);
+/* Failure detection, on by default: at the end of every step each world's
+ * bodies are checked for a non-finite position, orientation or velocity,
+ * and the next rbps_batch_synchronize / get_* call returns RBPS_ERR_STATE
+ * naming the first such world (the error is then cleared; the world keeps
+ * its state until rbps_batch_set_state or rbps_batch_restore replaces it).
+ * The reference has no such check (a NaN just propagates through
+ * World::step), so enable = 0 restores its behaviour exactly. */
+RBPS_API int rbps_batch_set_state_check(rbps_batch *batch, int32_t enable);
 /* One World::step of every world with host I/O, for callers that feed
  * forces and read poses every frame: copies force_in (3 doubles per body,
  * all worlds in world order; NULL keeps the current forces) host -> device,
@@ -458,14 +466,18 @@ RBPS_API int rbps_bp_configure(rbps_bp *bp, int32_t single_cta, int32_t block_th
  *   fat_aabbs : device, 6 doubles per object {min.xyz, max.xyz}
  *   user_ids  : device, 1 per object
  *   pairs     : device, 2 * pair_cap; (id_a, id_b), id_a < id_b, in the
- *               reference emission order
+ *               reference emission order; the first min(pair count,
+ *               pair_cap) pairs are written
  *   n_pairs   : device, receives the pair count (may exceed pair_cap), or
- *               0xFFFFFFFF when more than 65,536 pairs were found
- * At most 8,192 objects (larger counts return RBPS_ERR_INVALID).  Runs
- * asynchronously on `stream`.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
- * Calls share the array: calls that overlap on the GPU race, so order them
- * on one stream. */
+ *               0xFFFFFFFF when more than 65,536 pairs were found, or
+ *               0xFFFFFFFE when an internal consistency check of the sort
+ *               failed; with either value `pairs` is left unwritten
+ * At most 8,192 objects (larger counts return RBPS_ERR_INVALID); zero
+ * objects give zero pairs.  Runs asynchronously on `stream`.  The first call
+ * on a device looks up the array's device address; make that first call
+ * before any stream capture, and do not call it again on a device after a
+ * cudaDeviceReset of that device (the array may move).  Calls share the
+ * array: calls that overlap on the GPU race, so order them on one stream. */
 RBPS_API int rbps_sap_pairs_static(const double *fat_aabbs, const uint32_t *user_ids, uint32_t n_objects,
                                    uint32_t *pairs, uint32_t pair_cap, uint32_t *n_pairs, void *stream);
 

@@ -95,6 +95,7 @@ def lib():
             "rbps_batch_commit": (i, [_P]),
             "rbps_batch_step": (i, [_P, C.c_int32]),
             "rbps_batch_synchronize": (i, [_P]),
+            "rbps_batch_set_state_check": (i, [_P, C.c_int32]),
             "rbps_batch_get_state": (i, [_P, C.c_uint32, C.POINTER(StateView)]),
             "rbps_batch_set_state": (i, [_P, C.c_uint32, C.POINTER(StateView)]),
             "rbps_batch_get_state_all": (i, [_P, C.POINTER(StateView)]),
@@ -307,6 +308,12 @@ class Batch:
 
     def synchronize(self):
         _check(lib().rbps_batch_synchronize(self.h))
+
+    def set_state_check(self, on=True):
+        """Failure detection (on by default): a non-finite body state makes
+        the next synchronising call raise RbpsError(ERR_STATE).  Off
+        reproduces the reference, which lets a NaN propagate."""
+        _check(lib().rbps_batch_set_state_check(self.h, 1 if on else 0))
 
     def step_io(self, force_ptr, pos_ptr, rot_ptr):
         """One step with host I/O through raw host pointers (ints or None)."""

@@ -333,6 +333,7 @@ struct rbps_batch
     float *hm_heights = nullptr;
     HmDesc *hm_desc = nullptr;
     bool committed = false;
+    bool check_state = true; // rbps_batch_set_state_check
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 0;
@@ -864,6 +865,7 @@ namespace
         e.reinsert_threshold = b->desc.reinsert_threshold;
         e.solve_mode = b->desc.solve_mode;
         e.use_vel_exp = b->desc.use_velocity_expansion;
+        e.check_state = b->check_state ? 1 : 0;
         e.work_counter = b->work_counter;
         e.scratch = b->scratch;
         e.wcoff = b->wcoff;
@@ -1679,7 +1681,7 @@ template <class T, class P>
 static int step_typed(rbps_batch *b, int n)
 {
     Engine<T, P> e = make_engine<T, P>(b);
-    const int key = (b->dump ? 1 : 0) | (e.prof ? 2 : 0);
+    const int key = (b->dump ? 1 : 0) | (e.prof ? 2 : 0) | (e.check_state ? 4 : 0);
     if (b->graph_ok && n > 0 && (!b->graph_exec || b->graph_key != key))
         capture_step<T, P>(b, e, key);
     uint64_t launches = 0;
@@ -1730,12 +1732,29 @@ static int check_device_error(rbps_batch *b)
         CU(cudaDeviceSynchronize());
         static const char *sites[] = {"", "endpoint id out of range", "corrupt SAP pair record",
                                       "narrowphase candidate out of range", "endpoint keys not ordered after sort",
-                                      "pair keys not ordered after sort"};
-        const int site = (err[1] > 0 && err[1] < 6) ? err[1] : 0;
+                                      "pair keys not ordered after sort", "GJK queue full",
+                                      "non-finite body state"};
+        const int site = (err[1] > 0 && err[1] < 8) ? err[1] : 0;
+        if (err[0] == RBPS_ERR_STATE)
+            return fail(err[0], "device reported error %d (non-finite body position, orientation or velocity in "
+                                "world %d)", err[0], err[2]);
         return fail(err[0], "device reported error %d (%s%s%s, value %d)", err[0],
-                    err[0] == RBPS_ERR_CAPACITY ? "pair capacity exceeded: raise max_pairs_per_world" : "step failure",
+                    err[0] == RBPS_ERR_CAPACITY ? "capacity exceeded: raise max_pairs_per_world" : "step failure",
                     site ? ": " : "", sites[site], err[2]);
     }
+    return RBPS_OK;
+}
+
+extern "C" int rbps_batch_set_state_check(rbps_batch *b, int32_t enable)
+{
+    if (!b)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_set_state_check: null batch");
+    if (b->committed)
+    {
+        CU(cudaSetDevice(b->desc.device));
+        CU(cudaStreamSynchronize(b->stream));
+    }
+    b->check_state = enable != 0;
     return RBPS_OK;
 }
 

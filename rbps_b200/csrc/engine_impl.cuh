@@ -36,6 +36,7 @@ namespace rbps_gpu
     }
 
     constexpr int kErrInternal = -6;
+    constexpr int kErrState = -5; // RBPS_ERR_STATE
 
     __device__ __forceinline__ void set_error(int *err, int code)
     {
@@ -1323,6 +1324,24 @@ namespace rbps_gpu
         }
         if (local)
             atomicAdd(ncon, local);
+        if (E.check_state)
+        {
+            // failure detection: a non-finite pose or velocity anywhere in
+            // the world is reported with the world index (the reference has
+            // no such check; its state just propagates the NaN)
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            {
+                const uint32_t g = W.body_off + b;
+                const V4<P> x = E.B.pos[g];
+                const Q4<T> q = E.B.rot[g];
+                const V4<T> v = E.B.lin[g], om = E.B.ang[g];
+                const bool ok = isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(q.w) && isfinite(q.x) &&
+                                isfinite(q.y) && isfinite(q.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) &&
+                                isfinite(om.x) && isfinite(om.y) && isfinite(om.z);
+                if (!ok)
+                    set_error_at(E.error, kErrState, 7, w);
+            }
+        }
         tm.sync();
         if (tm.leader())
         {

@@ -211,6 +211,7 @@ namespace rbps_gpu
         double fat_margin, reinsert_threshold;
         int solve_mode;
         int use_vel_exp;
+        int check_state; // the stats phase reports a non-finite body state (RBPS_ERR_STATE)
         // executors
         char *scratch;            // per-world slices at WorldDev::scr_off
         uint32_t *work_counter;

@@ -30,6 +30,10 @@ namespace
     constexpr uint32_t kStaticMaxObjects = 8192;
     constexpr uint32_t kStaticMaxPairs = 65536;
     constexpr uint32_t kStaticBlock = 256;
+    // *n_pairs sentinels: more pairs than kStaticMaxPairs, and a failed
+    // internal consistency check of the sort (endpoint ids or key order)
+    constexpr uint32_t kStaticOverflow = 0xFFFFFFFFu;
+    constexpr uint32_t kStaticCheckFailed = 0xFFFFFFFEu;
     constexpr uint32_t kNep = 2 * kStaticMaxObjects + 1;
     constexpr uint32_t kPc = kStaticMaxPairs + 1;
     constexpr uint32_t kTiles = ((kNep > kPc ? kNep : kPc) + kStaticBlock - 1) / kStaticBlock + 1;
@@ -65,8 +69,9 @@ namespace
 
     // fat: 6 doubles per object {min.x,min.y,min.z,max.x,max.y,max.z};
     // user_ids: 1 per object; pairs: (id_a, id_b) with id_a < id_b in the
-    // reference emission order; *n_pairs = pairs found, or ~0u when they
-    // exceeded kStaticMaxPairs.
+    // reference emission order; *n_pairs = pairs found, kStaticOverflow when
+    // they exceeded kStaticMaxPairs, kStaticCheckFailed when a consistency
+    // check of the sort failed.
     __global__ void __launch_bounds__(kStaticBlock) k_sap_static(uint32_t *scratch, const double *fat_in,
                                                                  const uint32_t *user_ids, uint32_t n,
                                                                  uint32_t *pairs, uint32_t pair_cap,
@@ -94,19 +99,28 @@ namespace
                     scratch + oPrA, scratch + oPrB, scratch + oPk, scratch + oPv, scratch + oPk2,
                     scratch + oPv2, scratch + oMisc};
         const uint32_t total = sap_sort_sweep(tm, fat, key, id, pos, n, 2 * n, kStaticMaxPairs, err, S, sh);
-        const bool overflow = *err != 0;
-        for (uint32_t k = threadIdx.x; k < total && k < pair_cap; k += blockDim.x)
-        {
-            const uint32_t r = S.pv[k];
-            const uint32_t ua = user_ids[S.pr_a[r]], ub = user_ids[S.pr_b[r]];
-            pairs[2 * k] = ua < ub ? ua : ub;
-            pairs[2 * k + 1] = ua < ub ? ub : ua;
-        }
+        // sap_sort_sweep ends with a block barrier, so every thread reads the
+        // same error word here.  On any error the pairs buffer is left as it
+        // was: the pairs kept before an overflow are neither a prefix of the
+        // emission order nor complete.
+        const int e = *err;
+        if (e == 0)
+            for (uint32_t k = threadIdx.x; k < total && k < pair_cap; k += blockDim.x)
+            {
+                const uint32_t r = S.pv[k];
+                const uint32_t ua = user_ids[S.pr_a[r]], ub = user_ids[S.pr_b[r]];
+                pairs[2 * k] = ua < ub ? ua : ub;
+                pairs[2 * k + 1] = ua < ub ? ub : ua;
+            }
         if (threadIdx.x == 0)
-            *n_pairs = overflow ? ~0u : total;
+            *n_pairs = e == 0 ? total : e == RBPS_ERR_CAPACITY ? kStaticOverflow : kStaticCheckFailed;
     }
 
-    // Device address of g_sap_scratch, looked up once per device.
+    // Device address of g_sap_scratch, looked up once per device.  A
+    // cudaDeviceReset unloads the module, and the array may come back at
+    // another address: the cached address is then stale, so the entry point
+    // must not be called on a device after a reset of that device in the
+    // same process.
     constexpr int kMaxDevices = 64;
     uint32_t *g_scratch_ptr[kMaxDevices] = {};
     std::mutex g_setup_mutex;

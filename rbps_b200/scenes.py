@@ -443,10 +443,11 @@ def config2(seed=0, n_chains=1024, n_links=32, steps=300, radius=0.05, half_heig
                  f"{n_chains} chains x {n_links} capsules, ball joints with a {cone_deg:g} deg cone, seed {seed}")
 
 
-def config3(seed=0, n_worlds=4096, steps=1000, lo_bodies=8, hi_bodies=512):
+def config3(seed=0, n_worlds=4096, steps=1000, lo_bodies=8, hi_bodies=512, chain=True):
     """Batched uneven worlds: per world n ~ log-uniform[8,512] boxes/spheres
     (as config0) + one 13-link revolute capsule chain + ground plane,
-    dt=1/120, 4 substeps."""
+    dt=1/120, 4 substeps.  chain=False leaves the chains out and keeps every
+    other draw (the same boxes and spheres)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     counts = np.floor(np.exp(rng.uniform(math.log(lo_bodies), math.log(hi_bodies + 1), n_worlds))).astype(int)
     counts = np.clip(counts, lo_bodies, hi_bodies)
@@ -455,7 +456,8 @@ def config3(seed=0, n_worlds=4096, steps=1000, lo_bodies=8, hi_bodies=512):
         bodies, forces, colliders = box_sphere_world(rng, int(counts[w]))
         joints = []
         origin = (rng.uniform(-4.5, -3.5), rng.uniform(1.0, 21.0), rng.uniform(-5.0, 5.0))
-        capsule_chain(bodies, forces, colliders, joints, origin)
+        if chain:
+            capsule_chain(bodies, forces, colliders, joints, origin)
         worlds.append(_finish(bodies, forces, colliders, joints))
     return Scene("config3_batched_fp32", 1.0 / 120.0, 4, steps, worlds,
                  f"{n_worlds} worlds, bodies log-uniform[{lo_bodies},{hi_bodies}] + 13-link chain, seed {seed}")
@@ -734,3 +736,70 @@ def hull_world(seed=0, n=24, n_shapes=4, friction=0.5, restitution=0.0):
         forces.append(f)
         colliders.append(c)
     return _finish(bodies, forces, colliders, [], hulls)
+
+
+def with_state(scene, states, worlds=None):
+    """The same worlds restarted from given states: a new Scene whose bodies
+    start at `states[k]` (dicts with position, orientation, linear_velocity,
+    angular_velocity per body, as Batch.state returns) for world
+    `worlds[k]` (default: the first len(states) worlds).  Colliders, joints,
+    forces and hulls are shared; joint and contact multipliers start from
+    zero, as at any commit."""
+    idx = list(range(len(states))) if worlds is None else list(worlds)
+    out = []
+    for k, st in zip(idx, states):
+        w = scene.worlds[k]
+        b = w.bodies.copy()
+        for f in ("position", "orientation", "linear_velocity", "angular_velocity"):
+            b[f] = np.asarray(st[f], np.float64)
+        out.append(WorldSpec(b, w.forces, w.colliders, w.joints, w.hulls,
+                             getattr(w, "heightmaps", []), getattr(w, "meshes", [])))
+    return Scene(scene.name, scene.timestep, scene.substeps, scene.steps, out, scene.description)
+
+
+def config3_separated(seed=0, n_worlds=256, steps=1000, lo_bodies=8, hi_bodies=512):
+    """config3's worlds (same shape, size and count distributions, the same
+    13-link chain per world) with no two bodies' bounding spheres
+    overlapping at the start and every body clear of the ground: each body's
+    position is redrawn until its bounding sphere (box: |half-extents|,
+    sphere: radius, chain link: half-height + radius) is clear of every body
+    placed before it.  At rest; the first step is free fall plus the chain
+    joints."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    counts = np.floor(np.exp(rng.uniform(math.log(lo_bodies), math.log(hi_bodies + 1), n_worlds))).astype(int)
+    counts = np.clip(counts, lo_bodies, hi_bodies)
+    worlds = []
+    for w in range(n_worlds):
+        bodies, forces, colliders = box_sphere_world(rng, int(counts[w]))
+        joints = []
+        origin = (rng.uniform(-4.5, -3.5), rng.uniform(2.0, 21.0), rng.uniform(-5.0, 5.0))
+        capsule_chain(bodies, forces, colliders, joints, origin)
+        B = np.array(bodies, dtype=abi.BODY_DT)
+        Cl = np.array(colliders, dtype=abi.COLLIDER_DT)
+        rad = np.zeros(len(B))
+        for c in Cl:
+            p = c["params"]
+            if c["shape"] == abi.SHAPE_BOX:
+                rad[c["body_id"]] = float(np.linalg.norm(p[:3]))
+            elif c["shape"] == abi.SHAPE_SPHERE:
+                rad[c["body_id"]] = float(p[0])
+            elif c["shape"] == abi.SHAPE_CAPSULE:
+                rad[c["body_id"]] = float(p[0] + p[1])
+        dyn = np.nonzero(B["type"] == abi.BODY_DYNAMIC)[0]
+        chain = dyn[-13:]
+        P = np.zeros((len(B), 3))
+        R = np.zeros(len(B))
+        P[:13], R[:13] = B["position"][chain], rad[chain]
+        n_placed = 13
+        for i in dyn[:-13]:
+            for _ in range(10000):
+                p = B["position"][i]
+                gap = np.linalg.norm(P[:n_placed] - p, axis=1) - R[:n_placed]
+                if p[1] - rad[i] > 0.05 and (gap > rad[i]).all():
+                    break
+                B["position"][i] = rng.uniform((-5.0, 1.0, -5.0), (5.0, 21.0, 5.0))
+            P[n_placed], R[n_placed] = B["position"][i], rad[i]
+            n_placed += 1
+        worlds.append(_finish(list(B), forces, list(Cl), joints))
+    return Scene("config3_separated", 1.0 / 120.0, 4, steps, worlds,
+                 f"{n_worlds} config-3 worlds without initial overlap, seed {seed}")

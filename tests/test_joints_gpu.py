@@ -160,6 +160,7 @@ def test_joint_world_matches_reference(rbps, ref, name):
     spec = _world(links, joints)
     sc = scenes.Scene(name, DT, SUB, STEPS, [spec])
     b = rbps.Batch.from_scene(sc, abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER)
+    b.set_state_check(False)  # some cases reproduce the reference's own NaN trap below
     w = ref.RefWorld(spec, DT, SUB)
     moved = 0.0
     x0 = spec.bodies["position"].copy()
