@@ -5,8 +5,9 @@ Workload: 4,096 independent worlds, bodies per world log-uniform in [8,512]
 (random boxes and spheres, sizes U[0.2,0.5] m) plus one 13-link revolute
 capsule chain per world, over a ground plane; dt = 1/120 s, 4 substeps, FP32
 state, graph-coloured Gauss-Seidel; all worlds step in one launch per step.
-Seeded synthetic scene (rbps_b200.scenes.config3); under torchrun every rank
-steps its own 4,096 worlds (weak scaling, no collective on the step path).
+Seeded synthetic scene (rbps_b200.scenes.config3); under torchrun the N
+ranks split one set of 4,096 x N worlds by balanced body count
+(rbps_b200.shard: weak scaling, no collective on the step path).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rbps|reference]
 
@@ -37,6 +38,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -86,8 +88,8 @@ def reduce_over_ranks(x, op, ws):
 
 
 def rank_seed(seed, rank):
-    """Each rank steps its own scene (weak scaling): same distribution,
-    independent draw."""
+    """Single-world workloads do not shard: each rank steps its own replica
+    (same distribution, independent draw)."""
     return seed + rank
 
 
@@ -112,7 +114,8 @@ class ClockSampler:
 
     def start(self):
         try:
-            self.out = open(os.path.join(ROOT, ".clocks_tmp.csv"), "w")
+            fd, self.path = tempfile.mkstemp(prefix="rbps_clocks_", suffix=".csv")
+            self.out = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
@@ -124,7 +127,7 @@ class ClockSampler:
         self.proc.terminate()
         self.proc.wait()
         self.out.close()
-        path = os.path.join(ROOT, ".clocks_tmp.csv")
+        path = self.path
         rows = []
         with open(path) as f:
             for line in f:
@@ -222,41 +225,122 @@ def plain_gpu_run(scene, batch, n_sample, steps, warmup, stream):
                    f"FP32 colored, {warmup} untimed + {steps} timed steps from the batched state")
 
 
-def one_step_error(scene, n_worlds, stream):
-    """Per-world one-step state error of FP32 against the FP64
-    reference-order engine (the device engine that matches the oracle bit
-    for bit) on the first n_worlds worlds of the scene, from the initial
-    state: max over a world's bodies of the relative position / orientation
-    error (relative to max(|x|, 1)).  Two FP32 runs: the colored solver the
-    bench times (its colour order differs from the reference's sequential
-    order) and the FP32 reference order (precision alone).  Worlds where
-    the reference itself goes non-finite are counted, not compared."""
+ERROR_MODES = (("fp64", "PRECISION_FP64", "SOLVE_REFERENCE_ORDER"),
+               ("fp32_reference_order", "PRECISION_FP32", "SOLVE_REFERENCE_ORDER"),
+               ("fp32_colored", "PRECISION_FP32", "SOLVE_COLORED"))
+
+
+def _run_modes(scene, stream, steps=1, dump=False, modes=ERROR_MODES):
+    """Each mode's batch of `scene`, stepped `steps` times: {name: (states,
+    contacts of the last substep or None)}.  The failure check is off:
+    worlds where the reference itself goes non-finite are counted below."""
     import rbps_b200
     from rbps_b200 import abi
-    sub = type(scene)(scene.name, scene.timestep, scene.substeps, scene.steps, scene.worlds[:n_worlds])
-    runs = {}
-    for name, prec, solve in (("fp32_colored", abi.PRECISION_FP32, abi.SOLVE_COLORED),
-                              ("fp32_reference_order", abi.PRECISION_FP32, abi.SOLVE_REFERENCE_ORDER),
-                              ("fp64", abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER)):
-        b = rbps_b200.Batch.from_scene(sub, prec, solve, stream=stream.cuda_stream)
-        b.step(1)
-        runs[name] = [b.state(w) for w in range(len(sub.worlds))]
+    out = {}
+    for name, prec, solve in modes:
+        b = rbps_b200.Batch.from_scene(scene, getattr(abi, prec), getattr(abi, solve), stream=stream.cuda_stream)
+        b.set_state_check(False)
+        if dump and steps > 1:
+            b.step(steps - 1)
+        if dump:
+            b.set_dump(True)
+        b.step(1 if dump else steps)
+        st = [b.state(w) for w in range(len(scene.worlds))]
+        con = [b.contacts(w) for w in range(len(scene.worlds))] if dump else None
         b.close()
-    ok = [np.isfinite(r["position"]).all() and np.isfinite(r["orientation"]).all() for r in runs["fp64"]]
-    out = {"worlds": int(sum(ok)), "fp64_nonfinite_worlds": int(len(ok) - sum(ok)),
-           "against": "FP64 reference order (bit-identical to the reference engine), state after step 1"}
-    for name in ("fp32_colored", "fp32_reference_order"):
-        e = []
-        for a, r, good in zip(runs[name], runs["fp64"], ok):
-            if not good:
+        out[name] = (st, con)
+    return out
+
+
+def _one_step(scene, runs, base, against, ok, comp=None):
+    """Per-world one-step errors of each run against `base`, as summaries
+    (max over a world's bodies; with comp, also over the bodies outside
+    each world's jointed component) plus the fraction of bodies within
+    1e-5."""
+    from rbps_b200 import metrics as M
+    out = {}
+    for name, st in runs.items():
+        e_all, e_out, b_in, b_n = [], [], 0, 0
+        for w in range(len(scene.worlds)):
+            if not ok[w]:
                 continue
-            ep = np.abs(a["position"] - r["position"]) / np.maximum(np.abs(r["position"]), 1.0)
-            sign = np.where((a["orientation"] * r["orientation"]).sum(1, keepdims=True) < 0, -1.0, 1.0)
-            eq = np.abs(a["orientation"] * sign - r["orientation"])
-            e.append(float(max(ep.max(), eq.max())))
-        e = np.array(e) if e else np.zeros(1)
-        out[name] = {"median": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
-                     "within_1e-5": int((e <= 1e-5).sum())}
+            e = M.state_error(st[w], base[w])
+            e_all.append(float(e.max()))
+            b_in += int((e <= 1e-5).sum())
+            b_n += len(e)
+            if comp is not None:
+                m = np.ones(len(e), bool)
+                m[comp[w]] = False
+                e_out.append(float(e[m].max()) if m.any() else 0.0)
+        r = {"max_over_world": M.summary(e_all), "bodies_within_1e-5": b_in / max(b_n, 1)}
+        if comp is not None:
+            r["max_over_world_outside_jointed_component"] = M.summary(e_out)
+        out[name] = r
+    out["against"] = against
+    return out
+
+
+def error_vs_fp64(scene, n_worlds, settled_states, stream, drift_steps=60):
+    """Errors of the FP32 modes against the FP64 reference-order engine
+    (the device engine that equals the reference bit for bit), on the first
+    n_worlds worlds:
+      cold_start   one step from the scene's initial state;
+      settled      one step from `settled_states` (the first timed step's
+                   state), over all bodies and over the bodies outside
+                   each world's jointed component (the revolute chain and
+                   whatever touches it); beside them the FP64 engine
+                   started from the same state moved by one float32 ulp per
+                   coordinate, which measures how strongly one step
+                   amplifies the smallest change a float state can carry;
+      drift        `drift_steps` steps from the settled state per mode:
+                   relative change of total energy, change of total linear
+                   momentum over the gravity impulse M g T, deepest contact
+                   and joint attachment gaps at the end.
+    Worlds where the reference itself goes non-finite are counted, not
+    compared."""
+    from rbps_b200 import metrics as M, scenes
+    sub = type(scene)(scene.name, scene.timestep, scene.substeps, scene.steps, scene.worlds[:n_worlds])
+    out = {"worlds": n_worlds,
+           "against": "FP64 reference order (bit-identical to the reference engine)"}
+    # cold start
+    runs = _run_modes(sub, stream)
+    base = runs["fp64"][0]
+    ok = [bool(np.isfinite(s["position"]).all() and np.isfinite(s["orientation"]).all()) for s in base]
+    out["fp64_nonfinite_worlds"] = int(len(ok) - sum(ok))
+    out["cold_start"] = _one_step(sub, {k: runs[k][0] for k in ("fp32_colored", "fp32_reference_order")}, base,
+                                  "state after step 1 from the initial state", ok)
+    # settled: the timed state
+    settled = scenes.with_state(sub, settled_states[:n_worlds])
+    runs = _run_modes(settled, stream, dump=True)
+    base, c64 = runs["fp64"]
+    ok = [bool(np.isfinite(s["position"]).all() and np.isfinite(s["orientation"]).all()) for s in base]
+    comp = [M.jointed_component(settled.worlds[w], c64[w]) for w in range(n_worlds)]
+    pert = scenes.with_state(settled, [M.perturb_ulp(s) for s in settled_states[:n_worlds]])
+    ulp = _run_modes(pert, stream, modes=ERROR_MODES[:1])["fp64"][0]
+    gaps0 = [M.joint_gaps(settled.worlds[w], settled_states[w]) for w in range(n_worlds)]
+    out["settled"] = _one_step(settled, {"fp32_colored": runs["fp32_colored"][0],
+                                         "fp32_reference_order": runs["fp32_reference_order"][0],
+                                         "fp64_one_ulp_perturbed_start": ulp},
+                               base, "state after one step from the first timed step's state", ok, comp)
+    out["settled"]["chains_broken_worlds"] = int(sum(len(g) and g.max() > 0.1 for g in gaps0))
+    out["settled"]["jointed_component_bodies_median"] = float(np.median([len(c) for c in comp]))
+    # drift from the settled state
+    e0 = sum(M.world_energy(settled.worlds[w], settled_states[w]) for w in range(n_worlds))
+    p0 = sum(M.world_momentum(settled.worlds[w], settled_states[w]) for w in range(n_worlds))
+    mass = sum(float(w.bodies["mass"][w.bodies["type"] == 1].sum()) for w in settled.worlds)
+    impulse = mass * 9.81 * drift_steps * scene.timestep
+    drift = {"steps": drift_steps}
+    for name, (st, con) in _run_modes(settled, stream, steps=drift_steps, dump=True).items():
+        fin = [bool(np.isfinite(s["position"]).all()) for s in st]
+        ws = [w for w in range(n_worlds) if fin[w]]
+        e = sum(M.world_energy(settled.worlds[w], st[w]) for w in ws)
+        p = sum(M.world_momentum(settled.worlds[w], st[w]) for w in ws)
+        gaps = np.concatenate([M.joint_gaps(settled.worlds[w], st[w]) for w in ws])
+        depth = max((float(con[w]["penetration_depth"].max()) for w in ws if len(con[w])), default=0.0)
+        drift[name] = {"energy_rel": (e - e0) / abs(e0), "momentum_over_gravity_impulse": float(np.linalg.norm(p - p0) / impulse),
+                       "max_penetration_m": depth, "joint_gap_median_m": float(np.median(gaps)) if len(gaps) else 0.0,
+                       "joint_gap_max_m": float(gaps.max()) if len(gaps) else 0.0, "nonfinite_worlds": len(fin) - len(ws)}
+    out["drift_from_settled"] = drift
     return out
 
 
@@ -492,6 +576,8 @@ def main():
     ap.add_argument("--preroll", type=int, default=240,
                     help="untimed steps before the warm-up (240 = 2 s simulated: the bodies have landed)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--error-worlds", type=int, default=256,
+                    help="worlds in the error report against FP64 (0 = skip it)")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--autotune", type=int, default=1, help="1: run the launch-shape autotuner before timing")
     ap.add_argument("--plain-worlds", type=int, default=64,
@@ -539,7 +625,10 @@ def main():
             torch.distributed.destroy_process_group()
         return
 
-    scene = scenes.config3(seed=rank_seed(args.seed, rank), n_worlds=args.worlds)
+    # one set of worlds * ranks worlds, split across the ranks by balanced
+    # body count (weak scaling: each rank keeps about `worlds` worlds)
+    from rbps_b200 import shard
+    scene, _ = shard.shard_scene(scenes.config3(seed=args.seed, n_worlds=args.worlds * ws), ws, rank)
     stream = torch.cuda.Stream()  # a real stream: the legacy NULL stream would not order our launches
     torch.cuda.set_stream(stream)
     free0 = torch.cuda.mem_get_info(local)[0]
@@ -631,7 +720,12 @@ def main():
     e2e_value = n_dyn_all * scene.substeps * e2e_steps / (e2e_ms / 1e3)
     finite = bool(np.isfinite(p_host.numpy()).all() and np.isfinite(p_host2.numpy()).all())
 
-    err1 = one_step_error(scene, min(256, len(scene.worlds)), stream) if rank == 0 else None
+    err1 = None
+    if rank == 0 and args.error_worlds > 0:
+        batch.restore(snap)  # the first timed step's state
+        nw = min(args.error_worlds, len(scene.worlds))
+        settled = [batch.state(w) for w in range(nw)]
+        err1 = error_vs_fp64(scene, nw, settled, stream)
 
     plain = None
     if args.plain_worlds > 0:
@@ -660,7 +754,8 @@ def main():
                            "device_bytes": dev_bytes,
                            "l2": f"inputs larger than L2: {dev_bytes / 1e6:.0f} MB of world state and scratch "
                                  "touched every step (L2 126 MB)",
-                           "parallelism": f"world-sharded replicas x{ws}", "seed": args.seed,
+                           "parallelism": f"worlds split over {ws} rank(s) by balanced body count",
+                           "worlds_total": args.worlds * ws, "seed": args.seed,
                            "autotune": tune,
                            "state_finite": finite},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -669,7 +764,7 @@ def main():
                              "kernel": f"one step = {st['kernel_launches'] // max(args.steps, 1)} phase-kernel launches"},
                 "cpu_baseline": cpu,
                 "plain_gpu": plain,
-                "one_step_error_vs_fp64": err1,
+                "error_vs_fp64": err1,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n_tot_all) * 24,
                         "d2h_bytes_per_step": int(n_tot_all) * 56, "steps": e2e_steps,
                         "window": "the same steps as value (device snapshot after the warm-up, restored)"},

@@ -51,7 +51,8 @@ class StateView(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("frame_block", C.c_int32), ("narrow_grid", C.c_int32), ("ms_per_step", C.c_double),
-                ("ms_per_step_default", C.c_double), ("trials", C.c_uint32), ("team_bodies", C.c_uint32)]
+                ("ms_per_step_default", C.c_double), ("trials", C.c_uint32), ("team_bodies", C.c_uint32),
+                ("narrow_per_warp", C.c_uint32), ("color_chunk", C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -89,6 +90,7 @@ def lib():
             "rbps_batch_snapshot_update": (i, [_P, C.c_uint32]),
             "rbps_batch_restore": (i, [_P, C.c_uint32]),
             "rbps_batch_autotune": (i, [_P, C.c_int32, C.POINTER(TuneResult)]),
+            "rbps_batch_set_launch": (i, [_P, C.POINTER(TuneResult)]),
             "rbps_world_add_collider": (i, [_P, C.c_uint32, _P, _U]),
             "rbps_world_add_colliders": (i, [_P, C.c_uint32, C.c_uint32, _P, _U]),
             "rbps_world_add_joint": (i, [_P, C.c_uint32, _P, _U]),
@@ -325,6 +327,15 @@ class Batch:
         r = TuneResult()
         _check(lib().rbps_batch_autotune(self.h, trial_steps, C.byref(r)))
         return {k: getattr(r, k) for k, _ in TuneResult._fields_ if k != "pad_"}
+
+    def set_launch(self, **cfg):
+        """Applies launch-shape fields (frame_block, narrow_grid, team_bodies,
+        narrow_per_warp, color_chunk) as rbps_batch_set_launch; others keep
+        their values.  Results do not depend on them."""
+        r = TuneResult()
+        for k, v in cfg.items():
+            setattr(r, k, v)
+        _check(lib().rbps_batch_set_launch(self.h, C.byref(r)))
 
     def snapshot(self):
         """Device-side snapshot of the whole batch state; returns its slot."""

@@ -334,6 +334,8 @@ struct rbps_batch
     HmDesc *hm_desc = nullptr;
     bool committed = false;
     bool check_state = true; // rbps_batch_set_state_check
+    uint32_t narrow_per_warp = 32;        // narrowphase candidates a warp takes per pass (autotuned)
+    uint32_t color_chunk = kColorStage;   // candidates the colouring stages per batch (autotuned)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 0;
@@ -866,6 +868,8 @@ namespace
         e.solve_mode = b->desc.solve_mode;
         e.use_vel_exp = b->desc.use_velocity_expansion;
         e.check_state = b->check_state ? 1 : 0;
+        e.narrow_per_warp = b->narrow_per_warp;
+        e.color_chunk = b->color_chunk;
         e.work_counter = b->work_counter;
         e.scratch = b->scratch;
         e.wcoff = b->wcoff;
@@ -2586,6 +2590,64 @@ static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
         if (!rc)
             rc = set_team_split<T, P>(b, best_t);
     }
+    // then the narrowphase candidates per warp and the colouring batch, one
+    // knob at a time with the others at their best
+    const uint32_t npw0 = b->narrow_per_warp, cc0 = b->color_chunk;
+    uint32_t best_npw = npw0, best_cc = cc0;
+    auto time_knobs = [&](uint32_t npw, uint32_t cc, double *ms_out) -> int {
+        b->narrow_per_warp = npw;
+        b->color_chunk = cc;
+        int r2 = apply_launch<T, P>(b, best_c.first, best_c.second);
+        if (!r2)
+            r2 = snapshot_copy<T, P>(b, b->snaps[slot], 1);
+        if (!r2)
+            r2 = step_typed<T, P>(b, 1);
+        if (r2)
+            return r2;
+        if (cudaEventRecord(e0, b->stream) != cudaSuccess)
+            return fail(RBPS_ERR_CUDA, "autotune: event record failed");
+        if ((r2 = step_typed<T, P>(b, trials)))
+            return r2;
+        float ms = 0.f;
+        if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            return fail(RBPS_ERR_CUDA, "autotune: event timing failed");
+        *ms_out = ms / trials;
+        return RBPS_OK;
+    };
+    if (!rc && b->use_flat)
+    {
+        for (uint32_t npw : {64u, 128u, 256u})
+        {
+            double ms = 0.0;
+            if (rc || npw == npw0)
+                continue;
+            ++n_trials;
+            if ((rc = time_knobs(npw, best_cc, &ms)))
+                break;
+            if (ms < best)
+            {
+                best = ms;
+                best_npw = npw;
+            }
+        }
+        for (uint32_t cc : {64u, 128u})
+        {
+            double ms = 0.0;
+            if (rc || cc == cc0)
+                continue;
+            ++n_trials;
+            if ((rc = time_knobs(best_npw, cc, &ms)))
+                break;
+            if (ms < best)
+            {
+                best = ms;
+                best_cc = cc;
+            }
+        }
+    }
+    b->narrow_per_warp = best_npw;
+    b->color_chunk = best_cc;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc)
@@ -2604,6 +2666,8 @@ static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
         out->ms_per_step_default = first;
         out->trials = n_trials;
         out->team_bodies = best_t;
+        out->narrow_per_warp = best_npw;
+        out->color_chunk = best_cc;
     }
     return check_device_error(b);
 }
@@ -2614,6 +2678,34 @@ extern "C" int rbps_batch_autotune(rbps_batch *b, int32_t trial_steps, rbps_tune
         return fail(RBPS_ERR_INVALID, "rbps_batch_autotune: commit first; trial_steps >= 1");
     CU(cudaSetDevice(b->desc.device));
     return DISPATCH_PREC(b, autotune_typed, b, trial_steps, out);
+}
+
+template <class T, class P>
+static int set_launch_typed(rbps_batch *b, const rbps_tune_result *cfg)
+{
+    int rc;
+    if (b->use_flat && cfg->team_bodies && (rc = set_team_split<T, P>(b, cfg->team_bodies)))
+        return rc;
+    if (cfg->narrow_per_warp)
+        b->narrow_per_warp = cfg->narrow_per_warp;
+    if (cfg->color_chunk)
+        b->color_chunk = cfg->color_chunk;
+    return apply_launch<T, P>(b, cfg->frame_block ? cfg->frame_block : b->phase.block[kKFrame],
+                              cfg->narrow_grid ? cfg->narrow_grid : b->flat.grid_narrow);
+}
+
+extern "C" int rbps_batch_set_launch(rbps_batch *b, const rbps_tune_result *cfg)
+{
+    if (!b || !b->committed || !cfg)
+        return fail(RBPS_ERR_INVALID, "rbps_batch_set_launch: commit first; non-null configuration");
+    if ((cfg->frame_block && cfg->frame_block != 128 && cfg->frame_block != 256) || cfg->narrow_grid < 0 ||
+        (cfg->narrow_per_warp && (cfg->narrow_per_warp % 32 || cfg->narrow_per_warp > 4096)) ||
+        (cfg->color_chunk && (cfg->color_chunk > kColorStage || cfg->color_chunk < 32)))
+        return fail(RBPS_ERR_INVALID, "rbps_batch_set_launch: frame_block 128 or 256, narrow_per_warp a multiple "
+                                      "of 32 up to 4096, color_chunk in [32, %u] (0 keeps a field)", kColorStage);
+    CU(cudaSetDevice(b->desc.device));
+    CU(cudaStreamSynchronize(b->stream));
+    return DISPATCH_PREC(b, set_launch_typed, b, cfg);
 }
 
 extern "C" int rbps_batch_step_io(rbps_batch *b, const double *force_in, double *position_out, double *orientation_out)

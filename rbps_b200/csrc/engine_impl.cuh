@@ -1634,6 +1634,24 @@ namespace rbps_gpu
 
     // Narrowphase of every candidate of the small worlds but the box-box
     // ones, in class order.
+    // Entries [0, n) of a class-sorted range, dealt to the grid's warps in
+    // chunks of `per_warp` (a multiple of 32) consecutive entries, a lane
+    // taking every 32nd entry of its warp's chunk; per_warp = 32 is the
+    // plain grid-stride loop.  f(k) runs once per entry.
+    template <class F>
+    __device__ __forceinline__ void for_warp_chunks(uint32_t n, uint32_t per_warp, F &&f)
+    {
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+        for (uint32_t base = warp * per_warp; base < n; base += n_warps * per_warp)
+        {
+            const uint32_t end = min(n, base + per_warp);
+            for (uint32_t k = base + lane; k < end; k += 32)
+                f(k);
+        }
+    }
+
     template <class T, class P>
     __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow(const Engine<T, P> E)
     {
@@ -1641,8 +1659,8 @@ namespace rbps_gpu
         const uint32_t total = E.gcol[kGcolOff + kPairClasses];
         const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
         const uint32_t n = total - (bb1 - bb0);
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-            narrow_flat<T, P, kSelNoBoxBox>(E, k < bb0 ? k : k + (bb1 - bb0));
+        for_warp_chunks(n, E.narrow_per_warp,
+                        [&](uint32_t k) { narrow_flat<T, P, kSelNoBoxBox>(E, k < bb0 ? k : k + (bb1 - bb0)); });
     }
 
     // The box-box class on its own: its SAT, clipping buffers and registers
@@ -1651,8 +1669,7 @@ namespace rbps_gpu
     __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow_boxbox(const Engine<T, P> E)
     {
         const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
-        for (uint32_t i = bb0 + blockIdx.x * blockDim.x + threadIdx.x; i < bb1; i += gridDim.x * blockDim.x)
-            narrow_flat<T, P, kSelBoxBox>(E, i);
+        for_warp_chunks(bb1 - bb0, E.narrow_per_warp, [&](uint32_t k) { narrow_flat<T, P, kSelBoxBox>(E, bb0 + k); });
     }
 
     // The rest of a substep for one world per warp: colouring, integrate
@@ -1660,7 +1677,7 @@ namespace rbps_gpu
     // The contacting candidates of world W into S.alist, in candidate
     // order; returns their count to every thread of the team.
     template <class T, class P>
-    __device__ uint32_t compact_active(const WarpTeam &, const Scr<T, P> &S, uint32_t n_cand, BlockShared &)
+    __device__ uint32_t compact_active(const WarpTeam &, const Scr<T, P> &S, uint32_t n_cand, ScanShared &)
     {
         const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
         uint32_t n_act = 0;
@@ -1681,7 +1698,7 @@ namespace rbps_gpu
     }
 
     template <class T, class P>
-    __device__ uint32_t compact_active(const BlockTeam &, const Scr<T, P> &S, uint32_t n_cand, BlockShared &sh)
+    __device__ uint32_t compact_active(const BlockTeam &, const Scr<T, P> &S, uint32_t n_cand, ScanShared &sh)
     {
         uint32_t n_act = 0;
         for (uint32_t base = 0; base < n_cand; base += blockDim.x)
@@ -1710,7 +1727,7 @@ namespace rbps_gpu
     // colours to every thread.
     template <class T, class P, class Team>
     __device__ uint32_t greedy_color_world(const Engine<T, P> &E, const Team &tm, uint32_t w,
-                                           unsigned long long *mask, BlockShared &sh, uint32_t *book,
+                                           unsigned long long *mask, ScanShared &sh, uint32_t *book,
                                            uint32_t *stage = nullptr)
     {
         const WorldDev W = E.worlds[w];
@@ -1736,9 +1753,10 @@ namespace rbps_gpu
             // -- the same candidates in the same order -- touches shared
             // memory only.
             uint8_t *scol = reinterpret_cast<uint8_t *>(stage + kColorStage);
-            for (uint32_t q0 = 0; q0 < n_act; q0 += kColorStage)
+            const uint32_t chunk = E.color_chunk; // <= kColorStage
+            for (uint32_t q0 = 0; q0 < n_act; q0 += chunk)
             {
-                const uint32_t m = min(kColorStage, n_act - q0);
+                const uint32_t m = min(chunk, n_act - q0);
                 for (uint32_t k = tm.rank(); k < m; k += tm.size())
                 {
                     const Cand cd = S.cand[S.alist[q0 + k]];
@@ -1853,8 +1871,13 @@ namespace rbps_gpu
         return book ? book[132] : misc[kMiscNColors];
     }
 
+// Resident 128-thread CTAs per SM the registers must allow (128 registers a
+// thread at 4).  Measured on the batched workload (4,096 worlds, settled):
+// 3 CTAs (168 registers) 7.58 ms a step, 4 CTAs with the previous pose in
+// shared memory (which then does not fit four) 7.89, 4 CTAs with it in
+// place 7.16, 5 CTAs (96 registers, heavy spills) 7.40.
 #ifndef RBPS_SUBSTEP_MIN_BLOCKS
-#define RBPS_SUBSTEP_MIN_BLOCKS 3 // resident 128-thread CTAs per SM the registers must allow
+#define RBPS_SUBSTEP_MIN_BLOCKS 4
 #endif
     // The rest of a substep for every small world: colouring, integrate
     // (Body.cpp:18-39), position solve + velocity update, velocity solve.
@@ -1867,14 +1890,22 @@ namespace rbps_gpu
     // `cap` bodies per array (cap a multiple of 16 keeps every array 16-byte
     // aligned).  Force, torque and the inertia tensors are read in place
     // through the batch arrays offset to the world.
+// The previous pose (written once by integrate, read by the friction rows
+// and the velocity update) stays in the batch arrays by default: without it
+// a 512-body world's shared copy fits four 128-thread CTAs on an SM (see
+// RBPS_SUBSTEP_MIN_BLOCKS).  1 keeps it in the shared copy too.
+#ifndef RBPS_SMEM_PREV
+#define RBPS_SMEM_PREV 0
+#endif
     template <class T, class P>
     struct SmemWorld
     {
         static constexpr size_t kBook = 136 * sizeof(uint32_t);
         // colouring stage: kColorStage packed candidate records + their colours
         static constexpr size_t kStage = kColorStage * (sizeof(uint32_t) + 1);
-        static constexpr size_t kPerBody =
-            sizeof(unsigned long long) + 2 * sizeof(V4<P>) + 2 * sizeof(Q4<T>) + 2 * sizeof(V4<T>) + 1;
+        static constexpr bool kPrev = RBPS_SMEM_PREV != 0;
+        static constexpr size_t kPerBody = sizeof(unsigned long long) + (kPrev ? 2 : 1) * sizeof(V4<P>) +
+                                           (kPrev ? 2 : 1) * sizeof(Q4<T>) + 2 * sizeof(V4<T>) + 1;
 
         __host__ __device__ static size_t bytes(uint32_t cap) { return kBook + kStage + (size_t)cap * kPerBody; }
 
@@ -1890,12 +1921,20 @@ namespace rbps_gpu
             Bodies<T, P> V;
             V.pos = reinterpret_cast<V4<P> *>(p);
             p += (size_t)cap * sizeof(V4<P>);
-            V.prev_pos = reinterpret_cast<V4<P> *>(p);
-            p += (size_t)cap * sizeof(V4<P>);
             V.rot = reinterpret_cast<Q4<T> *>(p);
             p += (size_t)cap * sizeof(Q4<T>);
-            V.prev_rot = reinterpret_cast<Q4<T> *>(p);
-            p += (size_t)cap * sizeof(Q4<T>);
+            if (kPrev)
+            {
+                V.prev_pos = reinterpret_cast<V4<P> *>(p);
+                p += (size_t)cap * sizeof(V4<P>);
+                V.prev_rot = reinterpret_cast<Q4<T> *>(p);
+                p += (size_t)cap * sizeof(Q4<T>);
+            }
+            else
+            {
+                V.prev_pos = G.prev_pos + body_off;
+                V.prev_rot = G.prev_rot + body_off;
+            }
             V.lin = reinterpret_cast<V4<T> *>(p);
             p += (size_t)cap * sizeof(V4<T>);
             V.ang = reinterpret_cast<V4<T> *>(p);
@@ -1916,7 +1955,7 @@ namespace rbps_gpu
     // substep and are written back once.
     template <class T, class P, class Team>
     __device__ void substep_world(const Engine<T, P> &E, const Team &tm, uint32_t w, unsigned char *smem,
-                                  uint32_t cap, BlockShared &sh)
+                                  uint32_t cap, ScanShared &sh)
     {
         const WorldDev W = E.worlds[w];
         const bool local = smem && W.n_bodies <= cap;
@@ -1944,8 +1983,11 @@ namespace rbps_gpu
                 V.rot[b] = G.rot[g];
                 V.lin[b] = G.lin[g];
                 V.ang[b] = G.ang[g];
-                V.prev_pos[b] = G.prev_pos[g];
-                V.prev_rot[b] = G.prev_rot[g];
+                if (SmemWorld<T, P>::kPrev)
+                {
+                    V.prev_pos[b] = G.prev_pos[g];
+                    V.prev_rot[b] = G.prev_rot[g];
+                }
                 V.type[b] = G.type[g];
             }
             tm.sync();
@@ -1968,8 +2010,11 @@ namespace rbps_gpu
                 G.rot[g] = V.rot[b];
                 G.lin[g] = V.lin[b];
                 G.ang[g] = V.ang[b];
-                G.prev_pos[g] = V.prev_pos[b];
-                G.prev_rot[g] = V.prev_rot[b];
+                if (SmemWorld<T, P>::kPrev)
+                {
+                    G.prev_pos[g] = V.prev_pos[b];
+                    G.prev_rot[g] = V.prev_rot[b];
+                }
             }
             tm.sync();
         }
@@ -1983,7 +2028,7 @@ namespace rbps_gpu
     template <class T, class P>
     __global__ void __launch_bounds__(128, RBPS_SUBSTEP_MIN_BLOCKS) k_substep(const Engine<T, P> E)
     {
-        __shared__ BlockShared sh;
+        __shared__ ScanShared sh; // the colouring's compaction scan is all the team needs
         extern __shared__ __align__(16) unsigned char smem[];
         if (blockIdx.x < E.n_block_worlds)
         {

@@ -212,6 +212,12 @@ namespace rbps_gpu
         int solve_mode;
         int use_vel_exp;
         int check_state; // the stats phase reports a non-finite body state (RBPS_ERR_STATE)
+        // launch-shape knobs of the flat coloured pipeline (autotuned; results
+        // do not depend on them): narrowphase candidates a warp takes per
+        // pass (a multiple of 32), and active candidates the colouring stages
+        // per batch (<= kColorStage)
+        uint32_t narrow_per_warp;
+        uint32_t color_chunk;
         // executors
         char *scratch;            // per-world slices at WorldDev::scr_off
         uint32_t *work_counter;

@@ -55,10 +55,16 @@ namespace rbps_gpu
     constexpr int kMaxWarps = 32;
 
     // Shared scratch of the block primitives (one per CTA).
-    struct BlockShared
+    // Shared scratch of a block scan (all a kernel needs that only scans).
+    struct ScanShared
     {
         uint32_t warp[kMaxWarps];
         uint32_t bcast[4];
+    };
+
+    // Shared scratch of the block scans and the radix sort's ranking passes.
+    struct BlockShared : ScanShared
+    {
         uint32_t hist[256];
         uint32_t wdig[8 * 256]; // per-warp digit counts, <= 8 warps per tile rank pass
     };
@@ -80,7 +86,7 @@ namespace rbps_gpu
 
     // Exclusive block scan of one value per thread; *total gets the sum.
     // Contains two __syncthreads; every thread of the block must call it.
-    __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, BlockShared &sh, uint32_t *total)
+    __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, ScanShared &sh, uint32_t *total)
     {
         const uint32_t inc = warp_incl_scan(v);
         const uint32_t nw = (blockDim.x + 31) >> 5;

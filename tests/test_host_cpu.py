@@ -99,8 +99,17 @@ def _rank_main(rank, ws, port, out_dir):
         t = bench.reduce_over_ranks(10.0 + rank, "max", ws)     # per-rank device time
         n = bench.reduce_over_ranks(100 * (rank + 1), "sum", ws)  # per-rank dynamic bodies
         seed = bench.rank_seed(7, rank)
+        # the batched workload: one set of worlds, split as bench.py splits it
+        from rbps_b200 import shard
+        full = scenes.config3(seed=3, n_worlds=48 * ws)
+        mine, idx = shard.shard_scene(full, ws, rank)
+        bodies = sum(w.n_bodies for w in mine.worlds)
+        total = bench.reduce_over_ranks(bodies, "sum", ws)
+        hi = bench.reduce_over_ranks(bodies, "max", ws)
+        lo = -bench.reduce_over_ranks(-bodies, "max", ws)
         with open(os.path.join(out_dir, f"r{rank}.json"), "w") as f:
-            json.dump({"t": t, "n": n, "seed": seed}, f)
+            json.dump({"t": t, "n": n, "seed": seed, "idx": idx.tolist(), "total": total, "hi": hi, "lo": lo,
+                       "full_total": full.n_bodies, "max_world": max(w.n_bodies for w in full.worlds)}, f)
     finally:
         dist.destroy_process_group()
 
@@ -111,7 +120,28 @@ def test_multirank_aggregation_gloo(tmp_path):
     r = [json.load(open(tmp_path / f"r{k}.json")) for k in range(2)]
     assert r[0]["t"] == r[1]["t"] == 11.0        # time: max over ranks
     assert r[0]["n"] == r[1]["n"] == 300.0       # work: sum over ranks
-    assert r[0]["seed"] != r[1]["seed"]          # each rank draws its own worlds
+    assert r[0]["seed"] != r[1]["seed"]          # single-world replicas draw their own worlds
+    # the batched worlds: one set, split exactly once, balanced by bodies
+    idx = sorted(r[0]["idx"] + r[1]["idx"])
+    assert idx == list(range(96))
+    assert r[0]["total"] == r[0]["full_total"]
+    assert r[0]["hi"] - r[0]["lo"] <= r[0]["max_world"]
+
+
+def test_partition_balance_and_order():
+    from rbps_b200 import shard
+    rng = np.random.default_rng(0)
+    counts = np.floor(np.exp(rng.uniform(np.log(8), np.log(513), 4096))).astype(int) + 14
+    for n in (1, 2, 3, 8):
+        parts = shard.partition_worlds(counts, n)
+        assert len(parts) == n
+        allidx = np.sort(np.concatenate(parts))
+        np.testing.assert_array_equal(allidx, np.arange(len(counts)))
+        loads = [int(counts[p].sum()) for p in parts]
+        assert max(loads) - min(loads) <= counts.max()
+        for p in parts:
+            assert (np.diff(p) > 0).all()  # worlds keep their order within a rank
+    np.testing.assert_array_equal(shard.partition_worlds(counts, 1)[0], np.arange(len(counts)))
 
 
 def test_reduce_single_rank_is_identity():

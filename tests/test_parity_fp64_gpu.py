@@ -77,20 +77,23 @@ def test_golden_step10(rbps, name):
 
 
 def test_config0_live_oracle(rbps, ref):
-    """Config 0 (512 boxes + spheres, FP64): pair lists identical every step
-    for 30 steps, state after step 1 within the gate."""
-    sc = scenes.config0(seed=0, steps=30)
+    """Config 0 as specified (512 boxes + spheres over a plane, FP64, dt
+    1/60, 10 substeps, 600 steps): the pair list identical to the live
+    reference's every step for all 600 steps, the state after step 1 within
+    the gate and the state bit-identical at every 50th step."""
+    sc = scenes.config0(seed=0, steps=600)
     w_ref = ref.RefWorld(sc.worlds[0], sc.timestep, sc.substeps)
     b = _batch(rbps, sc)
-    for step in range(1, 31):
+    for step in range(1, 601):
         w_ref.step(1)
         b.step(1)
         np.testing.assert_array_equal(b.pairs(0), w_ref.pairs(), err_msg=f"step {step}")
         if step == 1:
             err = state_err(b.state(0), w_ref.state())
             assert max(err.values()) <= ONE_STEP_TOL, err
-    st, rs = b.state(0), w_ref.state()
-    assert bit_equal(st, rs) or max(state_err(st, rs).values()) <= ONE_STEP_TOL
+        if step % 50 == 0:
+            st, rs = b.state(0), w_ref.state()
+            assert bit_equal(st, rs), f"step {step}: {state_err(st, rs)}"
 
 
 def test_hull_world_live_oracle(rbps, ref):
