@@ -379,7 +379,6 @@ struct rbps_batch
     uint2 *gjk_list = nullptr;
     uint32_t *gjk_count = nullptr;
     uint32_t gjk_cap = 0, gjk_slots = 0;
-    void *gjk_ws = nullptr;
     PhaseLaunch phase{};      // grid / block of each phase kernel
     FlatLaunch flat{};        // flat colored pipeline
     bool use_flat = false;
@@ -899,7 +898,6 @@ namespace
         e.gjk_count = b->gjk_count;
         e.gjk_cap = b->gjk_cap;
         e.gjk_slots = b->gjk_slots;
-        e.gjk_ws = b->gjk_ws;
         e.origin = b->origin_d;
         e.body_world = b->body_world_d;
         return e;
@@ -1533,10 +1531,11 @@ static int commit_typed(rbps_batch *b)
         if (any_hull && cap)
         {
             b->gjk_cap = (uint32_t)std::min<size_t>(cap, 0xffffffffu);
-            b->gjk_slots = (uint32_t)(((size_t)b->sm_count * 16 + 127) / 128 * 128);
+            // the GJK pass: one warp per queued pair, its polytope and
+            // clipping buffers in shared memory; as many CTAs as stay resident
+            CU(prepare_gjk<T, P>(b->sm_count, &b->gjk_slots));
             if ((rc = b->alloc((void **)&b->gjk_list, sizeof(uint2) * cap)) ||
-                (rc = b->alloc((void **)&b->gjk_count, 64)) ||
-                (rc = b->alloc(&b->gjk_ws, gjk_work_bytes<T, P>() * b->gjk_slots)))
+                (rc = b->alloc((void **)&b->gjk_count, 64)))
                 return rc;
         }
     }
@@ -2235,11 +2234,9 @@ static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> 
     bool gjk = false;
     for (uint32_t i = 0; i < n && !gjk; ++i)
         gjk = (gjk_kind(sa[i].kind) || gjk_kind(sb[i].kind)) && sa[i].kind != kPlane && sb[i].kind != kPlane;
-    // GJK pairs need a workspace per thread: fewer threads, each looping
-    const uint32_t threads = (uint32_t)std::min<size_t>(((size_t)n + 127) / 128 * 128, gjk ? 1024 : 65536);
-    const size_t ws_bytes = gjk ? gjk_work_bytes<T, P>() * threads : 0;
+    (void)gjk; // one warp per pair, GJK workspaces in shared memory
     char *d = nullptr;
-    const size_t total = 2 * shape_bytes + 2 * tf_bytes + (size_t)n * sizeof(CollideOut) + ws_bytes;
+    const size_t total = 2 * shape_bytes + 2 * tf_bytes + (size_t)n * sizeof(CollideOut);
     CU(cudaMalloc(&d, total));
     ShapeDev *dsa = (ShapeDev *)d, *dsb = (ShapeDev *)(d + shape_bytes);
     double *dta = (double *)(d + 2 * shape_bytes), *dtb = (double *)(d + 2 * shape_bytes + tf_bytes);
@@ -2251,9 +2248,8 @@ static int collide_typed(rbps_batch *b, uint32_t n, const std::vector<ShapeDev> 
         e = cudaMemcpyAsync(dta, tf_a, tf_bytes, cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dtb, tf_b, tf_bytes, cudaMemcpyHostToDevice, b->stream);
-    void *ws = gjk ? (void *)(d + 2 * shape_bytes + 2 * tf_bytes + (size_t)n * sizeof(CollideOut)) : nullptr;
     if (e == cudaSuccess)
-        e = launch_collide<T, P>(dsa, dta, dsb, dtb, hs, n, dout, ws, threads, b->error_d, b->stream);
+        e = launch_collide<T, P>(dsa, dta, dsb, dtb, hs, n, dout, b->error_d, b->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(out, dout, (size_t)n * sizeof(CollideOut), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess)

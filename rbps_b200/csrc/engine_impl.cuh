@@ -803,10 +803,7 @@ namespace rbps_gpu
         }
     }
 
-    // GJK / EPA / manifold of one queued pair (world w, candidate c) on the
-    // workspace of the calling thread.
-    // GJK and EPA run in double in every precision: their tolerances
-    // (EPA convergence 1e-6, coplanarity 1e-12) are below float resolution.
+    // A double manifold in precision T.
     template <class T>
     __device__ __forceinline__ Manifold<T> manifold_cast(const Manifold<double> &d)
     {
@@ -821,21 +818,29 @@ namespace rbps_gpu
         return m;
     }
 
+    // GJK / EPA / manifold of one queued pair (world w, candidate c) on one
+    // warp: every lane runs GJK / EPA with the warp's shared workspace `ws`;
+    // lane 0 writes the contact block.  GJK and EPA run in double in every
+    // precision: their tolerances (EPA convergence 1e-6, coplanarity 1e-12)
+    // are below float resolution.
     template <class T, class P>
-    __device__ void gjk_candidate(const Engine<T, P> &E, uint32_t w, uint32_t c, GjkWork<double> &ws)
+    __device__ void gjk_candidate_warp(const Engine<T, P> &E, uint32_t w, uint32_t c, unsigned char *ws)
     {
         const WorldDev W = E.worlds[w];
         const Cand cd = E.wcand ? E.wcand[w][c] : world_scratch(E, W).cand[c];
-        CandContacts<T, P> &out = E.wcc ? E.wcc[w][c] : world_scratch(E, W).cc[c];
         const uint32_t gca = W.coll_off + cd.ca, gcb = W.coll_off + cd.cb;
         const uint32_t gba = W.body_off + cd.ba, gbb = W.body_off + cd.bb;
         const tf<double> ta = collider_tf_d(E, gca, gba);
         const tf<double> tb = collider_tf_d(E, gcb, gbb);
         Manifold<double> m;
         m.n = 0;
-        const bool hit = gjk_epa_manifold(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, ws, m, E.error);
-        const Manifold<T> mt = manifold_cast<T>(m);
-        emit_manifold(E, gca, gcb, gba, gbb, mt, hit ? mt.n : 0, out);
+        const bool hit = gjk_epa_manifold_warp(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, ws, m, E.error);
+        if ((threadIdx.x & 31u) == 0)
+        {
+            CandContacts<T, P> &out = E.wcc ? E.wcc[w][c] : world_scratch(E, W).cc[c];
+            const Manifold<T> mt = manifold_cast<T>(m);
+            emit_manifold(E, gca, gcb, gba, gbb, mt, hit ? mt.n : 0, out);
+        }
     }
 
     // All contact rows of one candidate pair (global bodies ba, bb), in list
@@ -998,6 +1003,7 @@ namespace rbps_gpu
         {
             S.misc[kMiscNGjk] = 0u;
             S.misc[kMiscMaxColors] = 0u;
+            S.misc[kMiscColorValid] = 0u; // a new candidate list: no colouring yet
         }
         const uint32_t n_pairs = broadphase(E, tm, W, S, sh, sort_smem);
         clk.mark(kPhBroadphase);
@@ -1676,46 +1682,81 @@ namespace rbps_gpu
     // (Body.cpp:18-39), position solve + velocity update, velocity solve.
     // The contacting candidates of world W into S.alist, in candidate
     // order; returns their count to every thread of the team.
-    template <class T, class P>
-    __device__ uint32_t compact_active(const WarpTeam &, const Scr<T, P> &S, uint32_t n_cand, ScanShared &)
+    // Compaction of candidate indices [0, n_cand) for which sel(c) holds into
+    // out[0, count), in candidate order; returns the count to every thread.
+    template <class F>
+    __device__ __forceinline__ uint32_t team_compact(const WarpTeam &, uint32_t n_cand, uint32_t *out, ScanShared &,
+                                                     F &&sel)
     {
         const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
-        uint32_t n_act = 0;
+        uint32_t n = 0;
         for (uint32_t base = 0; base < n_cand; base += 32)
         {
             const uint32_t c = base + lane;
-            const bool live = c < n_cand;
-            const bool act = live && S.cc[c].n > 0;
-            const uint32_t m = __ballot_sync(0xffffffffu, act);
-            if (act)
-                S.alist[n_act + __popc(m & lt)] = c;
-            if (live)
-                S.color[c] = act ? 0xffffffffu : kColorIdle;
-            n_act += __popc(m);
+            const bool take = c < n_cand && sel(c);
+            const uint32_t m = __ballot_sync(0xffffffffu, take);
+            if (take)
+                out[n + __popc(m & lt)] = c;
+            n += __popc(m);
         }
         __syncwarp();
-        return n_act;
+        return n;
     }
 
-    template <class T, class P>
-    __device__ uint32_t compact_active(const BlockTeam &, const Scr<T, P> &S, uint32_t n_cand, ScanShared &sh)
+    template <class F>
+    __device__ __forceinline__ uint32_t team_compact(const BlockTeam &, uint32_t n_cand, uint32_t *out, ScanShared &sh,
+                                                     F &&sel)
     {
-        uint32_t n_act = 0;
+        uint32_t n = 0;
         for (uint32_t base = 0; base < n_cand; base += blockDim.x)
         {
             const uint32_t c = base + threadIdx.x;
-            const bool live = c < n_cand;
-            const bool act = live && S.cc[c].n > 0;
+            const bool take = c < n_cand && sel(c);
             uint32_t tot;
-            const uint32_t ex = block_excl_scan(act ? 1u : 0u, sh, &tot);
-            if (act)
-                S.alist[n_act + ex] = c;
-            if (live)
-                S.color[c] = act ? 0xffffffffu : kColorIdle;
-            n_act += tot;
+            const uint32_t ex = block_excl_scan(take ? 1u : 0u, sh, &tot);
+            if (take)
+                out[n + ex] = c;
+            n += tot;
         }
         __syncthreads();
-        return n_act;
+        return n;
+    }
+
+    // The contacting candidates of the world into S.alist, in candidate
+    // order, their colours reset; the others marked idle.  Returns the count.
+    template <class T, class P, class Team>
+    __device__ uint32_t compact_active(const Team &tm, const Scr<T, P> &S, uint32_t n_cand, ScanShared &sh)
+    {
+        return team_compact(tm, n_cand, S.alist, sh, [&](uint32_t c) {
+            const bool act = S.cc[c].n > 0;
+            S.color[c] = act ? 0xffffffffu : kColorIdle;
+            return act;
+        });
+    }
+
+    // Substeps after the first of a step reuse the colouring: a candidate
+    // that is still contacting keeps its colour (a regular one), and goes to
+    // S.alist[0, *n_keep); the newly contacting ones (and those of the
+    // overflow colour) follow in candidate order with their colour reset;
+    // the rest are marked idle.  The kept candidates still share no dynamic
+    // body within a colour, so first-fit colouring of the new ones against
+    // the kept ones' body masks gives a valid colouring again.  Returns the
+    // total count.
+    template <class T, class P, class Team>
+    __device__ uint32_t compact_keep_active(const Team &tm, const Scr<T, P> &S, uint32_t n_cand, ScanShared &sh,
+                                            uint32_t *n_keep)
+    {
+        const uint32_t kept = team_compact(tm, n_cand, S.alist, sh, [&](uint32_t c) {
+            const bool act = S.cc[c].n > 0;
+            const uint32_t old = S.color[c];
+            const bool keep = act && old < kColorSerial;
+            S.color[c] = keep ? old : act ? 0xffffffffu : kColorIdle;
+            return keep;
+        });
+        const uint32_t fresh =
+            team_compact(tm, n_cand, S.alist + kept, sh, [&](uint32_t c) { return S.color[c] == 0xffffffffu; });
+        *n_keep = kept;
+        return kept + fresh;
     }
 
     // Greedy colouring of the world's contacting candidates: in candidate
@@ -1723,8 +1764,13 @@ namespace rbps_gpu
     // (kColorSerial once a body has used all 64).  The team leader colours
     // sequentially with the per-body colour masks in `mask` (shared memory
     // when the world fits); the team then buckets the candidates by colour
-    // (corder, colour offsets in misc).  Returns the number of regular
-    // colours to every thread.
+    // (corder, colour offsets in misc).  The first substep of a step colours
+    // every contacting candidate so; later substeps of the same step keep
+    // the colours of the candidates still contacting (their masks are set
+    // in parallel) and colour only the newly contacting ones first-fit
+    // against them, which on resting piles leaves the leader a few
+    // candidates instead of all.  Returns the number of regular colours to
+    // every thread.
     template <class T, class P, class Team>
     __device__ uint32_t greedy_color_world(const Engine<T, P> &E, const Team &tm, uint32_t w,
                                            unsigned long long *mask, ScanShared &sh, uint32_t *book,
@@ -1742,9 +1788,28 @@ namespace rbps_gpu
             mask[b] = 0ull;
         for (uint32_t k = tm.rank(); k < 66; k += tm.size())
             cnt[k] = 0u;
-        const uint32_t n_act = compact_active(tm, S, n_cand, sh);
-        tm.sync();
+        // after the first substep of a step the colouring of the same
+        // candidate list is reused: kept candidates first, then the new ones
+#ifndef RBPS_COLOR_REUSE
+#define RBPS_COLOR_REUSE 1
+#endif
+        const bool reuse = RBPS_COLOR_REUSE && misc[kMiscColorValid] != 0u;
+        uint32_t n_keep = 0;
+        const uint32_t n_act = reuse ? compact_keep_active(tm, S, n_cand, sh, &n_keep) : compact_active(tm, S, n_cand, sh);
         const uint8_t *type = E.B.type + W.body_off;
+        for (uint32_t q = tm.rank(); q < n_keep; q += tm.size())
+        {
+            const uint32_t c = S.alist[q];
+            const uint32_t col = S.color[c];
+            const Cand cd = S.cand[c];
+            const unsigned long long bit = 1ull << col;
+            if (type[cd.ba] == kDynamic)
+                atomicOr(&mask[cd.ba], bit);
+            if (type[cd.bb] == kDynamic)
+                atomicOr(&mask[cd.bb], bit);
+            atomicAdd(&cnt[col], 1u);
+        }
+        tm.sync();
         if (stage)
         {
             // Staged: the team loads a chunk of active candidates into shared
@@ -1754,7 +1819,7 @@ namespace rbps_gpu
             // memory only.
             uint8_t *scol = reinterpret_cast<uint8_t *>(stage + kColorStage);
             const uint32_t chunk = E.color_chunk; // <= kColorStage
-            for (uint32_t q0 = 0; q0 < n_act; q0 += chunk)
+            for (uint32_t q0 = n_keep; q0 < n_act; q0 += chunk)
             {
                 const uint32_t m = min(chunk, n_act - q0);
                 for (uint32_t k = tm.rank(); k < m; k += tm.size())
@@ -1793,7 +1858,7 @@ namespace rbps_gpu
         if (tm.leader())
         {
             constexpr uint32_t kAhead = 8; // candidates loaded ahead of the mask updates
-            for (uint32_t q0 = 0; q0 < (stage ? 0u : n_act); q0 += kAhead)
+            for (uint32_t q0 = n_keep; q0 < (stage ? 0u : n_act); q0 += kAhead)
             {
                 uint32_t cs[kAhead];
                 Cand cd[kAhead];
@@ -1840,6 +1905,7 @@ namespace rbps_gpu
             misc[kMiscNColors] = ncol;
             if (ncol > misc[kMiscMaxColors])
                 misc[kMiscMaxColors] = ncol;
+            misc[kMiscColorValid] = 1u;
             if (book)
                 book[132] = ncol;
         }

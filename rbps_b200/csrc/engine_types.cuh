@@ -107,6 +107,10 @@ namespace rbps_gpu
     constexpr uint32_t kMiscNColors = kMiscFlags + 1, kMiscNContacts = kMiscFlags + 2, kMiscNGjk = kMiscFlags + 3,
                        kMiscPairsRaw = kMiscFlags + 4, kMiscNPairs = kMiscFlags + 5, kMiscNCand = kMiscFlags + 6,
                        kMiscMaxColors = kMiscFlags + 7;
+    // 1 while S.color holds a colouring of the current candidate list (set by
+    // the colouring, cleared by the frame that rebuilds the list)
+    constexpr uint32_t kMiscColorValid = kMiscC2Off + 66;
+    static_assert(kMiscColorValid < kMiscWords, "misc words");
 
     RBPS_HD ScratchLayout make_layout(uint32_t nbp, uint32_t nb, uint32_t pair_cap, uint32_t npc, size_t cc_size)
     {
@@ -238,7 +242,6 @@ namespace rbps_gpu
         uint2 *gjk_list;
         uint32_t *gjk_count;
         uint32_t gjk_cap, gjk_slots;
-        void *gjk_ws;
         // RBPS_PRECISION_FP32_POS64: per-world origin (3 doubles a world) and
         // the world of every body; body positions are stored relative to it
         const double *origin;
@@ -322,16 +325,18 @@ namespace rbps_gpu
         double position[4][3];
         double depth[4];
     };
+    // one warp per pair, GJK / EPA workspaces in shared memory
     template <class T, class P>
     cudaError_t launch_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
-                               const HullSetDev &hulls, uint32_t n, CollideOut *out, void *gjk_ws, uint32_t threads,
-                               int *err, cudaStream_t stream);
-    // bytes of one GJK / EPA / manifold workspace in precision T
-    template <class T, class P>
-    size_t gjk_work_bytes();
-    // the GJK pass over the pairs the narrowphase queued (no-op without hulls)
+                               const HullSetDev &hulls, uint32_t n, CollideOut *out, int *err, cudaStream_t stream);
+    // the GJK pass over the pairs the narrowphase queued (no-op without
+    // hulls): Engine::gjk_slots CTAs, one warp per queued pair
     template <class T, class P>
     cudaError_t launch_gjk(const Engine<T, P> &e, cudaStream_t stream);
+    // opens the GJK pass kernel to its shared workspaces; *ctas receives the
+    // CTAs the device keeps resident at once
+    template <class T, class P>
+    cudaError_t prepare_gjk(int sm_count, uint32_t *ctas);
     template <class T, class P>
     cudaError_t launch_debug_broadphase(const Engine<T, P> &e, uint32_t world, int block, uint32_t *out,
                                         cudaStream_t stream);

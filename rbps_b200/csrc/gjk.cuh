@@ -17,8 +17,10 @@
 //     (Clipping.cpp:37-101) or the edge-edge closest points
 //     (Clipping.cpp:103-128); one EPA point otherwise; reduce_to_4
 //     (ContactManifoldGenerator.hpp:88-154).
-// The polytope, edge list and clipping buffers live in a per-thread
-// workspace in global memory (GjkWork), not on the stack.
+// One warp runs one pair: the scans over hull vertices, EPA faces and
+// horizon edges are split across its lanes, and the polytope, edge list and
+// clipping buffers live in the warp's shared-memory workspace (two views
+// of one region: the polytope while EPA runs, the clipping buffers after).
 #pragma once
 #include <cfloat>
 #include <cstdint>
@@ -65,19 +67,34 @@ namespace rbps_gpu
         uint8_t obsolete;
     };
 
-    // Per-thread workspace of one GJK / EPA / manifold evaluation.
+    // The clipping buffers of the hull-hull manifold alone: the second view
+    // of a warp's shared workspace, over the EPA polytope it no longer needs.
     template <class T>
-    struct GjkWork
+    struct GjkClipWork
     {
-        SVert<T> verts[kEpaMaxVerts];
-        EpaFace<T> faces[kEpaMaxFaces];
-        uint8_t edges[2 * kEpaMaxEdges];
         vec3<T> inc[kClipMaxPoly], ref[kClipMaxPoly];
         vec3<T> pl_n[kClipMaxPoly], pl_p[kClipMaxPoly];
         vec3<T> buf_a[kClipCap + 4], buf_b[kClipCap + 4];
         vec3<T> keep[kClipCap + 4];
         T keep_d[kClipCap + 4];
     };
+
+    // The EPA polytope of one warp's evaluation (first view of its workspace).
+    template <class T>
+    struct GjkEpaWork
+    {
+        SVert<T> verts[kEpaMaxVerts];
+        EpaFace<T> faces[kEpaMaxFaces];
+        uint8_t edges[2 * kEpaMaxEdges];
+    };
+
+    // Bytes of one warp's shared workspace: the two views overlap.
+    template <class T>
+    constexpr size_t gjk_warp_bytes()
+    {
+        return ((sizeof(GjkEpaWork<T>) > sizeof(GjkClipWork<T>) ? sizeof(GjkEpaWork<T>) : sizeof(GjkClipWork<T>)) +
+                15) / 16 * 16;
+    }
 
     // One convex shape in world space (shape_support, ShapeTypes.hpp:130-133,
     // through the transform as MinkowskiDiff::support_a/b, MinkowskiDiff.hpp).
@@ -137,6 +154,68 @@ namespace rbps_gpu
     __device__ __forceinline__ vec3<T> world_support(const ConvexShape<T> &c, const HullSetDev &hs, const vec3<T> &dir)
     {
         return c.t.transform_point(local_support(*c.s, hs, c.t.inverse_rotate_vector(dir)));
+    }
+
+    // ------------------------------------------------------------ one warp per pair
+    // In the warp forms below every lane of the warp runs the same control
+    // flow on the same values (scalar state is computed redundantly, so it
+    // is bit-identical on every lane); the loops over hull vertices, EPA
+    // faces, vertices and horizon edges are split across the lanes and
+    // joined by warp reductions that keep the serial scans' tie rules.
+    // Shared memory is written by one lane (or each lane its own entries)
+    // between __syncwarp()s.
+    constexpr unsigned kWarpAll = 0xffffffffu;
+
+    // Support of a hull: the first vertex (lowest index) of maximal dot
+    // product, as the serial scan's strict `>` keeps (ConvexHull.hpp:457-472);
+    // a NaN first dot keeps vertex 0 as the serial scan does.  Other shapes
+    // are closed forms, the same on every lane.
+    template <class T>
+    __device__ vec3<T> warp_local_support(const ShapeDev &s, const HullSetDev &hs, const vec3<T> &d)
+    {
+        if (s.kind != kHull)
+            return local_support(s, hs, d);
+        const uint32_t v0 = hs.v_off[s.hull], v1 = hs.v_off[s.hull + 1];
+        if (v1 == v0)
+            return vec3<T>();
+        const double *V = hs.verts;
+        const uint32_t lane = threadIdx.x & 31u;
+        T best_d = T(0);
+        uint32_t best_i = ~0u;
+        for (uint32_t i = v0 + lane; i < v1; i += 32)
+        {
+            const vec3<T> p{T(V[3 * i]), T(V[3 * i + 1]), T(V[3 * i + 2])};
+            const T dd = dot(p, d);
+            if (dd == dd && (best_i == ~0u || dd > best_d))
+            {
+                best_d = dd;
+                best_i = i;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const T od = __shfl_xor_sync(kWarpAll, best_d, o);
+            const uint32_t oi = __shfl_xor_sync(kWarpAll, best_i, o);
+            if (oi != ~0u && (best_i == ~0u || od > best_d || (od == best_d && oi < best_i)))
+            {
+                best_d = od;
+                best_i = oi;
+            }
+        }
+        const vec3<T> p0{T(V[3 * v0]), T(V[3 * v0 + 1]), T(V[3 * v0 + 2])};
+        const T d0 = dot(p0, d);
+        if (d0 != d0 || best_i == ~0u)
+            return p0;
+        return vec3<T>{T(V[3 * best_i]), T(V[3 * best_i + 1]), T(V[3 * best_i + 2])};
+    }
+
+    template <bool Warp, class T>
+    __device__ __forceinline__ vec3<T> support_of(const ConvexShape<T> &c, const HullSetDev &hs, const vec3<T> &dir)
+    {
+        if constexpr (Warp)
+            return c.t.transform_point(warp_local_support(*c.s, hs, c.t.inverse_rotate_vector(dir)));
+        else
+            return world_support(c, hs, dir);
     }
 
     // ------------------------------------------------------------ GJK
@@ -362,7 +441,8 @@ namespace rbps_gpu
         kGjkFailed = 2
     };
 
-    template <class T>
+    // Warp = true: every lane of a warp runs it (support_of the warp form).
+    template <class T, bool Warp = false>
     __device__ int gjk_evaluate(const ConvexShape<T> &A, const ConvexShape<T> &B, const HullSetDev &hs,
                                 const vec3<T> &guess, Simplex<T> &s)
     {
@@ -371,16 +451,16 @@ namespace rbps_gpu
             s.vi[i] = i;
         vec3<T> dir = length_sq(guess) > T(kEpsilon) ? guess : vec3<T>(T(1.0), T(0.0), T(0.0));
         SVert<T> v0;
-        v0.w0 = world_support(A, hs, dir);
-        v0.w1 = world_support(B, hs, -dir);
+        v0.w0 = support_of<Warp>(A, hs, dir);
+        v0.w1 = support_of<Warp>(B, hs, -dir);
         v0.w = v0.w0 - v0.w1;
         simplex_add(s, v0);
         dir = -v0.w;
         for (int it = 0; it < kGjkMaxIter; ++it)
         {
             SVert<T> nx;
-            nx.w0 = world_support(A, hs, dir);
-            nx.w1 = world_support(B, hs, -dir);
+            nx.w0 = support_of<Warp>(A, hs, dir);
+            nx.w1 = support_of<Warp>(B, hs, -dir);
             nx.w = nx.w0 - nx.w1;
             if (dot(nx.w, dir) < T(0.0))
                 return kGjkValid;
@@ -454,26 +534,6 @@ namespace rbps_gpu
         return true;
     }
 
-    // add_edge (EPA.cpp:71-84): cancels an edge present in either direction,
-    // keeping the order of the others.
-    __device__ __forceinline__ void epa_add_edge(uint8_t *E, int &ne, uint8_t a, uint8_t b)
-    {
-        for (int i = 0; i < ne; ++i)
-            if ((E[2 * i] == a && E[2 * i + 1] == b) || (E[2 * i] == b && E[2 * i + 1] == a))
-            {
-                for (int k = i; k + 1 < ne; ++k)
-                {
-                    E[2 * k] = E[2 * k + 2];
-                    E[2 * k + 1] = E[2 * k + 3];
-                }
-                --ne;
-                return;
-            }
-        E[2 * ne] = a;
-        E[2 * ne + 1] = b;
-        ++ne;
-    }
-
     template <class T>
     struct EpaResult
     {
@@ -481,155 +541,6 @@ namespace rbps_gpu
         T depth;
         vec3<T> contact;
     };
-
-    template <class T>
-    __device__ int epa_evaluate(const Simplex<T> &seed, const ConvexShape<T> &A, const ConvexShape<T> &B,
-                                const HullSetDev &hs, GjkWork<T> &ws, EpaResult<T> &out, int *err)
-    {
-        out.normal = vec3<T>(T(0), T(0), T(0));
-        out.depth = T(0.0);
-        out.contact = vec3<T>(T(0), T(0), T(0));
-        if (seed.rank != 4)
-            return kEpaNonLinear;
-        SVert<T> *V = ws.verts;
-        EpaFace<T> *F = ws.faces;
-        int nv = 0, nf = 0;
-        for (int i = 0; i < 4; ++i)
-            V[nv++] = seed.st[seed.vi[i]];
-        {
-            const vec3<T> va = V[0].w, vb = V[1].w, vc = V[2].w, vd = V[3].w;
-            const T e2 = T(kEpsilon) * T(kEpsilon);
-            vec3<T> pn = cross(vb - va, vc - va);
-            if (length_sq(pn) < e2)
-                pn = cross(vb - va, vd - va);
-            if (length_sq(pn) < e2)
-                pn = cross(vc - va, vd - va);
-            if (length_sq(pn) > e2)
-            {
-                pn = normalize(pn);
-                const T dist_d = rabs(dot(vd - va, pn));
-                if (dist_d < T(1e-5))
-                {
-                    const vec3<T> sp = world_support(A, hs, pn) - world_support(B, hs, -pn);
-                    const vec3<T> sn = world_support(A, hs, -pn) - world_support(B, hs, pn);
-                    const T dist_pos = dot(sp - va, pn);
-                    const T dist_neg = dot(sn - va, -pn);
-                    if (dist_pos < T(1e-4) || dist_neg < T(1e-4))
-                    {
-                        out.normal = (dist_pos <= dist_neg) ? pn : -pn;
-                        out.depth = T(0.0);
-                        out.contact = (V[0].w0 + V[1].w0 + V[2].w0 + V[3].w0) * T(0.25);
-                        return kEpaValid;
-                    }
-                }
-            }
-        }
-        // initial tetrahedron faces: (A,B,C), (A,C,D), (A,D,B), (B,C,D)
-        const uint8_t init[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 2, 3}};
-        for (int k = 0; k < 4; ++k)
-        {
-            EpaFace<T> &f = F[nf];
-            f.v[0] = init[k][0];
-            f.v[1] = init[k][1];
-            f.v[2] = init[k][2];
-            f.obsolete = 0;
-            if (!epa_face_normal(f, V, nv))
-                return kEpaNonLinear;
-            ++nf;
-        }
-        int ne = 0;
-        for (int it = 0; it < kEpaMaxIter; ++it)
-        {
-            int ci = -1;
-            T min_d = big_value<T>();
-            for (int i = 0; i < nf; ++i)
-            {
-                if (F[i].obsolete)
-                    continue;
-                if (F[i].d < min_d)
-                {
-                    min_d = F[i].d;
-                    ci = i;
-                }
-            }
-            if (ci < 0)
-                return kEpaFailed;
-            const EpaFace<T> cf = F[ci];
-            const vec3<T> dir = cf.n;
-            SVert<T> w;
-            w.w0 = world_support(A, hs, dir);
-            w.w1 = world_support(B, hs, -dir);
-            w.w = w.w0 - w.w1;
-            const T d_proj = dot(w.w, dir);
-            if (d_proj - min_d < T(1e-6))
-            {
-                out.normal = cf.n;
-                out.depth = min_d;
-                const vec3<T> q = cf.n * min_d;
-                const vec3<T> p0 = V[cf.v[0]].w, p1 = V[cf.v[1]].w, p2 = V[cf.v[2]].w;
-                const vec3<T> e0 = p1 - p0, e1 = p2 - p0, r = q - p0;
-                const T d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
-                const T d20 = dot(r, e0), d21 = dot(r, e1);
-                const T denom = d00 * d11 - d01 * d01;
-                if (rabs(denom) < T(kEpsilon))
-                    out.contact = V[cf.v[0]].w0;
-                else
-                {
-                    const T v_w = (d11 * d20 - d01 * d21) / denom;
-                    const T w_w = (d00 * d21 - d01 * d20) / denom;
-                    const T u_w = T(1.0) - v_w - w_w;
-                    out.contact = V[cf.v[0]].w0 * u_w + V[cf.v[1]].w0 * v_w + V[cf.v[2]].w0 * w_w;
-                }
-                return kEpaValid;
-            }
-            for (int i = 0; i < nv; ++i)
-                if (length_sq(V[i].w - w.w) < T(kEpsilon) * T(kEpsilon))
-                {
-                    out.normal = cf.n;
-                    out.depth = min_d;
-                    out.contact = V[cf.v[0]].w0;
-                    return kEpaValid;
-                }
-            if (nv >= kEpaMaxVerts)
-                return kEpaOutOfVertices;
-            const uint8_t wi = (uint8_t)nv;
-            V[nv++] = w;
-            ne = 0;
-            for (int i = 0; i < nf; ++i)
-            {
-                EpaFace<T> &f = F[i];
-                if (f.obsolete)
-                    continue;
-                const vec3<T> centroid = (V[f.v[0]].w + V[f.v[1]].w + V[f.v[2]].w) * (T(1.0) / T(3.0));
-                if (dot(f.n, w.w - centroid) > T(0.0))
-                {
-                    f.obsolete = 1;
-                    if (ne + 3 > kEpaMaxEdges)
-                    {
-                        set_gjk_error(err, 1);
-                        return kEpaFailed;
-                    }
-                    epa_add_edge(ws.edges, ne, f.v[0], f.v[1]);
-                    epa_add_edge(ws.edges, ne, f.v[1], f.v[2]);
-                    epa_add_edge(ws.edges, ne, f.v[2], f.v[0]);
-                }
-            }
-            for (int e = 0; e < ne; ++e)
-            {
-                if (nf >= kEpaMaxFaces)
-                    return kEpaOutOfFaces;
-                EpaFace<T> &nfc = F[nf];
-                nfc.v[0] = ws.edges[2 * e];
-                nfc.v[1] = ws.edges[2 * e + 1];
-                nfc.v[2] = wi;
-                nfc.obsolete = 0;
-                if (!epa_face_normal(nfc, V, nv))
-                    continue;
-                ++nf;
-            }
-        }
-        return kEpaFailed;
-    }
 
     // ------------------------------------------------------------ manifold
     template <class T>
@@ -946,9 +857,11 @@ namespace rbps_gpu
 
     // manifold_convex_convex (ContactManifoldGenerator.cpp:176-379) for two
     // hulls with polygon tables.
-    template <class T>
+    // WS: the clipping buffers (GjkClipWork, the second view of a warp's
+    // shared workspace).
+    template <class T, class WS>
     __device__ void manifold_hull_hull(const EpaResult<T> &r, const HullSetDev &hs, uint32_t ha, const tf<T> &ta,
-                                       uint32_t hb, const tf<T> &tb, GjkWork<T> &ws, Manifold<T> &m, int *err)
+                                       uint32_t hb, const tf<T> &tb, WS &ws, Manifold<T> &m, int *err)
     {
         m.normal = r.normal;
         m.n = 0;
@@ -1052,30 +965,290 @@ namespace rbps_gpu
         m.n = reduce_to_4(ws.keep, ws.keep_d, n_keep, m);
     }
 
-    // gjk_epa_manifold (ContactManifoldGenerator.cpp:415-440) with
-    // generate_manifold (:382-413): true when the shapes overlap.
+    // ------------------------------------------------------------ EPA on a warp
+    // add_edge (EPA.cpp:71-84) on a warp: the first stored edge equal to
+    // (a, b) in either direction is found by a ballot over 32 entries at a
+    // time and erased with the later entries moved down in order; otherwise
+    // (a, b) is appended.  Every lane calls it with the same arguments.
+    __device__ __forceinline__ void warp_add_edge(uint8_t *E, int &ne, uint8_t a, uint8_t b)
+    {
+        const int lane = (int)(threadIdx.x & 31u);
+        int hit = -1;
+        for (int base = 0; base < ne && hit < 0; base += 32)
+        {
+            const int i = base + lane;
+            const bool match = i < ne && ((E[2 * i] == a && E[2 * i + 1] == b) || (E[2 * i] == b && E[2 * i + 1] == a));
+            const unsigned m = __ballot_sync(kWarpAll, match);
+            if (m)
+                hit = base + __ffs(m) - 1;
+        }
+        if (hit >= 0)
+        {
+            for (int base = hit; base + 1 < ne; base += 32)
+            {
+                const int k = base + lane;
+                uint8_t x0 = 0, x1 = 0;
+                if (k + 1 < ne)
+                {
+                    x0 = E[2 * k + 2];
+                    x1 = E[2 * k + 3];
+                }
+                __syncwarp();
+                if (k + 1 < ne)
+                {
+                    E[2 * k] = x0;
+                    E[2 * k + 1] = x1;
+                }
+                __syncwarp();
+            }
+            --ne;
+        }
+        else
+        {
+            if (lane == 0)
+            {
+                E[2 * ne] = a;
+                E[2 * ne + 1] = b;
+            }
+            ++ne;
+        }
+        __syncwarp();
+    }
+
+    // epa_evaluate on one warp, the polytope in the warp's shared workspace.
+    // The same steps in the same order as the serial form (EPA.cpp:141-378):
+    // the nearest live face is a warp argmin keeping the lowest index on
+    // ties (the serial scan's strict `<`); the faces that see the new vertex
+    // are tested 32 at a time and their edges added in face order; the new
+    // faces are built 32 at a time and packed in edge order, a degenerate
+    // one leaving no slot, with OutOfFaces where the serial loop would meet
+    // 256 faces.  Every lane returns the same result.
     template <class T>
-    __device__ bool gjk_epa_manifold(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &sb, const tf<T> &tb,
-                                     const HullSetDev &hs, GjkWork<T> &ws, Manifold<T> &m, int *err)
+    __device__ int epa_evaluate_warp(const Simplex<T> &seed, const ConvexShape<T> &A, const ConvexShape<T> &B,
+                                     const HullSetDev &hs, GjkEpaWork<T> &ws, EpaResult<T> &out, int *err)
+    {
+        const uint32_t lane = threadIdx.x & 31u;
+        out.normal = vec3<T>(T(0), T(0), T(0));
+        out.depth = T(0.0);
+        out.contact = vec3<T>(T(0), T(0), T(0));
+        if (seed.rank != 4)
+            return kEpaNonLinear;
+        SVert<T> *V = ws.verts;
+        EpaFace<T> *F = ws.faces;
+        __syncwarp();
+        if (lane == 0)
+            for (int i = 0; i < 4; ++i)
+                V[i] = seed.st[seed.vi[i]];
+        __syncwarp();
+        int nv = 4, nf = 0;
+        {
+            const vec3<T> va = V[0].w, vb = V[1].w, vc = V[2].w, vd = V[3].w;
+            const T e2 = T(kEpsilon) * T(kEpsilon);
+            vec3<T> pn = cross(vb - va, vc - va);
+            if (length_sq(pn) < e2)
+                pn = cross(vb - va, vd - va);
+            if (length_sq(pn) < e2)
+                pn = cross(vc - va, vd - va);
+            if (length_sq(pn) > e2)
+            {
+                pn = normalize(pn);
+                const T dist_d = rabs(dot(vd - va, pn));
+                if (dist_d < T(1e-5))
+                {
+                    const vec3<T> sp = support_of<true>(A, hs, pn) - support_of<true>(B, hs, -pn);
+                    const vec3<T> sn = support_of<true>(A, hs, -pn) - support_of<true>(B, hs, pn);
+                    const T dist_pos = dot(sp - va, pn);
+                    const T dist_neg = dot(sn - va, -pn);
+                    if (dist_pos < T(1e-4) || dist_neg < T(1e-4))
+                    {
+                        out.normal = (dist_pos <= dist_neg) ? pn : -pn;
+                        out.depth = T(0.0);
+                        out.contact = (V[0].w0 + V[1].w0 + V[2].w0 + V[3].w0) * T(0.25);
+                        return kEpaValid;
+                    }
+                }
+            }
+        }
+        {
+            // initial tetrahedron faces (A,B,C), (A,C,D), (A,D,B), (B,C,D): lane k builds face k
+            const uint8_t init[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 2, 3}};
+            EpaFace<T> f;
+            bool ok = true;
+            if (lane < 4)
+            {
+                f.v[0] = init[lane][0];
+                f.v[1] = init[lane][1];
+                f.v[2] = init[lane][2];
+                f.obsolete = 0;
+                ok = epa_face_normal(f, V, nv);
+            }
+            if (__ballot_sync(kWarpAll, !ok))
+                return kEpaNonLinear;
+            if (lane < 4)
+                F[lane] = f;
+            nf = 4;
+            __syncwarp();
+        }
+        int ne = 0;
+        for (int it = 0; it < kEpaMaxIter; ++it)
+        {
+            T min_d = big_value<T>();
+            int ci = -1;
+            for (int i = (int)lane; i < nf; i += 32)
+                if (!F[i].obsolete && F[i].d < min_d)
+                {
+                    min_d = F[i].d;
+                    ci = i;
+                }
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                const T od = __shfl_xor_sync(kWarpAll, min_d, o);
+                const int oi = __shfl_xor_sync(kWarpAll, ci, o);
+                if (oi >= 0 && (ci < 0 || od < min_d || (od == min_d && oi < ci)))
+                {
+                    min_d = od;
+                    ci = oi;
+                }
+            }
+            if (ci < 0)
+                return kEpaFailed;
+            const EpaFace<T> cf = F[ci];
+            const vec3<T> dir = cf.n;
+            SVert<T> w;
+            w.w0 = support_of<true>(A, hs, dir);
+            w.w1 = support_of<true>(B, hs, -dir);
+            w.w = w.w0 - w.w1;
+            const T d_proj = dot(w.w, dir);
+            if (d_proj - min_d < T(1e-6))
+            {
+                out.normal = cf.n;
+                out.depth = min_d;
+                const vec3<T> q = cf.n * min_d;
+                const vec3<T> p0 = V[cf.v[0]].w, p1 = V[cf.v[1]].w, p2 = V[cf.v[2]].w;
+                const vec3<T> e0 = p1 - p0, e1 = p2 - p0, r = q - p0;
+                const T d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1);
+                const T d20 = dot(r, e0), d21 = dot(r, e1);
+                const T denom = d00 * d11 - d01 * d01;
+                if (rabs(denom) < T(kEpsilon))
+                    out.contact = V[cf.v[0]].w0;
+                else
+                {
+                    const T v_w = (d11 * d20 - d01 * d21) / denom;
+                    const T w_w = (d00 * d21 - d01 * d20) / denom;
+                    const T u_w = T(1.0) - v_w - w_w;
+                    out.contact = V[cf.v[0]].w0 * u_w + V[cf.v[1]].w0 * v_w + V[cf.v[2]].w0 * w_w;
+                }
+                return kEpaValid;
+            }
+            bool dup = false;
+            for (int i = (int)lane; i < nv; i += 32)
+                dup = dup || length_sq(V[i].w - w.w) < T(kEpsilon) * T(kEpsilon);
+            if (__any_sync(kWarpAll, dup))
+            {
+                out.normal = cf.n;
+                out.depth = min_d;
+                out.contact = V[cf.v[0]].w0;
+                return kEpaValid;
+            }
+            if (nv >= kEpaMaxVerts)
+                return kEpaOutOfVertices;
+            const uint8_t wi = (uint8_t)nv;
+            if (lane == 0)
+                V[nv] = w;
+            ++nv;
+            __syncwarp();
+            // the horizon: faces that see w, their edges in face order
+            ne = 0;
+            for (int base = 0; base < nf; base += 32)
+            {
+                const int i = base + (int)lane;
+                bool vis = false;
+                if (i < nf && !F[i].obsolete)
+                {
+                    const EpaFace<T> &f = F[i];
+                    const vec3<T> centroid = (V[f.v[0]].w + V[f.v[1]].w + V[f.v[2]].w) * (T(1.0) / T(3.0));
+                    vis = dot(f.n, w.w - centroid) > T(0.0);
+                }
+                unsigned m = __ballot_sync(kWarpAll, vis);
+                if (vis)
+                    F[i].obsolete = 1;
+                while (m)
+                {
+                    const int fi = base + __ffs(m) - 1;
+                    m &= m - 1;
+                    if (ne + 3 > kEpaMaxEdges)
+                    {
+                        if (lane == 0)
+                            set_gjk_error(err, 1);
+                        return kEpaFailed;
+                    }
+                    const uint8_t a = F[fi].v[0], b = F[fi].v[1], c = F[fi].v[2];
+                    warp_add_edge(ws.edges, ne, a, b);
+                    warp_add_edge(ws.edges, ne, b, c);
+                    warp_add_edge(ws.edges, ne, c, a);
+                }
+            }
+            __syncwarp();
+            // new faces on the horizon edges, packed in edge order
+            for (int base = 0; base < ne; base += 32)
+            {
+                const int e = base + (int)lane;
+                EpaFace<T> f;
+                bool ok = false;
+                if (e < ne)
+                {
+                    f.v[0] = ws.edges[2 * e];
+                    f.v[1] = ws.edges[2 * e + 1];
+                    f.v[2] = wi;
+                    f.obsolete = 0;
+                    ok = epa_face_normal(f, V, nv);
+                }
+                const unsigned okm = __ballot_sync(kWarpAll, ok);
+                const int before = nf + __popc(okm & ((1u << lane) - 1u));
+                if (__any_sync(kWarpAll, e < ne && before >= kEpaMaxFaces))
+                    return kEpaOutOfFaces;
+                if (ok)
+                    F[before] = f;
+                nf += __popc(okm);
+            }
+            __syncwarp();
+        }
+        return kEpaFailed;
+    }
+
+    // gjk_epa_manifold on one warp: every lane calls it with the same pair
+    // and `ws` the warp's shared workspace (gjk_warp_bytes<T>()).  The
+    // return value is the same on every lane; the manifold is complete on
+    // lane 0 (a hull-hull manifold is clipped by lane 0 alone, in the
+    // workspace's second view).
+    template <class T>
+    __device__ bool gjk_epa_manifold_warp(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &sb, const tf<T> &tb,
+                                          const HullSetDev &hs, unsigned char *ws, Manifold<T> &m, int *err)
     {
         const ConvexShape<T> A{&sa, ta}, B{&sb, tb};
         vec3<T> guess = tb.pos - ta.pos;
         if (length_sq(guess) < T(kEpsilon))
             guess = vec3<T>(T(1.0), T(0.0), T(0.0));
         Simplex<T> s;
-        if (gjk_evaluate(A, B, hs, guess, s) != kGjkInside)
+        if (gjk_evaluate<T, true>(A, B, hs, guess, s) != kGjkInside)
             return false;
         EpaResult<T> r;
-        if (epa_evaluate(s, A, B, hs, ws, r, err) != kEpaValid)
+        if (epa_evaluate_warp(s, A, B, hs, *reinterpret_cast<GjkEpaWork<T> *>(ws), r, err) != kEpaValid)
             return false;
         m.normal = r.normal;
         m.n = 0;
         const bool adj_a = sa.kind == kHull && hs.desc[sa.hull].np > 0;
         const bool adj_b = sb.kind == kHull && hs.desc[sb.hull].np > 0;
+        __syncwarp(); // the polytope is dead: the clipping view may overwrite it
         if (adj_a && adj_b)
-            manifold_hull_hull(r, hs, (uint32_t)sa.hull, ta, (uint32_t)sb.hull, tb, ws, m, err);
+        {
+            if ((threadIdx.x & 31u) == 0)
+                manifold_hull_hull(r, hs, (uint32_t)sa.hull, ta, (uint32_t)sb.hull, tb,
+                                   *reinterpret_cast<GjkClipWork<T> *>(ws), m, err);
+        }
         else
             single_point(m, r.normal, r.contact, r.depth);
+        __syncwarp();
         return true;
     }
 } // namespace rbps_gpu

@@ -9,19 +9,33 @@
 
 namespace rbps_gpu
 {
-    // The queued GJK pairs of this substep, one per thread, each thread on
-    // its own workspace (gridDim * blockDim <= gjk_slots).
-    template <class T, class P>
-    __global__ void __launch_bounds__(128) k_gjk(const Engine<T, P> E)
+    // Warps per CTA of the GJK kernels; each warp owns gjk_warp_bytes of the
+    // CTA's dynamic shared memory.
+    constexpr int kGjkWarps = 4;
+    constexpr size_t kGjkWarpBytes = gjk_warp_bytes<double>();
+    constexpr size_t kGjkSmem = kGjkWarps * kGjkWarpBytes;
+
+    // Opens a GJK kernel to its shared workspaces (once per device and kernel).
+    template <class K>
+    cudaError_t gjk_smem_attr(K kernel)
     {
-        const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-        const uint32_t nth = gridDim.x * blockDim.x;
+        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjkSmem);
+    }
+
+    // The queued GJK pairs of this substep, one warp per pair, the warp's
+    // polytope and clipping buffers in shared memory.
+    template <class T, class P>
+    __global__ void __launch_bounds__(kGjkWarps * 32) k_gjk(const Engine<T, P> E)
+    {
+        extern __shared__ __align__(16) unsigned char gjk_smem[];
+        unsigned char *ws = gjk_smem + (threadIdx.x >> 5) * kGjkWarpBytes;
+        const uint32_t warp = blockIdx.x * kGjkWarps + (threadIdx.x >> 5);
+        const uint32_t n_warps = gridDim.x * kGjkWarps;
         const uint32_t n = min(*E.gjk_count, E.gjk_cap);
-        GjkWork<double> &ws = reinterpret_cast<GjkWork<double> *>(E.gjk_ws)[tid];
-        for (uint32_t i = tid; i < n; i += nth)
+        for (uint32_t i = warp; i < n; i += n_warps)
         {
             const uint2 e = E.gjk_list[i];
-            gjk_candidate(E, e.x, e.y, ws);
+            gjk_candidate_warp(E, e.x, e.y, ws);
         }
     }
 
@@ -30,15 +44,31 @@ namespace rbps_gpu
     {
         if (!e.gjk_list)
             return cudaSuccess;
-        k_gjk<T, P><<<e.gjk_slots / 128, 128, 0, stream>>>(e);
+        k_gjk<T, P><<<e.gjk_slots, kGjkWarps * 32, kGjkSmem, stream>>>(e);
         return cudaGetLastError();
     }
 
-    // rbc::dispatch (Dispatcher.hpp:208-213) on independent shape pairs, one
-    // thread per pair; transforms are 7 doubles (position, quaternion wxyz).
+    // Sizes the GJK pass: CTAs of kGjkWarps warps that the device keeps
+    // resident at once (the grid loops over the queued pairs).
     template <class T, class P>
-    __device__ void collide_one(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
-                                const HullSetDev &hulls, uint32_t i, CollideOut *out, GjkWork<double> &ws, int *err)
+    cudaError_t prepare_gjk(int sm_count, uint32_t *ctas)
+    {
+        cudaError_t rc = gjk_smem_attr(k_gjk<T, P>);
+        int per_sm = 0;
+        if (rc == cudaSuccess)
+            rc = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gjk<T, P>, kGjkWarps * 32, kGjkSmem);
+        *ctas = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sm_count;
+        return rc;
+    }
+
+    // rbc::dispatch (Dispatcher.hpp:208-213) on independent shape pairs, one
+    // warp per pair: every lane runs the analytic routines alike (the same
+    // result on every lane) and, for a pair without one, GJK / EPA / the
+    // manifold together on the warp's shared workspace; lane 0 writes the
+    // result.  Transforms are 7 doubles (position, quaternion wxyz).
+    template <class T, class P>
+    __device__ void collide_one_warp(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
+                                     const HullSetDev &hulls, uint32_t i, CollideOut *out, unsigned char *ws, int *err)
     {
         auto load_tf_d = [](const double *p) {
             tf<double> t;
@@ -61,10 +91,12 @@ namespace rbps_gpu
             const tf<double> ad = load_tf_d(ta + 7 * (size_t)i), bd = load_tf_d(tb + 7 * (size_t)i);
             Manifold<double> md;
             md.n = 0;
-            const bool hit = gjk_epa_manifold(sa[i], ad, sb[i], bd, hulls, ws, md, err);
+            const bool hit = gjk_epa_manifold_warp(sa[i], ad, sb[i], bd, hulls, ws, md, err);
             m = manifold_cast<T>(md);
             res = hit ? kHit : kMiss;
         }
+        if ((threadIdx.x & 31u) != 0)
+            return;
         CollideOut o;
         o.status = res;
         o.n_points = res == kHit ? m.n : 0;
@@ -91,28 +123,29 @@ namespace rbps_gpu
     }
 
     template <class T, class P>
-    __global__ void k_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
-                              const HullSetDev hulls, uint32_t n, CollideOut *out, void *gjk_ws, int *err)
+    __global__ void __launch_bounds__(kGjkWarps * 32) k_collide(const ShapeDev *sa, const double *ta,
+                                                                 const ShapeDev *sb, const double *tb,
+                                                                 const HullSetDev hulls, uint32_t n, CollideOut *out,
+                                                                 int *err)
     {
-        const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-        for (uint32_t i = tid; i < n; i += gridDim.x * blockDim.x)
-            collide_one<T, P>(sa, ta, sb, tb, hulls, i, out, reinterpret_cast<GjkWork<double> *>(gjk_ws)[tid], err);
+        extern __shared__ __align__(16) unsigned char gjk_smem[];
+        unsigned char *ws = gjk_smem + (threadIdx.x >> 5) * kGjkWarpBytes;
+        const uint32_t warp = blockIdx.x * kGjkWarps + (threadIdx.x >> 5);
+        for (uint32_t i = warp; i < n; i += gridDim.x * kGjkWarps)
+            collide_one_warp<T, P>(sa, ta, sb, tb, hulls, i, out, ws, err);
     }
 
-    template <class T, class P>
-    size_t gjk_work_bytes()
-    {
-        return sizeof(GjkWork<double>);
-    }
-
-    // threads = workspaces in gjk_ws (a multiple of 128)
     template <class T, class P>
     cudaError_t launch_collide(const ShapeDev *sa, const double *ta, const ShapeDev *sb, const double *tb,
-                               const HullSetDev &hulls, uint32_t n, CollideOut *out, void *gjk_ws, uint32_t threads,
-                               int *err, cudaStream_t stream)
+                               const HullSetDev &hulls, uint32_t n, CollideOut *out, int *err, cudaStream_t stream)
     {
-        if (n)
-            k_collide<T, P><<<threads / 128, 128, 0, stream>>>(sa, ta, sb, tb, hulls, n, out, gjk_ws, err);
+        if (!n)
+            return cudaSuccess;
+        cudaError_t rc = gjk_smem_attr(k_collide<T, P>);
+        if (rc != cudaSuccess)
+            return rc;
+        const uint32_t ctas = (uint32_t)std::min<size_t>(((size_t)n + kGjkWarps - 1) / kGjkWarps, 4096);
+        k_collide<T, P><<<ctas, kGjkWarps * 32, kGjkSmem, stream>>>(sa, ta, sb, tb, hulls, n, out, err);
         return cudaGetLastError();
     }
 } // namespace rbps_gpu
@@ -122,6 +155,5 @@ namespace rbps_gpu
     template cudaError_t rbps_gpu::launch_collide<T, P>(const rbps_gpu::ShapeDev *, const double *,               \
                                                        const rbps_gpu::ShapeDev *, const double *,               \
                                                        const rbps_gpu::HullSetDev &, uint32_t,                   \
-                                                       rbps_gpu::CollideOut *, void *, uint32_t, int *,          \
-                                                       cudaStream_t);                                            \
-    template size_t rbps_gpu::gjk_work_bytes<T, P>();
+                                                       rbps_gpu::CollideOut *, int *, cudaStream_t);             \
+    template cudaError_t rbps_gpu::prepare_gjk<T, P>(int, uint32_t *);

@@ -14,8 +14,9 @@ substeps), through the C ABI.
   the problem's conditioning: the FP32 reference-order error, over the
   bodies outside each world's jointed component, stays within a small
   factor of the error FP64 itself makes from the same state moved by one
-  float32 ulp per coordinate, and nearly every body is within 1e-5 (about
-  as many as in that moved FP64 run).
+  float32 ulp per coordinate (the largest of three draws of the signs), and
+  nearly every body is within 1e-5 (about as many as in those moved FP64
+  runs).
 - Colored FP32 over 60 steps from the settled state: energy and momentum
   change, deepest contact and joint attachment gaps stay close to FP64
   reference order's.
@@ -90,8 +91,12 @@ def test_fp32_settled_error_within_float_conditioning(rbps):
     settled = scenes.with_state(sub, st0)
     base, c64 = _run(rbps, settled, abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER, dump=True)
     f32, _ = _run(rbps, settled, abi.PRECISION_FP32, abi.SOLVE_REFERENCE_ORDER)
-    pert = scenes.with_state(settled, [M.perturb_ulp(s) for s in st0])
-    ulp, _ = _run(rbps, pert, abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER)
+    # FP64 from the state moved by one float ulp per coordinate, three draws
+    # of the signs: the conditioning baseline is the largest of the three
+    ulps = []
+    for seed in range(3):
+        pert = scenes.with_state(settled, [M.perturb_ulp(s, seed=seed) for s in st0])
+        ulps.append(_run(rbps, pert, abi.PRECISION_FP64, abi.SOLVE_REFERENCE_ORDER)[0])
     e32, eulp, within, within_ulp, total = [], [], 0, 0, 0
     for w in range(len(sub.worlds)):
         if not np.isfinite(base[w]["position"]).all():
@@ -99,7 +104,7 @@ def test_fp32_settled_error_within_float_conditioning(rbps):
         keep = np.ones(len(st0[w]["position"]), bool)
         keep[M.jointed_component(settled.worlds[w], c64[w])] = False
         a = M.state_error(f32[w], base[w])[keep]
-        u = M.state_error(ulp[w], base[w])[keep]
+        u = np.max([M.state_error(ulp[w], base[w])[keep] for ulp in ulps], axis=0)
         if len(a):
             e32.append(a.max())
             eulp.append(u.max())
@@ -108,8 +113,8 @@ def test_fp32_settled_error_within_float_conditioning(rbps):
             total += len(a)
     e32, eulp = np.array(e32), np.array(eulp)
     assert len(e32) >= 60
-    assert np.median(e32) <= 4.0 * np.median(eulp), (np.median(e32), np.median(eulp))
-    assert np.percentile(e32, 90) <= 4.0 * np.percentile(eulp, 90), (np.percentile(e32, 90),
+    assert np.median(e32) <= 3.0 * np.median(eulp), (np.median(e32), np.median(eulp))
+    assert np.percentile(e32, 90) <= 5.0 * np.percentile(eulp, 90), (np.percentile(e32, 90),
                                                                       np.percentile(eulp, 90))
     # nearly every body within 1e-5, about as many as FP64 from the moved state
     assert within / total >= 0.95, within / total
