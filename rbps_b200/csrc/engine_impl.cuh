@@ -120,6 +120,67 @@ namespace rbps_gpu
         return t;
     }
 
+    // Radius of a sphere about the collider's origin that holds the shape;
+    // 0 for the unbounded or table-driven kinds (plane, heightmap, mesh).
+    template <class T>
+    __device__ __forceinline__ T shape_bound(const ShapeDev &s, const HullSetDev &hs)
+    {
+        const T a = T(s.p[0]), b = T(s.p[1]), c = T(s.p[2]);
+        switch (s.kind)
+        {
+        case kSphere: return a;
+        case kBox: return sqrt(a * a + b * b + c * c);
+        case kCapsule: return a + b;
+        case kEllipsoid: return rmax(a, rmax(b, c));
+        case kCylinder:
+        case kCone: return sqrt(a * a + b * b);
+        case kHull:
+        {
+            const double *la = hs.local_aabb + 6 * s.hull;
+            const T x = rmax(rabs(T(la[0])), rabs(T(la[3]))), y = rmax(rabs(T(la[1])), rabs(T(la[4])));
+            const T z = rmax(rabs(T(la[2])), rabs(T(la[5])));
+            return sqrt(x * x + y * y + z * z);
+        }
+        default: return T(0);
+        }
+    }
+
+    // True when the two shapes are certainly apart: their bounding spheres
+    // (or a bounding sphere and a plane) are separated by more than
+    // kBoundMargin, far beyond any contact tolerance of the narrowphase
+    // (the largest is the 1e-4 of the box-plane corner test), so GJK would
+    // report no contact.  The test only skips work: the contact rows are the
+    // same (none), bit for bit.
+    constexpr double kBoundMargin = 1e-2;
+
+    template <class T>
+    __device__ __forceinline__ bool bounds_separate(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &sb,
+                                                    const tf<T> &tb, const HullSetDev &hs)
+    {
+        if (sa.kind == kPlane || sb.kind == kPlane)
+        {
+            const bool a_plane = sa.kind == kPlane;
+            const ShapeDev &pl = a_plane ? sa : sb;
+            const ShapeDev &ot = a_plane ? sb : sa;
+            const tf<T> &tp = a_plane ? ta : tb;
+            const tf<T> &to = a_plane ? tb : ta;
+            const T r = shape_bound<T>(ot, hs);
+            if (!(r > T(0)))
+                return false;
+            const vec3<T> n = rotate(tp.rot, vec3<T>(T(pl.p[0]), T(pl.p[1]), T(pl.p[2])));
+            const T len = length(n);
+            if (!(len > T(0.5)))
+                return false;
+            const T dist = dot(n, to.pos - tp.pos) / len - T(pl.p[3]);
+            return dist > r + T(kBoundMargin);
+        }
+        const T ra = shape_bound<T>(sa, hs), rb = shape_bound<T>(sb, hs);
+        if (!(ra > T(0)) || !(rb > T(0)))
+            return false;
+        const T reach = ra + rb + T(kBoundMargin);
+        return length_sq(ta.pos - tb.pos) > reach * reach;
+    }
+
     template <class T, class P>
     __device__ __forceinline__ tf<double> collider_tf_d(const Engine<T, P> &E, uint32_t gc, uint32_t gb)
     {
@@ -781,7 +842,13 @@ namespace rbps_gpu
         const tf<T> tb = collider_tf(E, gcb, gbb);
         Manifold<T> m;
         m.n = 0;
-        const int res = dispatch_pair<T, Sel>(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, m);
+        int res = dispatch_pair<T, Sel>(E.shape[gca], ta, E.shape[gcb], tb, E.hulls, m);
+        // a pair for the GJK pass whose bounding spheres are apart stays out
+        // of the queue (GJK would find it apart); the analytic routines exit
+        // early on their own, and the same test in front of them measured
+        // slower on the batched workload
+        if (res == kNeedsGjk && bounds_separate(E.shape[gca], ta, E.shape[gcb], tb, E.hulls))
+            res = kMiss;
         emit_manifold(E, gca, gcb, gba, gbb, m, res == kHit ? m.n : 0, out);
         return res;
     }
