@@ -362,14 +362,16 @@ typedef struct rbps_tune_result {
     uint32_t team_bodies;         /* worlds this large step on a whole CTA     */
     uint32_t narrow_per_warp;     /* narrowphase candidates a warp takes per pass */
     uint32_t color_chunk;         /* active candidates coloured per staged batch  */
+    uint32_t pair_bodies;         /* worlds this large (below team_bodies) step on half a CTA */
+    uint32_t pad_;
 } rbps_tune_result;
 
 /* Project autotuner (no reference counterpart; the batched design picks its
  * launch shapes by measurement): times `trial_steps` steps of the batch's
  * own worlds under each candidate configuration -- frame kernel at 128 or
  * 256 threads, narrowphase grid at 1/2, 1 or 2 times its occupancy bound,
- * then the body count from which a world steps on a whole CTA instead of a
- * warp (64 to 192), then the narrowphase candidates a warp takes per pass
+ * then the body counts from which a world steps on a whole CTA or on half
+ * a CTA instead of a warp, then the narrowphase candidates a warp takes per pass
  * (32 to 256) and the colouring's batch of staged candidates (64 to 256) --
  * from the same device snapshot, keeps the fastest and rewinds the batch to
  * the snapshot, so the state is as before the call.  The configuration
@@ -379,7 +381,8 @@ RBPS_API int rbps_batch_autotune(rbps_batch *batch, int32_t trial_steps, rbps_tu
 /* Applies a launch configuration without timing anything (no reference
  * counterpart): e.g. one rbps_batch_autotune chose for a batch of the same
  * worlds earlier.  Fields frame_block (128 or 256), narrow_grid, team_bodies,
- * narrow_per_warp (a multiple of 32) and color_chunk (32 to 256) are used;
+ * pair_bodies, narrow_per_warp (a multiple of 32) and color_chunk (32 to 256)
+ * are used;
  * 0 keeps the current value; the timing fields are ignored.  Results do not
  * depend on the configuration. */
 RBPS_API int rbps_batch_set_launch(rbps_batch *batch, const rbps_tune_result *config);

@@ -52,7 +52,8 @@ class StateView(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [("frame_block", C.c_int32), ("narrow_grid", C.c_int32), ("ms_per_step", C.c_double),
                 ("ms_per_step_default", C.c_double), ("trials", C.c_uint32), ("team_bodies", C.c_uint32),
-                ("narrow_per_warp", C.c_uint32), ("color_chunk", C.c_uint32)]
+                ("narrow_per_warp", C.c_uint32), ("color_chunk", C.c_uint32), ("pair_bodies", C.c_uint32),
+                ("pad_", C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -330,8 +331,8 @@ class Batch:
 
     def set_launch(self, **cfg):
         """Applies launch-shape fields (frame_block, narrow_grid, team_bodies,
-        narrow_per_warp, color_chunk) as rbps_batch_set_launch; others keep
-        their values.  Results do not depend on them."""
+        pair_bodies, narrow_per_warp, color_chunk) as rbps_batch_set_launch;
+        others keep their values.  Results do not depend on them."""
         r = TuneResult()
         for k, v in cfg.items():
             setattr(r, k, v)

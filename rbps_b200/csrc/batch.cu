@@ -327,6 +327,7 @@ struct rbps_batch
     std::vector<HostHeightmap> heightmaps;
     std::vector<HostMesh> meshes;
     uint32_t team_bodies = 0; // worlds this large step on a whole CTA (set_team_split)
+    uint32_t pair_bodies = 0; // worlds this large (and below team_bodies) step on half a CTA
     MeshDesc *mesh_desc = nullptr;
     double *mesh_v = nullptr, *mesh_n = nullptr;
     uint32_t *mesh_i = nullptr;
@@ -386,7 +387,7 @@ struct rbps_batch
     uint2 *nlist = nullptr;
     void **wcand = nullptr, **wcc = nullptr;
     uint32_t n_sbodies = 0, n_sjoints = 0, n_sjcolors = 0, n_block_worlds = 0;
-    uint32_t smem_cap_block = 0, smem_cap_warp = 0;
+    uint32_t smem_cap_block = 0, smem_cap_warp = 0, smem_cap_pair = 0, n_pair_worlds = 0;
     int grid_big = 0;
     uint32_t n_counters = 0;  // phase work counters per step
     uint64_t total_bodies = 0, total_dynamic = 0;
@@ -887,6 +888,8 @@ namespace
         e.n_block_worlds = b->n_block_worlds;
         e.smem_cap_block = b->smem_cap_block;
         e.smem_cap_warp = b->smem_cap_warp;
+        e.n_pair_worlds = b->n_pair_worlds;
+        e.smem_cap_pair = b->smem_cap_pair;
         e.dump_pairs = b->dump ? b->dump_pairs : nullptr;
         e.dump_cand = b->dump ? b->dump_cand : nullptr;
         e.dump_cc = b->dump ? (CandContacts<T, P> *)b->dump_cc : nullptr;
@@ -919,32 +922,43 @@ namespace
 
     constexpr uint32_t kSmallWorldBodies = kGridWorldBodies; // larger worlds step on the cooperative grid
     constexpr int kMaxBlockHost = 256; // block of the flat kernels (their __launch_bounds__)
-    constexpr uint32_t kBlockTeamBodies = 128; // colored batches: worlds this large step on a whole CTA
+    constexpr uint32_t kBlockTeamBodies = 256; // colored batches: worlds this large step on a whole CTA
+    constexpr uint32_t kPairTeamBodies = 96;   // ... and worlds this large on half a CTA
     constexpr uint32_t kSmemBodiesMax = 1024;   // bodies a CTA world keeps in shared memory (137 KB in FP32)
 } // namespace
 
 // Worlds of `threshold` bodies or more step on a whole CTA in the substep
-// kernel, the rest on one warp each (small_ids is sorted by body count);
-// shared-memory world copies hold the largest CTA world or four warp worlds
-// (a world beyond its cap runs on the batch arrays).
+// kernel, worlds of `pair` bodies or more (and fewer than `threshold`) on
+// half a CTA, the rest on one warp each (small_ids is sorted by body count,
+// largest first); pair >= threshold leaves no half-CTA worlds.  Shared-memory
+// world copies hold the largest CTA world, two half-CTA worlds or four warp
+// worlds (a world beyond its cap runs on the batch arrays).
 template <class T, class P>
-static int set_team_split(rbps_batch *b, uint32_t threshold)
+static int set_team_split(rbps_batch *b, uint32_t threshold, uint32_t pair)
 {
+    pair = std::min(pair, threshold);
     const uint32_t ns = (uint32_t)b->small_ids.size();
     uint32_t nbw = 0;
     while (nbw < ns && b->wdev[b->small_ids[nbw]].n_bodies >= threshold)
         ++nbw;
+    uint32_t npw = 0;
+    while (nbw + npw < ns && b->wdev[b->small_ids[nbw + npw]].n_bodies >= pair)
+        ++npw;
     b->n_block_worlds = nbw;
-    b->flat.grid_solve = (int)(nbw + (ns - nbw + 3) / 4);
+    b->n_pair_worlds = npw;
+    b->flat.grid_solve = (int)(nbw + (npw + 1) / 2 + (ns - nbw - npw + 3) / 4);
     auto round16 = [](uint32_t x) { return (x + 15u) / 16u * 16u; };
-    b->smem_cap_warp = round16(threshold);
+    b->smem_cap_warp = round16(pair);
+    b->smem_cap_pair = npw ? round16(std::min<uint32_t>(b->wdev[b->small_ids[nbw]].n_bodies, kSmemBodiesMax)) : 0;
     b->smem_cap_block = 0;
     if (nbw)
         b->smem_cap_block = round16(std::min<uint32_t>(b->wdev[b->small_ids[0]].n_bodies, kSmemBodiesMax));
-    b->flat.substep_smem =
-        std::max(4 * smem_world_bytes<T, P>(b->smem_cap_warp), smem_world_bytes<T, P>(b->smem_cap_block));
+    b->flat.substep_smem = std::max({4 * smem_world_bytes<T, P>(b->smem_cap_warp),
+                                     2 * smem_world_bytes<T, P>(b->smem_cap_pair),
+                                     smem_world_bytes<T, P>(b->smem_cap_block)});
     CU(prepare_substep<T, P>(b->flat.substep_smem));
     b->team_bodies = threshold;
+    b->pair_bodies = pair;
     return RBPS_OK;
 }
 
@@ -1506,7 +1520,7 @@ static int commit_typed(rbps_batch *b)
         CU(occupancy_flat<T, P>(0, kMaxBlockHost, &per_sm, 0));
         b->flat.grid_narrow = std::max(1, per_sm) * b->sm_count;
         b->flat.block_solve = 128;
-        if ((rc = set_team_split<T, P>(b, kBlockTeamBodies)))
+        if ((rc = set_team_split<T, P>(b, kBlockTeamBodies, kPairTeamBodies)))
             return rc;
         b->use_flat = true;
         // side stream + events for the parallel narrowphase kernels
@@ -2554,20 +2568,23 @@ static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
             best_c = cand[k];
         }
     }
-    // then the CTA / warp team split of the substep kernel, with the best
-    // shapes above
-    const uint32_t tb0 = b->team_bodies;
-    uint32_t best_t = tb0;
+    // then the team split of the substep kernel (CTA from / half CTA from
+    // body counts), with the best shapes above
+    const uint32_t tb0 = b->team_bodies, pb0 = b->pair_bodies;
+    uint32_t best_t = tb0, best_p = pb0;
     uint32_t n_trials = (uint32_t)cand.size();
     if (!rc && b->use_flat)
     {
         rc = apply_launch<T, P>(b, best_c.first, best_c.second);
-        for (uint32_t tb : {64u, 96u, 160u, 192u})
+        const std::pair<uint32_t, uint32_t> splits[] = {{128u, 128u}, {96u, 96u}, {192u, 64u}, {256u, 64u},
+                                                        {256u, 128u}, {320u, 96u}, {384u, 128u}};
+        for (const auto &sp : splits)
         {
-            if (rc || tb == tb0)
+            if (rc || (sp.first == tb0 && sp.second == pb0))
                 continue;
             ++n_trials;
-            if ((rc = set_team_split<T, P>(b, tb)) || (rc = apply_launch<T, P>(b, best_c.first, best_c.second)) ||
+            if ((rc = set_team_split<T, P>(b, sp.first, sp.second)) ||
+                (rc = apply_launch<T, P>(b, best_c.first, best_c.second)) ||
                 (rc = snapshot_copy<T, P>(b, b->snaps[slot], 1)) || (rc = step_typed<T, P>(b, 1)))
                 break;
             CU(cudaEventRecord(e0, b->stream));
@@ -2580,11 +2597,12 @@ static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
             if (ms / trials < best)
             {
                 best = ms / trials;
-                best_t = tb;
+                best_t = sp.first;
+                best_p = sp.second;
             }
         }
         if (!rc)
-            rc = set_team_split<T, P>(b, best_t);
+            rc = set_team_split<T, P>(b, best_t, best_p);
     }
     // then the narrowphase candidates per warp and the colouring batch, one
     // knob at a time with the others at their best
@@ -2662,6 +2680,7 @@ static int autotune_typed(rbps_batch *b, int trials, rbps_tune_result *out)
         out->ms_per_step_default = first;
         out->trials = n_trials;
         out->team_bodies = best_t;
+        out->pair_bodies = best_p;
         out->narrow_per_warp = best_npw;
         out->color_chunk = best_cc;
     }
@@ -2680,7 +2699,9 @@ template <class T, class P>
 static int set_launch_typed(rbps_batch *b, const rbps_tune_result *cfg)
 {
     int rc;
-    if (b->use_flat && cfg->team_bodies && (rc = set_team_split<T, P>(b, cfg->team_bodies)))
+    if (b->use_flat && (cfg->team_bodies || cfg->pair_bodies) &&
+        (rc = set_team_split<T, P>(b, cfg->team_bodies ? cfg->team_bodies : b->team_bodies,
+                                   cfg->pair_bodies ? cfg->pair_bodies : b->pair_bodies)))
         return rc;
     if (cfg->narrow_per_warp)
         b->narrow_per_warp = cfg->narrow_per_warp;

@@ -1707,24 +1707,12 @@ namespace rbps_gpu
 
     // Narrowphase of every candidate of the small worlds but the box-box
     // ones, in class order.
-    // Entries [0, n) of a class-sorted range, dealt to the grid's warps in
-    // chunks of `per_warp` (a multiple of 32) consecutive entries, a lane
-    // taking every 32nd entry of its warp's chunk; per_warp = 32 is the
-    // plain grid-stride loop.  f(k) runs once per entry.
-    template <class F>
-    __device__ __forceinline__ void for_warp_chunks(uint32_t n, uint32_t per_warp, F &&f)
-    {
-        const uint32_t lane = threadIdx.x & 31u;
-        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-        const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
-        for (uint32_t base = warp * per_warp; base < n; base += n_warps * per_warp)
-        {
-            const uint32_t end = min(n, base + per_warp);
-            for (uint32_t k = base + lane; k < end; k += 32)
-                f(k);
-        }
-    }
-
+    // Entries [0, n) of a class-sorted range are dealt to the grid's warps
+    // in chunks of E.narrow_per_warp (a multiple of 32) consecutive entries,
+    // a lane taking every 32nd entry of its warp's chunk; 32 is the plain
+    // grid-stride loop.  (Written out in each kernel: a helper taking the
+    // kernel's Engine by reference inside a lambda made the compiler copy
+    // the whole parameter block to the stack, 650 bytes a thread.)
     template <class T, class P>
     __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow(const Engine<T, P> E)
     {
@@ -1732,8 +1720,15 @@ namespace rbps_gpu
         const uint32_t total = E.gcol[kGcolOff + kPairClasses];
         const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
         const uint32_t n = total - (bb1 - bb0);
-        for_warp_chunks(n, E.narrow_per_warp,
-                        [&](uint32_t k) { narrow_flat<T, P, kSelNoBoxBox>(E, k < bb0 ? k : k + (bb1 - bb0)); });
+        const uint32_t per_warp = E.narrow_per_warp, lane = threadIdx.x & 31u;
+        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+        for (uint32_t base = warp * per_warp; base < n; base += n_warps * per_warp)
+        {
+            const uint32_t end = min(n, base + per_warp);
+            for (uint32_t k = base + lane; k < end; k += 32)
+                narrow_flat<T, P, kSelNoBoxBox>(E, k < bb0 ? k : k + (bb1 - bb0));
+        }
     }
 
     // The box-box class on its own: its SAT, clipping buffers and registers
@@ -1742,7 +1737,16 @@ namespace rbps_gpu
     __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow_boxbox(const Engine<T, P> E)
     {
         const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
-        for_warp_chunks(bb1 - bb0, E.narrow_per_warp, [&](uint32_t k) { narrow_flat<T, P, kSelBoxBox>(E, bb0 + k); });
+        const uint32_t n = bb1 - bb0;
+        const uint32_t per_warp = E.narrow_per_warp, lane = threadIdx.x & 31u;
+        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+        for (uint32_t base = warp * per_warp; base < n; base += n_warps * per_warp)
+        {
+            const uint32_t end = min(n, base + per_warp);
+            for (uint32_t k = base + lane; k < end; k += 32)
+                narrow_flat<T, P, kSelBoxBox>(E, bb0 + k);
+        }
     }
 
     // The rest of a substep for one world per warp: colouring, integrate
@@ -1767,6 +1771,33 @@ namespace rbps_gpu
             n += __popc(m);
         }
         __syncwarp();
+        return n;
+    }
+
+    // A pair team's two warps exchange their counts through the CTA's scan
+    // words 2h and 2h + 1 (the other half uses the other two).
+    template <class F>
+    __device__ __forceinline__ uint32_t team_compact(const PairTeam &tm, uint32_t n_cand, uint32_t *out,
+                                                     ScanShared &sh, F &&sel)
+    {
+        const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
+        const uint32_t w = (threadIdx.x >> 5) & 1u, slot = 2u * tm.half();
+        uint32_t n = 0;
+        for (uint32_t base = 0; base < n_cand; base += 64)
+        {
+            const uint32_t c = base + tm.rank();
+            const bool take = c < n_cand && sel(c);
+            const uint32_t m = __ballot_sync(0xffffffffu, take);
+            if (lane == 0)
+                sh.warp[slot + w] = __popc(m);
+            tm.sync();
+            const uint32_t below = w ? sh.warp[slot] : 0u;
+            const uint32_t tot = sh.warp[slot] + sh.warp[slot + 1];
+            if (take)
+                out[n + below + __popc(m & lt)] = c;
+            n += tot;
+            tm.sync();
+        }
         return n;
     }
 
@@ -2154,14 +2185,15 @@ namespace rbps_gpu
     }
 
     // The largest worlds (the first n_block_worlds of the list) get a whole
-    // CTA each; the others one warp each, four per CTA.  Worlds progress
-    // independently: a barrier is the team's own.  Dynamic shared memory:
-    // E.smem_cap_block bodies for a CTA world, or E.smem_cap_warp bodies for
-    // each of the four warp worlds.
+    // CTA each, the next n_pair_worlds half a CTA (two warps) each, the
+    // others one warp each, four per CTA.  Worlds progress independently: a
+    // barrier is the team's own.  Dynamic shared memory: E.smem_cap_block
+    // bodies for a CTA world, E.smem_cap_pair for each of two half-CTA
+    // worlds, or E.smem_cap_warp for each of four warp worlds.
     template <class T, class P>
     __global__ void __launch_bounds__(128, RBPS_SUBSTEP_MIN_BLOCKS) k_substep(const Engine<T, P> E)
     {
-        __shared__ ScanShared sh; // the colouring's compaction scan is all the team needs
+        __shared__ ScanShared sh; // the colouring's compaction scans are all the teams need
         extern __shared__ __align__(16) unsigned char smem[];
         if (blockIdx.x < E.n_block_worlds)
         {
@@ -2169,7 +2201,21 @@ namespace rbps_gpu
             substep_world(E, tm, E.small_worlds[blockIdx.x], smem, E.smem_cap_block, sh);
             return;
         }
-        const uint32_t q = E.n_block_worlds + (blockIdx.x - E.n_block_worlds) * (blockDim.x >> 5) + warp_id();
+        const uint32_t pair_ctas = (E.n_pair_worlds + 1) / 2;
+        const uint32_t b = blockIdx.x - E.n_block_worlds;
+        if (b < pair_ctas)
+        {
+            // two mid-size worlds, one per half of the CTA, each on its own
+            // named barrier (a half without a world leaves at once)
+            const uint32_t k = 2 * b + (threadIdx.x >> 6);
+            if (k >= E.n_pair_worlds)
+                return;
+            PairTeam tm;
+            substep_world(E, tm, E.small_worlds[E.n_block_worlds + k],
+                          smem + (threadIdx.x >> 6) * SmemWorld<T, P>::bytes(E.smem_cap_pair), E.smem_cap_pair, sh);
+            return;
+        }
+        const uint32_t q = E.n_block_worlds + E.n_pair_worlds + (b - pair_ctas) * (blockDim.x >> 5) + warp_id();
         if (q >= E.n_small)
             return;
         WarpTeam tm;

@@ -228,8 +228,10 @@ namespace rbps_gpu
         const uint32_t *small_worlds;
         uint32_t n_small;
         uint32_t n_block_worlds;  // colored batches: the first n of small_worlds step on a whole CTA
+        uint32_t n_pair_worlds;   // the next n on half a CTA (two warps) each
         uint32_t smem_cap_block;  // bodies a CTA world keeps in shared memory (colored substep)
         uint32_t smem_cap_warp;   // bodies each warp world keeps in shared memory
+        uint32_t smem_cap_pair;   // bodies each half-CTA world keeps in shared memory
         // parity dumps (null when disabled)
         uint32_t *dump_pairs;   // 2 * pair_cap per slot
         Cand *dump_cand;        // cand_cap per slot

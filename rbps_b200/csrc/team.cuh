@@ -52,6 +52,23 @@ namespace rbps_gpu
         __device__ __forceinline__ void sync() const { __syncwarp(); }
     };
 
+    // Two warps of a 128-thread CTA as a team: threads [64 h, 64 h + 64) for
+    // half h, barrier = the named barrier 1 + h over its 64 threads (0 is
+    // __syncthreads', which the halves do not use).
+    struct PairTeam
+    {
+        __device__ __forceinline__ uint32_t cta() const { return 0; }
+        __device__ __forceinline__ uint32_t ncta() const { return 1; }
+        __device__ __forceinline__ uint32_t rank() const { return threadIdx.x & 63u; }
+        __device__ __forceinline__ uint32_t size() const { return 64; }
+        __device__ __forceinline__ bool leader() const { return (threadIdx.x & 63u) == 0; }
+        __device__ __forceinline__ uint32_t half() const { return threadIdx.x >> 6; }
+        __device__ __forceinline__ void sync() const
+        {
+            asm volatile("bar.sync %0, 64;" ::"r"(1 + (threadIdx.x >> 6)) : "memory");
+        }
+    };
+
     constexpr int kMaxWarps = 32;
 
     // Shared scratch of the block primitives (one per CTA).

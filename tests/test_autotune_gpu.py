@@ -35,7 +35,9 @@ def test_autotune_keeps_state_and_results(rbps):
 
 
 @pytest.mark.parametrize("cfg", [dict(narrow_per_warp=256, color_chunk=32, team_bodies=64, frame_block=128),
-                                 dict(narrow_per_warp=64, color_chunk=128, team_bodies=192, narrow_grid=37)])
+                                 dict(narrow_per_warp=64, color_chunk=128, team_bodies=192, narrow_grid=37),
+                                 dict(team_bodies=400, pair_bodies=16),
+                                 dict(team_bodies=128, pair_bodies=128)])
 def test_launch_shape_does_not_change_results(rbps, cfg):
     """Every knob of the autotuner, set by hand away from its default: the
     same bits as a batch at the defaults."""
