@@ -385,6 +385,7 @@ struct rbps_batch
     bool use_flat = false;
     uint32_t *wcoff = nullptr, *gcol = nullptr, *sbodies = nullptr, *sjoints = nullptr, *sjcoff = nullptr;
     uint2 *nlist = nullptr;
+    uint4 *nglob = nullptr; // global collider / body indices beside nlist
     void **wcand = nullptr, **wcc = nullptr;
     uint32_t n_sbodies = 0, n_sjoints = 0, n_sjcolors = 0, n_block_worlds = 0;
     uint32_t smem_cap_block = 0, smem_cap_warp = 0, smem_cap_pair = 0, n_pair_worlds = 0;
@@ -875,6 +876,7 @@ namespace
         e.wcoff = b->wcoff;
         e.gcol = b->gcol;
         e.nlist = b->nlist;
+        e.nglob = b->nglob;
         e.wcand = (Cand *const *)b->wcand;
         e.wcc = (CandContacts<T, P> *const *)b->wcc;
         e.sbodies = b->sbodies;
@@ -1511,6 +1513,7 @@ static int commit_typed(rbps_batch *b)
         if ((rc = b->alloc((void **)&b->wcoff, 4 * ((size_t)ns + 1))) ||
             (rc = b->alloc((void **)&b->gcol, 4 * (size_t)kGcolWords)) ||
             (rc = b->alloc((void **)&b->nlist, sizeof(uint2) * std::max<size_t>(cand_cap, 1))) ||
+            (rc = b->alloc((void **)&b->nglob, sizeof(uint4) * std::max<size_t>(cand_cap, 1))) ||
             (rc = b->upload(&b->wcand, wcand)) || (rc = b->upload(&b->wcc, wcc)) ||
             (rc = b->upload(&b->sbodies, sbodies)) || (rc = b->upload(&b->sjoints, sjoints)) ||
             (rc = b->upload(&b->sjcoff, sjcoff)))

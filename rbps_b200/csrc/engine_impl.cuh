@@ -826,18 +826,10 @@ namespace rbps_gpu
 
     // Narrowphase of one candidate (the analytic routines); returns
     // kNeedsGjk for a pair the GJK pass handles (its rows are left empty).
-    template <class T, class P, int Sel = kSelAll>
-    __device__ __forceinline__ int narrow_candidate(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
-                                                    CandContacts<T, P> &out)
+    template <class T, class P, int Sel>
+    __device__ __forceinline__ int narrow_pair(const Engine<T, P> &E, uint32_t gca, uint32_t gcb, uint32_t gba,
+                                               uint32_t gbb, CandContacts<T, P> &out)
     {
-        if (cd.ca >= W.n_coll || cd.cb >= W.n_coll || cd.ba >= W.n_bodies || cd.bb >= W.n_bodies)
-        {
-            set_error_at(E.error, kErrInternal, 3, cd.ca);
-            out.n = 0;
-            return kMiss;
-        }
-        const uint32_t gca = W.coll_off + cd.ca, gcb = W.coll_off + cd.cb;
-        const uint32_t gba = W.body_off + cd.ba, gbb = W.body_off + cd.bb;
         const tf<T> ta = collider_tf(E, gca, gba);
         const tf<T> tb = collider_tf(E, gcb, gbb);
         Manifold<T> m;
@@ -851,6 +843,20 @@ namespace rbps_gpu
             res = kMiss;
         emit_manifold(E, gca, gcb, gba, gbb, m, res == kHit ? m.n : 0, out);
         return res;
+    }
+
+    template <class T, class P, int Sel = kSelAll>
+    __device__ __forceinline__ int narrow_candidate(const Engine<T, P> &E, const WorldDev &W, const Cand &cd,
+                                                    CandContacts<T, P> &out)
+    {
+        if (cd.ca >= W.n_coll || cd.cb >= W.n_coll || cd.ba >= W.n_bodies || cd.bb >= W.n_bodies)
+        {
+            set_error_at(E.error, kErrInternal, 3, cd.ca);
+            out.n = 0;
+            return kMiss;
+        }
+        return narrow_pair<T, P, Sel>(E, W.coll_off + cd.ca, W.coll_off + cd.cb, W.body_off + cd.ba,
+                                      W.body_off + cd.bb, out);
     }
 
     // A GJK pair found by the narrowphase: queued for k_gjk and counted
@@ -1686,8 +1692,20 @@ namespace rbps_gpu
             const uint32_t q = world_of_flat(E, f);
             const uint32_t w = E.small_worlds[q];
             const uint32_t c = f - E.wcoff[q];
-            const uint32_t k = cand_class(E, E.worlds[w], E.wcand[w][c]);
-            E.nlist[base[k] + atomicAdd(&cnt[k], 1u)] = make_uint2(w, c);
+            const WorldDev W = E.worlds[w];
+            const Cand cd = E.wcand[w][c];
+            const uint32_t k = cand_class(E, W, cd);
+            const uint32_t slot = base[k] + atomicAdd(&cnt[k], 1u);
+            E.nlist[slot] = make_uint2(w, c);
+            // the global collider and body indices, so the narrowphase reads
+            // them with its entry instead of through the world and candidate
+            // (checked here, once a step, instead of every substep)
+            uint4 g = make_uint4(~0u, ~0u, ~0u, ~0u);
+            if (cd.ca < W.n_coll && cd.cb < W.n_coll && cd.ba < W.n_bodies && cd.bb < W.n_bodies)
+                g = make_uint4(W.coll_off + cd.ca, W.coll_off + cd.cb, W.body_off + cd.ba, W.body_off + cd.bb);
+            else
+                set_error_at(E.error, kErrInternal, 3, cd.ca);
+            E.nglob[slot] = g;
         }
     }
 
@@ -1697,12 +1715,19 @@ namespace rbps_gpu
     __device__ __forceinline__ void narrow_flat(const Engine<T, P> &E, uint32_t i)
     {
         const uint2 e = E.nlist[i];
-        const WorldDev W = E.worlds[e.x];
-        uint32_t n_gjk = 0;
-        if (narrow_candidate<T, P, Sel>(E, W, E.wcand[e.x][e.y], E.wcc[e.x][e.y]) == kNeedsGjk)
+        const uint4 g = E.nglob[i];
+        CandContacts<T, P> &out = E.wcc[e.x][e.y];
+        if (g.x == ~0u) // a corrupt candidate, reported by the class sort
+        {
+            out.n = 0;
+            return;
+        }
+        if (narrow_pair<T, P, Sel>(E, g.x, g.y, g.z, g.w, out) == kNeedsGjk)
+        {
+            uint32_t n_gjk = 0;
             queue_gjk(E, e.x, e.y, n_gjk);
-        if (n_gjk)
-            atomicAdd(world_scratch(E, W).misc + kMiscNGjk, n_gjk);
+            atomicAdd(world_scratch(E, E.worlds[e.x]).misc + kMiscNGjk, n_gjk);
+        }
     }
 
     // Narrowphase of every candidate of the small worlds but the box-box

@@ -252,6 +252,7 @@ namespace rbps_gpu
         uint32_t *wcoff;               // n_small + 1: candidate prefix over small_worlds
         uint32_t *gcol;                // global colour bookkeeping, kGcolWords
         uint2 *nlist;                  // (world, candidate) of all small worlds sorted by shape pair
+        uint4 *nglob;                  // beside each entry: global colliders a, b and bodies a, b
         Cand *const *wcand;            // per world: its candidate list
         CandContacts<T, P> *const *wcc; // per world: its contact manifolds
         const uint32_t *sbodies;       // bodies of the small worlds
