@@ -1522,6 +1522,10 @@ static int commit_typed(rbps_batch *b)
         int per_sm = 0;
         CU(occupancy_flat<T, P>(0, kMaxBlockHost, &per_sm, 0));
         b->flat.grid_narrow = std::max(1, per_sm) * b->sm_count;
+        // the class sort is a chain of dependent loads per candidate (a
+        // binary search over the worlds): it wants every warp it can get
+        CU(occupancy_flat<T, P>(2, kMaxBlockHost, &per_sm, 0));
+        b->flat.grid_sort = std::max(1, per_sm) * b->sm_count;
         b->flat.block_solve = 128;
         if ((rc = set_team_split<T, P>(b, kBlockTeamBodies, kPairTeamBodies)))
             return rc;

@@ -216,28 +216,278 @@ namespace rbps_gpu
     }
 
     // ------------------------------------------------------------ broadphase
+    // One-CTA fast path of the endpoint sort, in the staging area `smem`
+    // (kSmemSortWords words).  moved[i] (shared) flags the previous
+    // positions whose keys the frame's object update rewrote.  When the
+    // other endpoints (R) are still in key order, the stable sort of the
+    // whole array -- keys ordered, equal keys in previous order -- is the
+    // merge of R with the moved endpoints (M) by (key, previous position):
+    // R is sorted that way already, M is ranked by counting, and each
+    // endpoint's final position is its rank in its own list plus the count
+    // of the other list's endpoints before it (a binary search).  ep_key,
+    // ep_id and ep_pos are then written once.  Returns false with nothing
+    // written when M exceeds kMergeMax or R is out of order (the first frame
+    // after a commit, whose endpoints are in insertion order, and any array
+    // that is not the last sort's output); the caller then sorts in full.
+    // Every thread of the CTA must call it; it ends with a block barrier.
+    constexpr uint32_t kMergeMax = 512;
+
+    static __device__ __noinline__ bool merge_moved_endpoints(uint32_t *ep_key, uint32_t *ep_id, uint32_t *ep_pos, uint32_t nep,
+                                                       uint32_t id_limit, const uint32_t *moved, uint32_t *smem,
+                                                       ScanShared &sh, int *error)
+    {
+        uint32_t *rk = smem, *rp = smem + kSmemSortMax, *rid = smem + 2 * kSmemSortMax;
+        uint32_t *mk = smem + 3 * kSmemSortMax, *mp = mk + kMergeMax, *mid = mp + kMergeMax;
+        uint32_t *smk = mid + kMergeMax, *smp = smk + kMergeMax, *mfin = smp + kMergeMax;
+        const uint32_t B = blockDim.x, t = threadIdx.x;
+        // each thread a contiguous run of positions, so M and R keep order
+        const uint32_t per = (nep + B - 1) / B;
+        const uint32_t i0 = min(nep, t * per), i1 = min(nep, i0 + per);
+        uint32_t mine = 0;
+        for (uint32_t i = i0; i < i1; ++i)
+            mine += moved[i] ? 1u : 0u;
+        if (t == 0)
+            sh.bcast[2] = 0u; // R out of order (published by the scan's barriers)
+        uint32_t m;
+        uint32_t mi = block_excl_scan(mine, sh, &m);
+        if (m > kMergeMax)
+            return false;
+        for (uint32_t i = i0; i < i1; ++i)
+        {
+            const uint32_t key = ep_key[i], id = ep_id[i];
+            if (moved[i])
+            {
+                mk[mi] = key;
+                mp[mi] = i;
+                mid[mi] = id;
+                ++mi;
+            }
+            else
+            {
+                const uint32_t r = i - mi;
+                rk[r] = key;
+                rp[r] = i;
+                rid[r] = id;
+            }
+        }
+        __syncthreads();
+        const uint32_t nr = nep - m;
+        for (uint32_t r = t; r + 1 < nr; r += B)
+            if (rk[r] > rk[r + 1])
+                sh.bcast[2] = 1u;
+        for (uint32_t u = t; u < m; u += B)
+        {
+            const uint32_t k = mk[u], p = mp[u];
+            uint32_t rank = 0;
+            for (uint32_t v = 0; v < m; ++v)
+                rank += (mk[v] < k || (mk[v] == k && v < u)) ? 1u : 0u; // v < u <=> mp[v] < p
+            uint32_t lo = 0, hi = nr;
+            while (lo < hi)
+            {
+                const uint32_t h = (lo + hi) >> 1;
+                if (rk[h] < k || (rk[h] == k && rp[h] < p))
+                    lo = h + 1;
+                else
+                    hi = h;
+            }
+            smk[rank] = k;
+            smp[rank] = p;
+            mfin[u] = rank + lo;
+        }
+        __syncthreads();
+        const bool bad = sh.bcast[2] != 0u;
+        __syncthreads(); // everyone has read the flag before the caller reuses sh
+        if (bad)
+            return false;
+        if (m == 0)
+            return true; // nothing moved and the order holds: the arrays stand
+        for (uint32_t r = t; r < nr; r += B)
+        {
+            const uint32_t k = rk[r], p = rp[r];
+            uint32_t lo = 0, hi = m;
+            while (lo < hi)
+            {
+                const uint32_t h = (lo + hi) >> 1;
+                if (smk[h] < k || (smk[h] == k && smp[h] < p))
+                    lo = h + 1;
+                else
+                    hi = h;
+            }
+            const uint32_t f = r + lo, id = rid[r];
+            ep_key[f] = k;
+            ep_id[f] = id;
+            if (id < id_limit)
+                ep_pos[id] = f;
+            else
+                set_error_at(error, kErrInternal, 1, id);
+        }
+        for (uint32_t u = t; u < m; u += B)
+        {
+            const uint32_t f = mfin[u], id = mid[u];
+            ep_key[f] = mk[u];
+            ep_id[f] = id;
+            if (id < id_limit)
+                ep_pos[id] = f;
+            else
+                set_error_at(error, kErrInternal, 1, id);
+        }
+        __syncthreads();
+        return true;
+    }
+
+    // One-CTA fast path of the sweep, in the staging area `smem`: a single
+    // pass over the overlap runs that leaves the pairs in the reference's
+    // emission order without sorting them.  That order is by the position j
+    // of the later opening endpoint, then by the position i of the earlier
+    // one (BroadPhase.cpp:104-152).  The pass counts each j's pairs (hist),
+    // appends every hit (i, j) to a staging list (warp-aggregated slots, so
+    // the list has no particular order) and stores each opening endpoint's
+    // own count in S.cnt.  A scan of hist gives each j its first slot, a
+    // scatter groups the list by j, and an entry's final slot is its group's
+    // first plus the number of the group's entries with a smaller i.  The
+    // first min(total, pair_cap) pairs are written to S.pr_a / S.pr_b (pk =
+    // j, pv = identity).  Returns the pair count, or ~0u when the hits do not
+    // fit the staging list; S.cnt is complete then, and the caller emits and
+    // sorts in global memory.  Every thread of the CTA must call it.
+    template <class SC>
+    __device__ __noinline__ uint32_t sweep_staged(const FatBox *fat, const uint32_t *ep_id, const uint32_t *ep_pos,
+                                                  uint32_t nep, uint32_t id_limit, uint32_t pair_cap, int *error,
+                                                  const SC &S, ScanShared &sh, uint32_t *smem)
+    {
+        uint32_t *hist = smem, *fill = smem + kSmemSortMax;
+        uint32_t *lst = smem + 2 * kSmemSortMax, *grp = smem + 3 * kSmemSortMax;
+        const uint32_t B = blockDim.x, t = threadIdx.x, lane = t & 31u;
+        for (uint32_t i = t; i < nep; i += B)
+        {
+            hist[i] = 0u;
+            fill[i] = 0u;
+        }
+        if (t == 0)
+            sh.bcast[3] = 0u;
+        __syncthreads();
+        for (uint32_t i = t; i < nep; i += B)
+        {
+            const uint32_t id = ep_id[i];
+            uint32_t c = 0;
+            if (!(id & 1u) && id < id_limit)
+            {
+                const FatBox fa = fat[id >> 1];
+                const uint32_t end = min(ep_pos[id + 1], nep);
+                for (uint32_t j = i + 1; j < end; ++j)
+                {
+                    const uint32_t id2 = ep_id[j];
+                    const bool hit = !(id2 & 1u) && id2 < id_limit && fat_overlap(fa, fat[id2 >> 1]);
+                    // one list reservation per warp step, for the lanes that hit
+                    const uint32_t act = __activemask();
+                    const uint32_t hm = __ballot_sync(act, hit);
+                    if (hm)
+                    {
+                        const uint32_t leader = __ffs(hm) - 1;
+                        uint32_t s = 0;
+                        if (lane == leader)
+                            s = atomicAdd(&sh.bcast[3], (uint32_t)__popc(hm));
+                        s = __shfl_sync(act, s, leader) + __popc(hm & ((1u << lane) - 1u));
+                        if (hit)
+                        {
+                            if (s < kSmemSortMax)
+                                lst[s] = (i << 16) | j;
+                            atomicAdd(&hist[j], 1u);
+                            ++c;
+                        }
+                    }
+                }
+            }
+            S.cnt[i] = c;
+        }
+        __syncthreads();
+        const uint32_t total = sh.bcast[3];
+        if (total > kSmemSortMax)
+            return ~0u;
+        // first slot of each j
+        const uint32_t per = (nep + B - 1) / B;
+        const uint32_t i0 = min(nep, t * per), i1 = min(nep, i0 + per);
+        uint32_t mine = 0;
+        for (uint32_t i = i0; i < i1; ++i)
+            mine += hist[i];
+        uint32_t sum;
+        uint32_t run = block_excl_scan(mine, sh, &sum);
+        for (uint32_t i = i0; i < i1; ++i)
+        {
+            const uint32_t h = hist[i];
+            hist[i] = run;
+            run += h;
+        }
+        if (t == 0 && sum != total)
+            set_error_at(error, kErrInternal, 6, total); // the two counts of one pass must agree
+        __syncthreads();
+        for (uint32_t s = t; s < total; s += B)
+        {
+            const uint32_t v = lst[s], j = v & 0xffffu;
+            const uint32_t g = hist[j] + atomicAdd(&fill[j], 1u);
+            if (g < total)
+                grp[g] = v;
+        }
+        __syncthreads();
+        const uint32_t n_out = min(total, pair_cap);
+        for (uint32_t s = t; s < total; s += B)
+        {
+            const uint32_t v = grp[s], i = v >> 16, j = v & 0xffffu;
+            if (i >= nep || j >= nep)
+            {
+                set_error_at(error, kErrInternal, 6, v); // a slot the scatter left unwritten
+                continue;
+            }
+            const uint32_t g0 = hist[j], g1 = min(total, g0 + fill[j]);
+            uint32_t f = g0;
+            for (uint32_t u = g0; u < g1; ++u)
+                f += (grp[u] >> 16) < i ? 1u : 0u;
+            if (f < n_out)
+            {
+                S.pr_a[f] = ep_id[i] >> 1;
+                S.pr_b[f] = ep_id[j] >> 1;
+                S.pk[f] = j;
+                S.pv[f] = f;
+            }
+        }
+        __syncthreads();
+        return total;
+    }
+
     // Sort + sweep of one SAP state (BroadPhase.cpp:80-152).  On return
     // S.pk / S.pv hold the pairs in the reference emission order (pv indexes
     // the raw object pairs S.pr_a / S.pr_b); returns the pair count.
     // id_limit bounds the endpoint ids (2 * object slots; slots of removed
-    // objects leave gaps in the standalone broadphase).
+    // objects leave gaps in the standalone broadphase).  A one-CTA team
+    // with the shared staging area sort_smem takes the fast paths above:
+    // the merge of the endpoints flagged in `moved` (shared, one word per
+    // endpoint position; null to sort in full) and the single-pass sweep.
     template <class Team, class SC>
     __device__ __noinline__ uint32_t sap_sort_sweep(const Team &tm, const FatBox *fat, uint32_t *ep_key, uint32_t *ep_id,
                                        uint32_t *ep_pos, uint32_t nbp, uint32_t id_limit, uint32_t pair_cap,
                                        int *error, const SC &S, BlockShared &sh, uint32_t *sort_smem = nullptr,
-                                       float4 *yz = nullptr)
+                                       float4 *yz = nullptr, const uint32_t *moved = nullptr)
     {
         const uint32_t nep = 2 * nbp;
+        constexpr bool kBlock = std::is_same<Team, BlockTeam>::value;
+        const bool staged = kBlock && sort_smem != nullptr && nep <= kSmemSortMax && blockDim.x >= 128;
+        bool merged = false;
+        if constexpr (kBlock)
+            if (staged && moved)
+                merged = merge_moved_endpoints(ep_key, ep_id, ep_pos, nep, id_limit, moved, sort_smem, sh, error);
         // stable sort of the endpoints, previous order as the tie-break
-        team_sort_staged(tm, ep_key, ep_id, S.ep_k2, S.ep_v2, nep, 32, S.counts, S.tile_sums, sh, sort_smem);
-        // inverse permutation
+        if (!merged)
+            team_sort_staged(tm, ep_key, ep_id, S.ep_k2, S.ep_v2, nep, 32, S.counts, S.tile_sums, sh, sort_smem);
+        // inverse permutation (the merge wrote it already)
         for (uint32_t i = tm.rank(); i < nep; i += tm.size())
         {
-            const uint32_t id = ep_id[i];
-            if (id < id_limit)
-                ep_pos[id] = i;
-            else
-                set_error_at(error, kErrInternal, 1, id);
+            if (!merged)
+            {
+                const uint32_t id = ep_id[i];
+                if (id < id_limit)
+                    ep_pos[id] = i;
+                else
+                    set_error_at(error, kErrInternal, 1, id);
+            }
             if (i + 1 < nep && ep_key[i] > ep_key[i + 1])
                 set_error_at(error, kErrInternal, 4, i); // the endpoint sort must leave the keys ordered
         }
@@ -254,6 +504,30 @@ namespace rbps_gpu
                                     __double2float_rd(f.mn[2]), __double2float_ru(f.mx[2]));
             }
         tm.sync();
+        bool counted = false;
+        if constexpr (kBlock)
+            if (staged)
+            {
+                const uint32_t n = sweep_staged(fat, ep_id, ep_pos, nep, id_limit, pair_cap, error, S, sh, sort_smem);
+                if (n != ~0u)
+                {
+                    if (tm.leader())
+                        S.misc[kMiscFlags + 4] = n; // unclamped pair count
+                    uint32_t total = n;
+                    if (total > pair_cap)
+                    {
+                        if (tm.leader())
+                            set_error(error, -2);
+                        total = pair_cap;
+                    }
+                    for (uint32_t k = tm.rank(); k + 1 < total; k += tm.size())
+                        if (S.pk[k] > S.pk[k + 1])
+                            set_error_at(error, kErrInternal, 5, k); // pairs must leave in key order
+                    tm.sync();
+                    return total;
+                }
+                counted = true; // too many pairs to stage: S.cnt holds the counts
+            }
         // count the pairs each opening endpoint emits.  A team spread over
         // the cooperative grid (one large world) gives each opening endpoint
         // a warp that tests 32 endpoints of its overlap run at a time: the
@@ -261,7 +535,7 @@ namespace rbps_gpu
         // thread per endpoint would leave most lanes waiting on a few.
         const bool by_warp = tm.ncta() > 1;
         const uint32_t lane = threadIdx.x & 31u;
-        if (by_warp)
+        if (by_warp && !counted)
         {
             for (uint32_t i = tm.rank() >> 5; i < nep; i += tm.size() >> 5)
             {
@@ -289,7 +563,7 @@ namespace rbps_gpu
                     S.cnt[i] = c;
             }
         }
-        else
+        else if (!counted)
             for (uint32_t i = tm.rank(); i < nep; i += tm.size())
             {
                 const uint32_t id = ep_id[i];
@@ -396,6 +670,18 @@ namespace rbps_gpu
         uint32_t *ep_key = E.ep_key + eb;
         uint32_t *ep_id = E.ep_id + eb;
         uint32_t *ep_pos = E.ep_pos + eb;
+        const uint32_t nep = 2 * nbp;
+        // a one-CTA team with a staging area flags the endpoint positions
+        // whose keys it rewrites, for the sort's merge fast path
+        uint32_t *moved = nullptr;
+        if constexpr (std::is_same<Team, BlockTeam>::value)
+            if (sort_smem && nep <= kSmemSortMax)
+            {
+                moved = sh.wdig;
+                for (uint32_t i = tm.rank(); i < nep; i += tm.size())
+                    moved[i] = 0u;
+                tm.sync();
+            }
 
         // object update (update_broad_phase_aabbs + broad_phase_move_swept)
         for (uint32_t o = tm.rank(); o < nbp; o += tm.size())
@@ -424,12 +710,20 @@ namespace rbps_gpu
             fb.mn[0] = f1.mn.x; fb.mn[1] = f1.mn.y; fb.mn[2] = f1.mn.z;
             fb.mx[0] = f1.mx.x; fb.mx[1] = f1.mx.y; fb.mx[2] = f1.mx.z;
             fat[o] = fb;
-            ep_key[ep_pos[2 * o]] = order_key(__double2float_rn(f1.mn.x));
-            ep_key[ep_pos[2 * o + 1]] = order_key(__double2float_rn(f1.mx.x));
+            const uint32_t p0 = ep_pos[2 * o], p1 = ep_pos[2 * o + 1];
+            ep_key[p0] = order_key(__double2float_rn(f1.mn.x));
+            ep_key[p1] = order_key(__double2float_rn(f1.mx.x));
+            if (moved)
+            {
+                if (p0 < nep)
+                    moved[p0] = 1u;
+                if (p1 < nep)
+                    moved[p1] = 1u;
+            }
         }
         tm.sync();
-        return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, 2 * nbp, W.pair_cap, E.error, S, sh, sort_smem,
-                              W.n_bodies > kGridWorldBodies ? S.yz : nullptr);
+        return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, nep, W.pair_cap, E.error, S, sh, sort_smem,
+                              W.n_bodies > kGridWorldBodies ? S.yz : nullptr, moved);
     }
 
     // Filtered SAP pairs followed by the plane candidates; returns the count.
@@ -1462,8 +1756,17 @@ namespace rbps_gpu
         }
     }
 
+    // Resident 256-thread frame CTAs per SM the register allocation must
+    // allow.  The count ptxas prints for the kernel leaves out its
+    // non-inlined callees (the sort and sweep): unbounded, the kernel
+    // launched at 150 registers, one CTA per SM.  Three CTAs (80 registers,
+    // 36 bytes spilled) took a settled 4,096-world step from 8.05 to
+    // 6.87 ms; four (64 registers) 6.95 ms.
+#ifndef RBPS_FRAME_MIN_BLOCKS
+#define RBPS_FRAME_MIN_BLOCKS 3
+#endif
     template <class T, class P>
-    __global__ void __launch_bounds__(kMaxBlock) k_phase_frame(const Engine<T, P> E, uint32_t ctr)
+    __global__ void __launch_bounds__(kMaxBlock, RBPS_FRAME_MIN_BLOCKS) k_phase_frame(const Engine<T, P> E, uint32_t ctr)
     {
         __shared__ BlockShared sh;
         __shared__ uint32_t sort_smem[kSmemSortWords];
@@ -1738,8 +2041,15 @@ namespace rbps_gpu
     // grid-stride loop.  (Written out in each kernel: a helper taking the
     // kernel's Engine by reference inside a lambda made the compiler copy
     // the whole parameter block to the stack, 650 bytes a thread.)
+    // Resident 256-thread narrowphase CTAs per SM, both kernels.  Unbounded,
+    // k_flat_narrow launched at 162 registers (one CTA per SM) and the
+    // box-box kernel at 87 (two); at three each (80 registers) the step
+    // above went from 6.87 to 6.64 ms.
+#ifndef RBPS_NARROW_MIN_BLOCKS
+#define RBPS_NARROW_MIN_BLOCKS 3
+#endif
     template <class T, class P>
-    __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow(const Engine<T, P> E)
+    __global__ void __launch_bounds__(kMaxBlock, RBPS_NARROW_MIN_BLOCKS) k_flat_narrow(const Engine<T, P> E)
     {
         // every class but box-box: [0, off(bb)) and [off(bb + 1), total)
         const uint32_t total = E.gcol[kGcolOff + kPairClasses];
@@ -1759,7 +2069,7 @@ namespace rbps_gpu
     // The box-box class on its own: its SAT, clipping buffers and registers
     // stay out of the kernel that runs every other class.
     template <class T, class P>
-    __global__ void __launch_bounds__(kMaxBlock) k_flat_narrow_boxbox(const Engine<T, P> E)
+    __global__ void __launch_bounds__(kMaxBlock, RBPS_NARROW_MIN_BLOCKS) k_flat_narrow_boxbox(const Engine<T, P> E)
     {
         const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
         const uint32_t n = bb1 - bb0;
@@ -2276,9 +2586,9 @@ namespace rbps_gpu
     {
         k_phase_frame<T, P><<<pl.grid[kKFrame], pl.block[kKFrame], 0, stream>>>(e, 0);
         k_flat_prefix<T, P><<<1, kMaxBlock, 0, stream>>>(e);
-        k_type_count<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+        k_type_count<T, P><<<fl.grid_sort, kMaxBlock, 0, stream>>>(e);
         k_type_scan<T, P><<<1, 32, 0, stream>>>(e);
-        k_type_scatter<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+        k_type_scatter<T, P><<<fl.grid_sort, kMaxBlock, 0, stream>>>(e);
         for (int s = 0; s < e.substeps; ++s)
         {
             if (e.gjk_list)
@@ -2306,12 +2616,21 @@ namespace rbps_gpu
         return cudaGetLastError();
     }
 
-    // kernel 0: narrowphase, 1: substep
+    // kernel 0: narrowphase, 1: substep, 2: class sort
     template <class T, class P>
     cudaError_t occupancy_flat(int kernel, int block, int *blocks_per_sm, size_t fl_smem)
     {
         if (kernel == 0)
             return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_flat_narrow<T, P>, block, 0);
+        if (kernel == 2)
+        {
+            int a = 0, b = 0;
+            cudaError_t rc = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_type_count<T, P>, block, 0);
+            if (rc == cudaSuccess)
+                rc = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_type_scatter<T, P>, block, 0);
+            *blocks_per_sm = a < b ? a : b;
+            return rc;
+        }
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_substep<T, P>, block, fl_smem);
     }
 

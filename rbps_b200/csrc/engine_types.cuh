@@ -293,6 +293,7 @@ namespace rbps_gpu
     struct FlatLaunch
     {
         int grid_narrow, grid_solve, block_solve;
+        int grid_sort;       // the class-sort kernels: every CTA they can keep resident
         size_t substep_smem; // dynamic shared memory of k_substep
         // a second stream on which the box-box narrowphase runs beside the
         // other classes' (fork / join events), or null for one stream
