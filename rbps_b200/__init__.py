@@ -285,7 +285,9 @@ class Batch:
 
     def profile(self):
         """(n_worlds, 16) uint64: phase cycles (PROFILE_PHASES order), then
-        slot 12 = CTA, 13 / 14 = start / end globaltimer ns of the last step."""
+        slot 12 = CTA, 13 / 14 = start / end globaltimer ns of the last step.
+        For worlds on one CTA, slots 10, 11 and 15 split the broadphase: the
+        endpoint sort, the sweep and the pair order (cycles)."""
         out = np.zeros((self.n_worlds, 16), np.uint64)
         _check(lib().rbps_batch_get_profile(self.h, out.ctypes.data_as(C.POINTER(C.c_uint64)), self.n_worlds))
         return out

@@ -1646,10 +1646,10 @@ static long enqueue_step(rbps_batch *b, const Engine<T, P> &e)
         {
             if (launch_step_flat<T, P>(e, b->phase, b->flat, b->stream) != cudaSuccess)
                 return RBPS_ERR_CUDA;
-            // frame, prefix, 3 class-sort kernels, stats; per substep the two
-            // narrowphase kernels, the GJK pass (batches with hulls) and the
-            // substep
-            launches += 6 + (long)b->desc.substeps * (e.gjk_list ? 4 : 3);
+            // frame, prefix, 3 class-sort kernels, stats; per substep the
+            // three narrowphase kernels, the GJK pass (batches with hulls)
+            // and the substep
+            launches += 6 + (long)b->desc.substeps * (e.gjk_list ? 5 : 4);
         }
         else
         {

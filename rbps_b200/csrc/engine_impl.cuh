@@ -216,6 +216,18 @@ namespace rbps_gpu
     }
 
     // ------------------------------------------------------------ broadphase
+    // Sub-phase timer of the broadphase: the CTA's thread 0 adds the cycles
+    // since t to slot s of prof (null when profiling is off) and restarts t.
+    __device__ __forceinline__ void sub_mark(unsigned long long *prof, int s, long long &t)
+    {
+        if (prof && threadIdx.x == 0)
+        {
+            const long long now = clock64();
+            prof[s] += (unsigned long long)(now - t);
+            t = now;
+        }
+    }
+
     // One-CTA fast path of the endpoint sort, in the staging area `smem`
     // (kSmemSortWords words).  moved[i] (shared) flags the previous
     // positions whose keys the frame's object update rewrote.  When the
@@ -347,15 +359,21 @@ namespace rbps_gpu
     // first plus the number of the group's entries with a smaller i.  The
     // first min(total, pair_cap) pairs are written to S.pr_a / S.pr_b (pk =
     // j, pv = identity).  Returns the pair count, or ~0u when the hits do not
-    // fit the staging list; S.cnt is complete then, and the caller emits and
-    // sorts in global memory.  Every thread of the CTA must call it.
+    // fit the staging lists ((kSmemSortWords - 2 nep) / 2 entries each: 3,104
+    // at the largest nep); S.cnt is complete then, and the caller emits and
+    // sorts in global memory.  Every thread of the CTA must call it.  prof:
+    // sub-timers (sweep, pair order), or null.
     template <class SC>
     __device__ __noinline__ uint32_t sweep_staged(const FatBox *fat, const uint32_t *ep_id, const uint32_t *ep_pos,
                                                   uint32_t nep, uint32_t id_limit, uint32_t pair_cap, int *error,
-                                                  const SC &S, ScanShared &sh, uint32_t *smem)
+                                                  const SC &S, ScanShared &sh, uint32_t *smem,
+                                                  unsigned long long *prof)
     {
-        uint32_t *hist = smem, *fill = smem + kSmemSortMax;
-        uint32_t *lst = smem + 2 * kSmemSortMax, *grp = smem + 3 * kSmemSortMax;
+        long long tclk = prof ? clock64() : 0;
+        // hist and fill per endpoint, then the two hit lists in what is left
+        const uint32_t cap = (kSmemSortWords - 2 * nep) / 2;
+        uint32_t *hist = smem, *fill = smem + nep;
+        uint32_t *lst = smem + 2 * nep, *grp = lst + cap;
         const uint32_t B = blockDim.x, t = threadIdx.x, lane = t & 31u;
         for (uint32_t i = t; i < nep; i += B)
         {
@@ -389,7 +407,7 @@ namespace rbps_gpu
                         s = __shfl_sync(act, s, leader) + __popc(hm & ((1u << lane) - 1u));
                         if (hit)
                         {
-                            if (s < kSmemSortMax)
+                            if (s < cap)
                                 lst[s] = (i << 16) | j;
                             atomicAdd(&hist[j], 1u);
                             ++c;
@@ -400,8 +418,9 @@ namespace rbps_gpu
             S.cnt[i] = c;
         }
         __syncthreads();
+        sub_mark(prof, kPhSweep, tclk);
         const uint32_t total = sh.bcast[3];
-        if (total > kSmemSortMax)
+        if (total > cap)
             return ~0u;
         // first slot of each j
         const uint32_t per = (nep + B - 1) / B;
@@ -450,6 +469,7 @@ namespace rbps_gpu
             }
         }
         __syncthreads();
+        sub_mark(prof, kPhPairOrder, tclk);
         return total;
     }
 
@@ -465,9 +485,11 @@ namespace rbps_gpu
     __device__ __noinline__ uint32_t sap_sort_sweep(const Team &tm, const FatBox *fat, uint32_t *ep_key, uint32_t *ep_id,
                                        uint32_t *ep_pos, uint32_t nbp, uint32_t id_limit, uint32_t pair_cap,
                                        int *error, const SC &S, BlockShared &sh, uint32_t *sort_smem = nullptr,
-                                       float4 *yz = nullptr, const uint32_t *moved = nullptr)
+                                       float4 *yz = nullptr, const uint32_t *moved = nullptr,
+                                       unsigned long long *prof = nullptr)
     {
         const uint32_t nep = 2 * nbp;
+        long long tclk = prof ? clock64() : 0;
         constexpr bool kBlock = std::is_same<Team, BlockTeam>::value;
         const bool staged = kBlock && sort_smem != nullptr && nep <= kSmemSortMax && blockDim.x >= 128;
         bool merged = false;
@@ -491,6 +513,7 @@ namespace rbps_gpu
             if (i + 1 < nep && ep_key[i] > ep_key[i + 1])
                 set_error_at(error, kErrInternal, 4, i); // the endpoint sort must leave the keys ordered
         }
+        sub_mark(prof, kPhEndpointSort, tclk);
         // A grid team's sweep reads every object of an overlap run; most fail
         // on y or z.  With yz, it first tests 16-byte float extents rounded
         // outward and reads the 48-byte double box only where they overlap,
@@ -508,7 +531,10 @@ namespace rbps_gpu
         if constexpr (kBlock)
             if (staged)
             {
-                const uint32_t n = sweep_staged(fat, ep_id, ep_pos, nep, id_limit, pair_cap, error, S, sh, sort_smem);
+                const uint32_t n =
+                    sweep_staged(fat, ep_id, ep_pos, nep, id_limit, pair_cap, error, S, sh, sort_smem, prof);
+                if (prof && threadIdx.x == 0)
+                    tclk = clock64();
                 if (n != ~0u)
                 {
                     if (tm.leader())
@@ -650,6 +676,7 @@ namespace rbps_gpu
                 }
             }
         tm.sync();
+        sub_mark(prof, kPhSweep, tclk);
         // reference emission order: stable sort by the later opening position
         const int bits = nep > 1 ? 32 - __clz(nep - 1) : 1;
         team_sort_staged(tm, S.pk, S.pv, S.pk2, S.pv2, total, bits, S.counts, S.tile_sums, sh, sort_smem);
@@ -657,12 +684,15 @@ namespace rbps_gpu
             if (S.pk[k] > S.pk[k + 1])
                 set_error_at(error, kErrInternal, 5, k); // pair sort must leave the keys ordered
         tm.sync(); // the caller rewrites S.pk next
+        sub_mark(prof, kPhPairOrder, tclk);
         return total;
     }
 
+    // prof: the world's phase-timer slots for the sort / sweep / pair-order
+    // sub-timers (one-CTA teams; null otherwise).
     template <class T, class P, class Team>
     __device__ uint32_t broadphase(const Engine<T, P> &E, const Team &tm, const WorldDev &W, const Scr<T, P> &S,
-                                   BlockShared &sh, uint32_t *sort_smem = nullptr)
+                                   BlockShared &sh, uint32_t *sort_smem = nullptr, unsigned long long *prof = nullptr)
     {
         const uint32_t nbp = W.n_bp;
         const uint32_t eb = 2 * W.bp_off;
@@ -723,7 +753,7 @@ namespace rbps_gpu
         }
         tm.sync();
         return sap_sort_sweep(tm, fat, ep_key, ep_id, ep_pos, nbp, nep, W.pair_cap, E.error, S, sh, sort_smem,
-                              W.n_bodies > kGridWorldBodies ? S.yz : nullptr, moved);
+                              W.n_bodies > kGridWorldBodies ? S.yz : nullptr, moved, prof);
     }
 
     // Filtered SAP pairs followed by the plane candidates; returns the count.
@@ -1372,7 +1402,8 @@ namespace rbps_gpu
             S.misc[kMiscMaxColors] = 0u;
             S.misc[kMiscColorValid] = 0u; // a new candidate list: no colouring yet
         }
-        const uint32_t n_pairs = broadphase(E, tm, W, S, sh, sort_smem);
+        const uint32_t n_pairs =
+            broadphase(E, tm, W, S, sh, sort_smem, std::is_same<Team, BlockTeam>::value ? prof_slots(E, tm, w) : nullptr);
         clk.mark(kPhBroadphase);
         const uint32_t n_cand = build_candidates(E, tm, W, S, n_pairs, sh);
         if (tm.leader())
@@ -1894,13 +1925,24 @@ namespace rbps_gpu
             E.wcoff[E.n_small] = carry;
     }
 
-    // Shape-pair class of a candidate: index of (kind a, kind b) over the
-    // five shape kinds, 25 classes.
+    // Shape-pair class of a candidate, 25 classes over (kind a, kind b) with
+    // the kinds folded to sphere, box, capsule, plane and "other": the 16
+    // pairs of the four common kinds first (ia * 4 + ib; box-box is 5), then
+    // the pairs with an other kind (16-20 other first, 21-24 other second),
+    // so one kernel takes [0, 16) but box-box and another [16, 25).
     __device__ __forceinline__ uint32_t kind_index(int kind)
     {
         return kind == kSphere ? 0u : kind == kBox ? 1u : kind == kCapsule ? 2u : kind == kPlane ? 3u : 4u;
     }
-    constexpr uint32_t kClassBoxBox = 1u * 5u + 1u; // cand_class of a box-box pair
+    constexpr uint32_t kClassBoxBox = 1u * 4u + 1u; // cand_class of a box-box pair
+    constexpr uint32_t kClassCommonEnd = 16u;        // classes [0, 16): common kinds only
+
+    __device__ __forceinline__ uint32_t pair_class(uint32_t ia, uint32_t ib)
+    {
+        if (ia < 4u && ib < 4u)
+            return ia * 4u + ib;
+        return ia == 4u ? 16u + ib : 21u + ia;
+    }
 
     // The small world holding flat candidate f: last q with wcoff[q] <= f.
     template <class T, class P>
@@ -1921,7 +1963,7 @@ namespace rbps_gpu
     template <class T, class P>
     __device__ __forceinline__ uint32_t cand_class(const Engine<T, P> &E, const WorldDev &W, const Cand &cd)
     {
-        return kind_index(E.shape[W.coll_off + cd.ca].kind) * 5u + kind_index(E.shape[W.coll_off + cd.cb].kind);
+        return pair_class(kind_index(E.shape[W.coll_off + cd.ca].kind), kind_index(E.shape[W.coll_off + cd.cb].kind));
     }
 
     template <class T, class P>
@@ -2051,8 +2093,8 @@ namespace rbps_gpu
     template <class T, class P>
     __global__ void __launch_bounds__(kMaxBlock, RBPS_NARROW_MIN_BLOCKS) k_flat_narrow(const Engine<T, P> E)
     {
-        // every class but box-box: [0, off(bb)) and [off(bb + 1), total)
-        const uint32_t total = E.gcol[kGcolOff + kPairClasses];
+        // the common-kind classes but box-box: [0, off(bb)) and [off(bb + 1), off(16))
+        const uint32_t total = E.gcol[kGcolOff + kClassCommonEnd];
         const uint32_t bb0 = E.gcol[kGcolOff + kClassBoxBox], bb1 = E.gcol[kGcolOff + kClassBoxBox + 1];
         const uint32_t n = total - (bb1 - bb0);
         const uint32_t per_warp = E.narrow_per_warp, lane = threadIdx.x & 31u;
@@ -2062,7 +2104,25 @@ namespace rbps_gpu
         {
             const uint32_t end = min(n, base + per_warp);
             for (uint32_t k = base + lane; k < end; k += 32)
-                narrow_flat<T, P, kSelNoBoxBox>(E, k < bb0 ? k : k + (bb1 - bb0));
+                narrow_flat<T, P, kSelCommon>(E, k < bb0 ? k : k + (bb1 - bb0));
+        }
+    }
+
+    // The classes with any other kind (ellipsoid, cylinder, cone, hull,
+    // heightmap, mesh): [off(16), total), with every routine but box-box.
+    template <class T, class P>
+    __global__ void __launch_bounds__(kMaxBlock, RBPS_NARROW_MIN_BLOCKS) k_flat_narrow_other(const Engine<T, P> E)
+    {
+        const uint32_t o0 = E.gcol[kGcolOff + kClassCommonEnd], total = E.gcol[kGcolOff + kPairClasses];
+        const uint32_t n = total - o0;
+        const uint32_t per_warp = E.narrow_per_warp, lane = threadIdx.x & 31u;
+        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+        for (uint32_t base = warp * per_warp; base < n; base += n_warps * per_warp)
+        {
+            const uint32_t end = min(n, base + per_warp);
+            for (uint32_t k = base + lane; k < end; k += 32)
+                narrow_flat<T, P, kSelNoBoxBox>(E, o0 + k);
         }
     }
 
@@ -2600,6 +2660,7 @@ namespace rbps_gpu
                 cudaEventRecord(fl.fork[s], stream);
                 cudaStreamWaitEvent(fl.side, fl.fork[s], 0);
                 k_flat_narrow_boxbox<T, P><<<fl.grid_narrow, kMaxBlock, 0, fl.side>>>(e);
+                k_flat_narrow_other<T, P><<<fl.grid_narrow, kMaxBlock, 0, fl.side>>>(e);
                 cudaEventRecord(fl.join[s], fl.side);
                 k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
                 cudaStreamWaitEvent(stream, fl.join[s], 0);
@@ -2608,6 +2669,7 @@ namespace rbps_gpu
             {
                 k_flat_narrow<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
                 k_flat_narrow_boxbox<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
+                k_flat_narrow_other<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
             }
             launch_gjk(e, stream);
             k_substep<T, P><<<fl.grid_solve, 128, fl.substep_smem, stream>>>(e);

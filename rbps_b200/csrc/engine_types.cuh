@@ -173,6 +173,10 @@ namespace rbps_gpu
         kPhVelUpdate = 7,
         kPhVelSolve = 8,
         kPhStats = 9,
+        // parts of kPhBroadphase on one-CTA teams, timed by the leader
+        kPhEndpointSort = 10,
+        kPhSweep = 11,
+        kPhPairOrder = 15,
         kProfCta = 12,
         kProfStartNs = 13,
         kProfEndNs = 14,

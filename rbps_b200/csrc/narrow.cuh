@@ -1565,10 +1565,11 @@ namespace rbps_gpu
     }
 
     // Sel selects the routines compiled in: kSelAll every pair; kSelNoBoxBox
-    // all but box-box; kSelBoxBox box-box only (the caller guarantees the
-    // kinds), so a kernel that never meets a box pair carries no box-box
-    // code, registers or clip buffers.
-    constexpr int kSelAll = 0, kSelNoBoxBox = 1, kSelBoxBox = 2;
+    // all but box-box; kSelBoxBox box-box only; kSelCommon the pairs of
+    // spheres, boxes, capsules and planes but box-box (the caller guarantees
+    // the kinds), so a kernel carries only the code, registers and local
+    // buffers of the routines it can meet.
+    constexpr int kSelAll = 0, kSelNoBoxBox = 1, kSelBoxBox = 2, kSelCommon = 3;
 
     template <class T, int Sel = kSelAll>
     __device__ __forceinline__ int dispatch_pair(const ShapeDev &sa, const tf<T> &ta, const ShapeDev &sb,
@@ -1579,6 +1580,7 @@ namespace rbps_gpu
                            tb, m)
                        ? kHit
                        : kMiss;
+        constexpr bool kAny = Sel != kSelCommon; // kinds beyond the four common ones
         const int ka = sa.kind, kb = sb.kind;
         bool hit = false;
         bool flip = false;
@@ -1590,6 +1592,10 @@ namespace rbps_gpu
                 hit = box_plane(vec3<T>(T(sa.p[0]), T(sa.p[1]), T(sa.p[2])), ta, sb, tb, m);
             else if (ka == kCapsule)
                 hit = capsule_plane(T(sa.p[0]), T(sa.p[1]), ta, sb, tb, m);
+            else if (!kAny)
+            {
+                // no other kind reaches a kSelCommon kernel
+            }
             else if (ka == kHull)
                 hit = hull_plane(hs, sa.hull, ta, sb, tb, m);
             else if (ka == kCylinder)
@@ -1608,6 +1614,10 @@ namespace rbps_gpu
                 hit = box_plane(vec3<T>(T(sb.p[0]), T(sb.p[1]), T(sb.p[2])), tb, sa, ta, m);
             else if (kb == kCapsule)
                 hit = capsule_plane(T(sb.p[0]), T(sb.p[1]), tb, sa, ta, m);
+            else if (!kAny)
+            {
+                // no other kind reaches a kSelCommon kernel
+            }
             else if (kb == kHull)
                 hit = hull_plane(hs, sb.hull, tb, sa, ta, m);
             else if (kb == kCylinder)
@@ -1620,7 +1630,7 @@ namespace rbps_gpu
                 m.normal = -m.normal;
             return hit ? kHit : kMiss;
         }
-        if (ka == kMesh || kb == kMesh)
+        if (kAny && (ka == kMesh || kb == kMesh))
         {
             if (ka == kHeightmap || kb == kHeightmap)
                 return kMiss; // no Mesh / Heightmap algorithm: the primary one finds nothing
@@ -1634,7 +1644,7 @@ namespace rbps_gpu
             }
             return hit ? kHit : kMiss;
         }
-        if (ka == kHeightmap || kb == kHeightmap)
+        if (kAny && (ka == kHeightmap || kb == kHeightmap))
         {
             if (kb == kHeightmap)
                 hit = shape_heightmap(sa, ta, sb, hs, m);
@@ -1646,7 +1656,7 @@ namespace rbps_gpu
             }
             return hit ? kHit : kMiss;
         }
-        if (gjk_kind(ka) || gjk_kind(kb))
+        if (kAny && (gjk_kind(ka) || gjk_kind(kb)))
             return kNeedsGjk;
         if (ka == kSphere && kb == kSphere)
             hit = sphere_sphere(T(sa.p[0]), ta, T(sb.p[0]), tb, m);
