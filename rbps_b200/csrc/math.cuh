@@ -26,8 +26,23 @@ namespace rbps_gpu
     RBPS_HD float rabs(float x) { return fabsf(x); }
     RBPS_HD double sqrt_t(double x) { return sqrt(x); }
     RBPS_HD float sqrt_t(float x) { return sqrtf(x); }
+    // x / y where y is known to be at least EPSILON (1e-9) in magnitude: in
+    // double correctly rounded, as the reference divides; in float on the
+    // device the hardware's approximate division (within 2 ulp; it differs
+    // in kind from IEEE division only for |y| above 2^126 or denormal, which
+    // such a y never is).  The FP32 solver rows divide only through here.
+    RBPS_HD double div_guarded(double x, double y) { return x / y; }
+    RBPS_HD float div_guarded(float x, float y)
+    {
+#ifdef __CUDA_ARCH__
+        return __fdividef(x, y);
+#else
+        return x / y;
+#endif
+    }
+    // 1 / sqrt(x) for x >= EPSILON (the normalisations guard it).
     RBPS_HD double inv_sqrt(double x) { return 1.0 / sqrt(x); }
-    RBPS_HD float inv_sqrt(float x) { return 1.0f / sqrtf(x); }
+    RBPS_HD float inv_sqrt(float x) { return div_guarded(1.0f, sqrtf(x)); }
     // Squared-length threshold below which a cross product of two unit axes
     // counts as degenerate (parallel edges).  The reference uses EPSILON^2 in
     // double (BoxBox.hpp:45, CapsuleBox.hpp:112); in float the rounding noise
@@ -121,7 +136,7 @@ namespace rbps_gpu
     {
         const T mag_sq = q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z;
         if (rabs(T(1.0) - mag_sq) < T(kQuatUlp))
-            return q * (T(2.0) / (T(1.0) + mag_sq));
+            return q * div_guarded(T(2.0), T(1.0) + mag_sq);
         if (mag_sq < T(kEpsilon))
             return {T(1), T(0), T(0), T(0)};
         return q * inv_sqrt(mag_sq);

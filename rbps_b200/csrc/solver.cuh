@@ -300,7 +300,7 @@ namespace rbps_gpu
             const T denom = w_a + w_b;
             if (!(denom < T(kEpsilon)))
             {
-                const T dl = -d / denom;
+                const T dl = div_guarded(-d, denom);
                 c.lam_n += dl;
                 if (c.lam_n > T(0.0))
                     c.lam_n = T(0.0);
@@ -330,7 +330,7 @@ namespace rbps_gpu
             const T denom = w_a + w_b;
             if (denom < T(kEpsilon))
                 return;
-            const T dl = -slip / denom;
+            const T dl = div_guarded(-slip, denom);
             const T old = c.lam_t;
             c.lam_t += dl;
             const T cone = static_friction * c.lam_n;
@@ -366,7 +366,7 @@ namespace rbps_gpu
         T dv_t = T(0.0);
         if (v_t_mag > T(kEpsilon))
         {
-            const T limit = dynamic_friction * rabs(c.lam_n) / h;
+            const T limit = div_guarded(dynamic_friction * rabs(c.lam_n), h);
             dv_t = -rmin(limit, v_t_mag);
         }
         smat3<T> Ia, Ib;
@@ -375,19 +375,19 @@ namespace rbps_gpu
         const T denom_n = w_a_n + w_b_n;
         if (denom_n > T(kEpsilon) && rabs(dv_n) > T(kEpsilon))
         {
-            const vec3<T> imp = (dv_n / denom_n) * n;
+            const vec3<T> imp = div_guarded(dv_n, denom_n) * n;
             pos_vel_impulse(A, Ia, imp, r_a);
             pos_vel_impulse(Bb, Ib, -imp, r_b);
         }
         if (v_t_mag > T(kEpsilon) && rabs(dv_t) > T(kEpsilon))
         {
-            const vec3<T> t = v_t / v_t_mag;
+            const vec3<T> t = v_t * div_guarded(T(1.0), v_t_mag);
             const T w_a_t = pos_w(A, r_a, t, Ia);
             const T w_b_t = pos_w(Bb, r_b, t, Ib);
             const T denom_t = w_a_t + w_b_t;
             if (denom_t > T(kEpsilon))
             {
-                const vec3<T> imp = (dv_t / denom_t) * t;
+                const vec3<T> imp = div_guarded(dv_t, denom_t) * t;
                 pos_vel_impulse(A, Ia, imp, r_a);
                 pos_vel_impulse(Bb, Ib, -imp, r_b);
             }
@@ -457,7 +457,7 @@ namespace rbps_gpu
             if constexpr (sizeof(T) == 8)
                 d = normalize(value);
             else
-                d = value * (T(1) / mag);
+                d = value * div_guarded(T(1), mag);
         }
         r.dir = V4<T>{d.x, d.y, d.z, mag};
     }
@@ -471,7 +471,7 @@ namespace rbps_gpu
         const T mag = length(value);
         vec3<T> d(T(1.0), T(0.0), T(0.0));
         if (mag > T(kEpsilon))
-            d = value * (T(1.0) / mag);
+            d = value * div_guarded(T(1.0), mag);
         r.dir = V4<T>{d.x, d.y, d.z, mag};
     }
 
