@@ -1373,6 +1373,24 @@ namespace rbps_gpu
         }
     }
 
+    // Candidate and bodies of colour-ordered slot q: from the team's shared
+    // slots when the colouring left them there, else as slot_pair.
+    template <class T, class P>
+    __device__ __forceinline__ void slot_entry(const Scr<T, P> &S, const uint32_t *book, const uint2 *slots, uint32_t q,
+                                               uint32_t &c, uint32_t &ba, uint32_t &bb)
+    {
+        if (slots)
+        {
+            const uint2 e = slots[q];
+            c = e.x;
+            ba = e.y & 0xffffu;
+            bb = e.y >> 16;
+            return;
+        }
+        c = S.corder[q];
+        slot_pair(S, book, q, c, ba, bb);
+    }
+
     // Asks L2 for every 128-byte line of [p, p + bytes) (prefetch.global.L2).
     __device__ __forceinline__ void prefetch_l2_range(const void *p, size_t bytes)
     {
@@ -1510,7 +1528,7 @@ namespace rbps_gpu
 
     template <class T, class P, class Team>
     __device__ void phase_position_on(const Engine<T, P> &E, const Team &tm, uint32_t w, const Bodies<T, P> &B,
-                                      uint32_t boff, const uint32_t *book = nullptr)
+                                      uint32_t boff, const uint32_t *book = nullptr, const uint2 *slots = nullptr)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
@@ -1549,10 +1567,10 @@ namespace rbps_gpu
         {
             const uint32_t *coff = book ? book + 66 : S.misc + kMiscCOff;
             const uint32_t n_colors = book ? book[132] : S.misc[kMiscNColors];
+            const bool sl = slots && book && book[133];
             sweep_colors(tm, coff, n_colors, [&](uint32_t q) {
-                const uint32_t c = S.corder[q];
-                uint32_t ba, bb;
-                slot_pair(S, book, q, c, ba, bb);
+                uint32_t c, ba, bb;
+                slot_entry(S, book, sl ? slots : nullptr, q, c, ba, bb);
                 solve_pair_position(B, E.inv_h, boff + ba, boff + bb, S.cc[c]);
             });
             if (coff[kColorSerial + 1] > coff[kColorSerial])
@@ -1573,7 +1591,7 @@ namespace rbps_gpu
                 if (tm.leader())
                     for (uint32_t q = serial0; q < coff[kColorSerial + 1]; ++q)
                     {
-                        const uint32_t c = S.corder[q];
+                        const uint32_t c = sl ? slots[q].x : S.corder[q];
                         const Cand cd = S.cand[c];
                         solve_pair_position(B, E.inv_h, boff + cd.ba, boff + cd.bb, S.cc[c]);
                     }
@@ -1621,7 +1639,7 @@ namespace rbps_gpu
     // Velocity solve (World.hpp:176-180): restitution / friction, joint damping.
     template <class T, class P, class Team>
     __device__ void phase_velocity_on(const Engine<T, P> &E, const Team &tm, uint32_t w, const Bodies<T, P> &B,
-                                      uint32_t boff, const uint32_t *book = nullptr)
+                                      uint32_t boff, const uint32_t *book = nullptr, const uint2 *slots = nullptr)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
@@ -1651,10 +1669,10 @@ namespace rbps_gpu
         {
             const uint32_t *coff = book ? book + 66 : S.misc + kMiscCOff;
             const uint32_t n_colors = book ? book[132] : S.misc[kMiscNColors];
+            const bool sl = slots && book && book[133];
             sweep_colors(tm, coff, n_colors, [&](uint32_t q) {
-                const uint32_t c = S.corder[q];
-                uint32_t ba, bb;
-                slot_pair(S, book, q, c, ba, bb);
+                uint32_t c, ba, bb;
+                slot_entry(S, book, sl ? slots : nullptr, q, c, ba, bb);
                 solve_pair_velocity(B, E.h, boff + ba, boff + bb, S.cc[c]);
             });
             if (coff[kColorSerial + 1] > coff[kColorSerial])
@@ -1673,7 +1691,7 @@ namespace rbps_gpu
                 if (tm.leader())
                     for (uint32_t q = serial0; q < coff[kColorSerial + 1]; ++q)
                     {
-                        const uint32_t c = S.corder[q];
+                        const uint32_t c = sl ? slots[q].x : S.corder[q];
                         const Cand cd = S.cand[c];
                         solve_pair_velocity(B, E.h, boff + cd.ba, boff + cd.bb, S.cc[c]);
                     }
@@ -2264,10 +2282,72 @@ namespace rbps_gpu
     // against them, which on resting piles leaves the leader a few
     // candidates instead of all.  Returns the number of regular colours to
     // every thread.
+    // The greedy pass over one staged chunk on the team's first warp, with
+    // the serial pass's result.  Candidates are taken 32 at a time; in rounds,
+    // every candidate none of whose dynamic bodies belongs to an earlier
+    // uncoloured candidate of its 32 takes the lowest colour free on its
+    // bodies.  It sees exactly the masks the serial pass would: every earlier
+    // candidate on those bodies is coloured, no later one is.  Candidates
+    // coloured in one round share no dynamic body, and the earliest
+    // uncoloured one is always ready, so at most 32 rounds run.  claim holds
+    // a word per body of scratch (the lowest uncoloured lane on the body).
+    __device__ __forceinline__ void greedy_chunk_warp(const uint32_t *stage, uint8_t *scol, uint32_t m,
+                                                      unsigned long long *mask, uint32_t *cnt, uint32_t *claim)
+    {
+        const uint32_t lane = threadIdx.x & 31u;
+        for (uint32_t k0 = 0; k0 < m; k0 += 32)
+        {
+            const uint32_t k = k0 + lane;
+            const bool live = k < m;
+            const uint32_t r = live ? stage[k] : 0u;
+            const uint32_t a = r & 2047u, b = (r >> 11) & 2047u;
+            const bool da = live && ((r >> 22) & 1u), db = live && ((r >> 23) & 1u);
+            bool pending = live;
+            while (__any_sync(0xffffffffu, pending))
+            {
+                if (pending)
+                {
+                    if (da)
+                        claim[a] = ~0u;
+                    if (db)
+                        claim[b] = ~0u;
+                }
+                __syncwarp();
+                if (pending)
+                {
+                    if (da)
+                        atomicMin(&claim[a], lane);
+                    if (db)
+                        atomicMin(&claim[b], lane);
+                }
+                __syncwarp();
+                if (pending && (!da || claim[a] == lane) && (!db || claim[b] == lane))
+                {
+                    const unsigned long long used = (da ? mask[a] : 0ull) | (db ? mask[b] : 0ull);
+                    uint32_t col = kColorSerial;
+                    if (used != ~0ull)
+                    {
+                        col = (uint32_t)(__ffsll((long long)~used) - 1);
+                        const unsigned long long bit = 1ull << col;
+                        if (da)
+                            mask[a] |= bit;
+                        if (db)
+                            mask[b] |= bit;
+                    }
+                    scol[k] = (uint8_t)col;
+                    atomicAdd(&cnt[col], 1u);
+                    pending = false;
+                }
+                __syncwarp();
+            }
+        }
+    }
+
     template <class T, class P, class Team>
     __device__ uint32_t greedy_color_world(const Engine<T, P> &E, const Team &tm, uint32_t w,
                                            unsigned long long *mask, ScanShared &sh, uint32_t *book,
-                                           uint32_t *stage = nullptr)
+                                           uint32_t *stage = nullptr, uint32_t *claim = nullptr,
+                                           uint2 *slots = nullptr, uint32_t slot_cap = 0)
     {
         const WorldDev W = E.worlds[w];
         const Scr<T, P> S = world_scratch(E, W);
@@ -2323,7 +2403,12 @@ namespace rbps_gpu
                                ((type[cd.bb] == kDynamic ? 1u : 0u) << 23);
                 }
                 tm.sync();
-                if (tm.leader())
+                if (claim)
+                {
+                    if (tm.rank() < 32)
+                        greedy_chunk_warp(stage, scol, m, mask, cnt, claim);
+                }
+                else if (tm.leader())
                     for (uint32_t k = 0; k < m; ++k)
                     {
                         const uint32_t r = stage[k];
@@ -2400,21 +2485,34 @@ namespace rbps_gpu
                 misc[kMiscMaxColors] = ncol;
             misc[kMiscColorValid] = 1u;
             if (book)
+            {
                 book[132] = ncol;
+                book[133] = slots && n_act <= slot_cap ? 1u : 0u;
+            }
         }
         tm.sync();
+        // the colour-ordered slots go to shared memory when they fit
+        const bool in_smem = slots && n_act <= slot_cap;
         for (uint32_t q = tm.rank(); q < n_act; q += tm.size())
         {
             const uint32_t c = S.alist[q];
             const uint32_t slot = atomicAdd(&cnt[S.color[c]], 1u);
-            S.corder[slot] = c;
             // a team with its world in shared memory keeps the body pair of
-            // each slot beside corder (world-local indices < 65536), so the
-            // colour-by-colour solves need not read the candidate first
-            if (book)
+            // each slot beside its candidate (world-local indices < 65536), so
+            // the colour-by-colour solves need not read the candidate first
+            if (in_smem)
             {
                 const Cand cd = S.cand[c];
-                S.act[slot] = cd.ba | (cd.bb << 16);
+                slots[slot] = make_uint2(c, cd.ba | (cd.bb << 16));
+            }
+            else
+            {
+                S.corder[slot] = c;
+                if (book)
+                {
+                    const Cand cd = S.cand[c];
+                    S.act[slot] = cd.ba | (cd.bb << 16);
+                }
             }
             // the position and velocity solves read this candidate's contact
             // block colour by colour, each read behind a barrier: start it
@@ -2463,18 +2561,24 @@ namespace rbps_gpu
         // colouring stage: kColorStage packed candidate records + their colours
         static constexpr size_t kStage = kColorStage * (sizeof(uint32_t) + 1);
         static constexpr bool kPrev = RBPS_SMEM_PREV != 0;
+        // colour-ordered slots (candidate, packed body pair) for up to
+        // kSlotsPerBody x cap contacting candidates
+        static constexpr uint32_t kSlotsPerBody = 2;
         static constexpr size_t kPerBody = sizeof(unsigned long long) + (kPrev ? 2 : 1) * sizeof(V4<P>) +
-                                           (kPrev ? 2 : 1) * sizeof(Q4<T>) + 2 * sizeof(V4<T>) + 1;
+                                           (kPrev ? 2 : 1) * sizeof(Q4<T>) + 2 * sizeof(V4<T>) + 1 +
+                                           kSlotsPerBody * sizeof(uint2);
 
         __host__ __device__ static size_t bytes(uint32_t cap) { return kBook + kStage + (size_t)cap * kPerBody; }
 
         __device__ static Bodies<T, P> view(unsigned char *p, uint32_t cap, const Bodies<T, P> &G, uint32_t body_off,
-                                            unsigned long long **mask, uint32_t **book, uint32_t **stage)
+                                            unsigned long long **mask, uint32_t **book, uint32_t **stage, uint2 **slots)
         {
             *book = reinterpret_cast<uint32_t *>(p);
             p += kBook;
             *stage = reinterpret_cast<uint32_t *>(p);
             p += kStage;
+            *slots = reinterpret_cast<uint2 *>(p);
+            p += (size_t)cap * kSlotsPerBody * sizeof(uint2);
             *mask = reinterpret_cast<unsigned long long *>(p);
             p += (size_t)cap * sizeof(unsigned long long);
             Bodies<T, P> V;
@@ -2520,17 +2624,21 @@ namespace rbps_gpu
         const bool local = smem && W.n_bodies <= cap;
         unsigned long long *mask = nullptr;
         uint32_t *book = nullptr, *stage = nullptr;
+        uint2 *slots = nullptr;
         Bodies<T, P> V = E.B;
         uint32_t boff = W.body_off;
         if (local)
         {
-            V = SmemWorld<T, P>::view(smem, cap, E.B, W.body_off, &mask, &book, &stage);
+            V = SmemWorld<T, P>::view(smem, cap, E.B, W.body_off, &mask, &book, &stage, &slots);
             boff = 0;
         }
         else
             mask = world_scratch(E, W).bmask;
         PhaseClock clk(prof_slots(E, tm, w), false);
-        greedy_color_world(E, tm, w, mask, sh, book, stage);
+        // the pose copy is not loaded yet: its first words serve the
+        // colouring as per-body scratch
+        greedy_color_world(E, tm, w, mask, sh, book, stage, local ? reinterpret_cast<uint32_t *>(V.pos) : nullptr, slots,
+                           cap * SmemWorld<T, P>::kSlotsPerBody);
         clk.mark(kPhColor);
         if (local)
         {
@@ -2555,8 +2663,8 @@ namespace rbps_gpu
             integrate_body(V, boff + b, E.h);
         tm.sync();
         clk.mark(kPhIntegrate);
-        phase_position_on(E, tm, w, V, boff, book);
-        phase_velocity_on(E, tm, w, V, boff, book);
+        phase_position_on(E, tm, w, V, boff, book, slots);
+        phase_velocity_on(E, tm, w, V, boff, book, slots);
         if (local)
         {
             const Bodies<T, P> &G = E.B;
