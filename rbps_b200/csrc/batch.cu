@@ -869,6 +869,7 @@ namespace
         e.solve_mode = b->desc.solve_mode;
         e.use_vel_exp = b->desc.use_velocity_expansion;
         e.check_state = b->check_state ? 1 : 0;
+        e.stats_in_substep = 0;
         e.narrow_per_warp = b->narrow_per_warp;
         e.color_chunk = b->color_chunk;
         e.work_counter = b->work_counter;
@@ -1646,10 +1647,11 @@ static long enqueue_step(rbps_batch *b, const Engine<T, P> &e)
         {
             if (launch_step_flat<T, P>(e, b->phase, b->flat, b->stream) != cudaSuccess)
                 return RBPS_ERR_CUDA;
-            // frame, prefix, 3 class-sort kernels, stats; per substep the
-            // three narrowphase kernels, the GJK pass (batches with hulls)
-            // and the substep
-            launches += 6 + (long)b->desc.substeps * (e.gjk_list ? 5 : 4);
+            // frame, prefix, 3 class-sort kernels, stats (only with dumps:
+            // otherwise the last substep writes them); per substep the three
+            // narrowphase kernels, the GJK pass (batches with hulls) and the
+            // substep
+            launches += (e.dump_cc || b->desc.substeps < 1 ? 6 : 5) + (long)b->desc.substeps * (e.gjk_list ? 5 : 4);
         }
         else
         {

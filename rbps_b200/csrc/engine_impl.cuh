@@ -2234,12 +2234,16 @@ namespace rbps_gpu
     }
 
     // The contacting candidates of the world into S.alist, in candidate
-    // order, their colours reset; the others marked idle.  Returns the count.
+    // order, their colours reset; the others marked idle.  Returns the count;
+    // adds this thread's share of the contact rows to *rows.
     template <class T, class P, class Team>
-    __device__ uint32_t compact_active(const Team &tm, const Scr<T, P> &S, uint32_t n_cand, ScanShared &sh)
+    __device__ uint32_t compact_active(const Team &tm, const Scr<T, P> &S, uint32_t n_cand, ScanShared &sh,
+                                       uint32_t *rows)
     {
         return team_compact(tm, n_cand, S.alist, sh, [&](uint32_t c) {
-            const bool act = S.cc[c].n > 0;
+            const int n = S.cc[c].n;
+            *rows += (uint32_t)n;
+            const bool act = n > 0;
             S.color[c] = act ? 0xffffffffu : kColorIdle;
             return act;
         });
@@ -2255,10 +2259,12 @@ namespace rbps_gpu
     // total count.
     template <class T, class P, class Team>
     __device__ uint32_t compact_keep_active(const Team &tm, const Scr<T, P> &S, uint32_t n_cand, ScanShared &sh,
-                                            uint32_t *n_keep)
+                                            uint32_t *n_keep, uint32_t *rows)
     {
         const uint32_t kept = team_compact(tm, n_cand, S.alist, sh, [&](uint32_t c) {
-            const bool act = S.cc[c].n > 0;
+            const int n = S.cc[c].n;
+            *rows += (uint32_t)n;
+            const bool act = n > 0;
             const uint32_t old = S.color[c];
             const bool keep = act && old < kColorSerial;
             S.color[c] = keep ? old : act ? 0xffffffffu : kColorIdle;
@@ -2367,8 +2373,13 @@ namespace rbps_gpu
 #define RBPS_COLOR_REUSE 1
 #endif
         const bool reuse = RBPS_COLOR_REUSE && misc[kMiscColorValid] != 0u;
-        uint32_t n_keep = 0;
-        const uint32_t n_act = reuse ? compact_keep_active(tm, S, n_cand, sh, &n_keep) : compact_active(tm, S, n_cand, sh);
+        uint32_t n_keep = 0, rows = 0;
+        if (tm.leader())
+            misc[kMiscNContacts] = 0u; // this substep's contact rows, summed below
+        const uint32_t n_act = reuse ? compact_keep_active(tm, S, n_cand, sh, &n_keep, &rows)
+                                     : compact_active(tm, S, n_cand, sh, &rows);
+        if (rows) // after the compaction's closing barrier, so after the reset
+            atomicAdd(misc + kMiscNContacts, rows);
         const uint8_t *type = E.B.type + W.body_off;
         for (uint32_t q = tm.rank(); q < n_keep; q += tm.size())
         {
@@ -2611,6 +2622,44 @@ namespace rbps_gpu
         }
     };
 
+    // The statistics of a colored step, run by the last substep when no dump
+    // needs the stats phase (phase_stats, which it replaces): the state check
+    // on the world's bodies as the substep leaves them (the shared copy, or
+    // the batch arrays), then WorldStats from the counters the step kept
+    // (the contact rows are those the colouring counted this substep).
+    template <class T, class P, class Team>
+    __device__ void substep_stats(const Engine<T, P> &E, const Team &tm, uint32_t w, const Bodies<T, P> &V,
+                                  uint32_t boff)
+    {
+        const WorldDev W = E.worlds[w];
+        if (E.check_state)
+            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
+            {
+                const V4<P> x = V.pos[boff + b];
+                const Q4<T> q = V.rot[boff + b];
+                const V4<T> v = V.lin[boff + b], om = V.ang[boff + b];
+                const bool ok = isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(q.w) && isfinite(q.x) &&
+                                isfinite(q.y) && isfinite(q.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) &&
+                                isfinite(om.x) && isfinite(om.y) && isfinite(om.z);
+                if (!ok)
+                    set_error_at(E.error, kErrState, 7, w);
+            }
+        if (tm.leader())
+        {
+            const uint32_t *misc = world_scratch(E, W).misc;
+            WorldStats st;
+            st.n_pairs = misc[kMiscNPairs];
+            st.n_cand = misc[kMiscNCand];
+            st.n_contacts = misc[kMiscNContacts];
+            st.n_colors = misc[kMiscMaxColors];
+            st.n_serial = misc[kMiscCOff + kColorSerial + 1] - misc[kMiscCOff + kColorSerial];
+            st.n_gjk = misc[kMiscNGjk];
+            st.pad_[0] = st.pad_[1] = 0;
+            E.stats[w] = st;
+        }
+        tm.sync();
+    }
+
     // The rest of a substep for one world on team tm: colouring of the
     // contacting candidates, integrate (Body.cpp:18-39), position solve +
     // velocity update, velocity solve.  With `smem` (room for `cap` bodies)
@@ -2685,6 +2734,13 @@ namespace rbps_gpu
             }
             tm.sync();
         }
+        if (E.stats_in_substep)
+        {
+            PhaseClock sclk(prof_slots(E, tm, w), false);
+            substep_stats(E, tm, w, V, boff);
+            sclk.mark(kPhStats);
+            sclk.finish();
+        }
     }
 
     // The largest worlds (the first n_block_worlds of the list) get a whole
@@ -2752,6 +2808,9 @@ namespace rbps_gpu
     cudaError_t launch_step_flat(const Engine<T, P> &e, const PhaseLaunch &pl, const FlatLaunch &fl,
                                  cudaStream_t stream)
     {
+        // without dumps the last substep launch also writes the statistics
+        Engine<T, P> el = e;
+        el.stats_in_substep = e.dump_cc || e.substeps < 1 ? 0 : 1;
         k_phase_frame<T, P><<<pl.grid[kKFrame], pl.block[kKFrame], 0, stream>>>(e, 0);
         k_flat_prefix<T, P><<<1, kMaxBlock, 0, stream>>>(e);
         k_type_count<T, P><<<fl.grid_sort, kMaxBlock, 0, stream>>>(e);
@@ -2780,9 +2839,10 @@ namespace rbps_gpu
                 k_flat_narrow_other<T, P><<<fl.grid_narrow, kMaxBlock, 0, stream>>>(e);
             }
             launch_gjk(e, stream);
-            k_substep<T, P><<<fl.grid_solve, 128, fl.substep_smem, stream>>>(e);
+            k_substep<T, P><<<fl.grid_solve, 128, fl.substep_smem, stream>>>(s + 1 == e.substeps ? el : e);
         }
-        k_phase_stats<T, P><<<pl.grid[kKStats], pl.block[kKStats], 0, stream>>>(e, 1);
+        if (!el.stats_in_substep)
+            k_phase_stats<T, P><<<pl.grid[kKStats], pl.block[kKStats], 0, stream>>>(e, 1);
         return cudaGetLastError();
     }
 

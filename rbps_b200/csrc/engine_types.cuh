@@ -220,6 +220,10 @@ namespace rbps_gpu
         int solve_mode;
         int use_vel_exp;
         int check_state; // the stats phase reports a non-finite body state (RBPS_ERR_STATE)
+        // 1 on the last substep launch of a colored step without dumps: the
+        // substep kernel writes the world statistics and runs the state
+        // check itself, and no stats kernel follows
+        int stats_in_substep;
         // launch-shape knobs of the flat coloured pipeline (autotuned; results
         // do not depend on them): narrowphase candidates a warp takes per
         // pass (a multiple of 32), and active candidates the colouring stages
