@@ -2689,27 +2689,13 @@ namespace rbps_gpu
         greedy_color_world(E, tm, w, mask, sh, book, stage, local ? reinterpret_cast<uint32_t *>(V.pos) : nullptr, slots,
                            cap * SmemWorld<T, P>::kSlotsPerBody);
         clk.mark(kPhColor);
-        if (local)
-        {
-            const Bodies<T, P> &G = E.B;
-            for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
-            {
-                const uint32_t g = W.body_off + b;
-                V.pos[b] = G.pos[g];
-                V.rot[b] = G.rot[g];
-                V.lin[b] = G.lin[g];
-                V.ang[b] = G.ang[g];
-                if (SmemWorld<T, P>::kPrev)
-                {
-                    V.prev_pos[b] = G.prev_pos[g];
-                    V.prev_rot[b] = G.prev_rot[g];
-                }
-                V.type[b] = G.type[g];
-            }
-            tm.sync();
-        }
+        // integrate (Body.cpp:18-39); a world in shared memory is loaded
+        // into its copy by the same pass
         for (uint32_t b = tm.rank(); b < W.n_bodies; b += tm.size())
-            integrate_body(V, boff + b, E.h);
+            if (local)
+                integrate_body_into(E.B, W.body_off + b, V, b, E.h);
+            else
+                integrate_body(V, boff + b, E.h);
         tm.sync();
         clk.mark(kPhIntegrate);
         phase_position_on(E, tm, w, V, boff, book, slots);

@@ -112,6 +112,50 @@ namespace rbps_gpu
         B.set_q(i, normalize(q0 + r * q0));
     }
 
+    // integrate_body of body i of S, written to body j of D: the pose and
+    // velocities go to D (a static body is copied as it is), the previous
+    // pose to D's previous-pose arrays, and the type is copied.  The same
+    // operations in the same order as integrate_body; a team that keeps its
+    // world in shared memory loads and integrates each body in one pass.
+    template <class T, class P>
+    __device__ void integrate_body_into(const Bodies<T, P> &S, uint32_t i, const Bodies<T, P> &D, uint32_t j, T dt)
+    {
+        const uint8_t ty = S.type[i];
+        const V4<P> p0 = S.pos[i];
+        const Q4<T> r0 = S.rot[i];
+        const V4<T> l = S.lin[i];
+        const V4<T> a0 = S.ang[i];
+        D.type[j] = ty;
+        if (ty == kStatic)
+        {
+            D.pos[j] = p0;
+            D.rot[j] = r0;
+            D.lin[j] = l;
+            D.ang[j] = a0;
+            D.prev_pos[j] = S.prev_pos[i];
+            D.prev_rot[j] = S.prev_rot[i];
+            return;
+        }
+        const quat<T> q0 = q4(r0);
+        const mat3<T> R = mat3_cast(q0);
+        const smat3<T> Iw = sym_of(mul(R, s3(S.inertia[i])) * R.transpose());
+        const smat3<T> Iinvw = sym_of(mul(R, s3(S.inv_inertia[i])) * R.transpose());
+        D.prev_pos[j] = p0;
+        vec3<T> v = v3(l);
+        v += v3(S.force[i]) * l.w * dt;
+        D.lin[j] = v4(v, l.w);
+        vec3<T> x = vec3<T>(v3(p0));
+        x += v * dt;
+        D.pos[j] = V4<P>{P(x.x), P(x.y), P(x.z), P(0)};
+        D.prev_rot[j] = r0;
+        vec3<T> w = v3(a0);
+        w += (Iinvw * dt) * (v3(S.torque[i]) - cross(w, Iw * w));
+        D.ang[j] = v4(w);
+        const vec3<T> os = w * (T(0.5) * dt);
+        const quat<T> r(T(0.0), os.x, os.y, os.z);
+        D.rot[j] = q4s(normalize(q0 + r * q0));
+    }
+
     // update_velocities for one body (Body.cpp:41-57)
     template <class T, class P>
     __device__ void update_velocity_body(const Bodies<T, P> &B, uint32_t i, T inv_dt)
