@@ -1864,8 +1864,16 @@ namespace rbps_gpu
     // One phase of one large world on the whole cooperative grid; the phases
     // are separate launches so that the GJK pass can run between the
     // narrowphase and the colouring, as it does for the small worlds.
+    // Resident 256-thread CTAs per SM of the cooperative grid, as for the
+    // frame: capped at 128 registers (two CTAs), collision stress went from
+    // 7.45 to 6.53 ms a step and joint-heavy from 5.53 to 5.12 ms (same box);
+    // three CTAs (80 registers) spilled: 6.52 and 5.69 ms.
+#ifndef RBPS_BIG_MIN_BLOCKS
+#define RBPS_BIG_MIN_BLOCKS 2
+#endif
     template <class T, class P>
-    __global__ void __launch_bounds__(kMaxBlock) k_big_phase(const Engine<T, P> E, uint32_t w, int phase)
+    __global__ void __launch_bounds__(kMaxBlock, RBPS_BIG_MIN_BLOCKS) k_big_phase(const Engine<T, P> E, uint32_t w,
+                                                                               int phase)
     {
         __shared__ BlockShared sh;
         GridTeam tm;
