@@ -243,6 +243,7 @@ namespace rbps_gpu
     // that is not the last sort's output); the caller then sorts in full.
     // Every thread of the CTA must call it; it ends with a block barrier.
     constexpr uint32_t kMergeMax = 512;
+    static_assert(3 * kSmemSortMax + 6 * kMergeMax <= kSmemSortWords, "the merge's lists fit the staging area");
 
     static __device__ __noinline__ bool merge_moved_endpoints(uint32_t *ep_key, uint32_t *ep_id, uint32_t *ep_pos, uint32_t nep,
                                                        uint32_t id_limit, const uint32_t *moved, uint32_t *smem,
